@@ -1,0 +1,167 @@
+/* bd_b200 -- B200-native Brownian-dynamics step path for charged bead-spring
+ * chains in deforming-brick shear and Kraynik-Reinelt planar extension.
+ *
+ * C ABI of the drop-in boundary.  The reference simulator's step loop is a
+ * set of `void f(void)` routines that exchange data through file-scope
+ * globals (shear/src/main.h:7-65, shear/src/Parameters.h:44-201).  Each
+ * routine below replaces one of them, operating on device-resident state
+ * owned by a bd_ctx instead of on globals; the upload/download calls move
+ * the reference's global arrays in and out, with the reference's layouts
+ * (three double arrays rx/ry/rz of N beads, forces fx/fy/fz, noise R[3N]
+ * interleaved x,y,z per bead, dense mobility M[9 N^2] row-major by 3x3
+ * block).
+ *
+ * Conventions
+ *  - every call returns a bd_status; 0 is success;
+ *  - calls are asynchronous on the context's CUDA stream unless they return
+ *    data to the host (downloads, bd_sync), which synchronise and report any
+ *    error a kernel recorded since the last check;
+ *  - where the reference prints a message and calls exit(1) (FENE
+ *    overstretch, shear/src/main26.c:553-558), the library records a status
+ *    and returns it instead; nothing in the library exits the process;
+ *  - no call falls back to the CPU: without a usable CUDA device bd_create
+ *    fails with BD_ERR_CUDA.
+ */
+#ifndef BD_B200_H
+#define BD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  BD_OK = 0,
+  BD_ERR_ARG = 1,          /* bad argument or size */
+  BD_ERR_CUDA = 2,         /* CUDA runtime failure / no device */
+  BD_ERR_OOM = 3,          /* device allocation failed */
+  BD_ERR_OVERSTRETCH = 4,  /* FENE bond longer than qmax */
+  BD_ERR_NONFINITE = 5,    /* NaN/Inf in a force or displacement */
+  BD_ERR_NBR_OVERFLOW = 6, /* neighbour row longer than the configured cap */
+  BD_ERR_GRID_RANGE = 7,   /* far-field displacement outside the lookup table */
+  BD_ERR_STATE = 8,        /* call out of order (e.g. no mobility built) */
+  BD_ERR_TIMEOUT = 9,      /* a bounded device wait gave up */
+  BD_ERR_LANCZOS = 10,     /* Krylov square root missed its tolerance */
+  BD_ERR_ASYMMETRIC = 11   /* lookup tensor not symmetric */
+} bd_status;
+
+typedef enum { BD_FLOW_SHEAR = 0, BD_FLOW_EXT = 1 } bd_flow;
+typedef enum { BD_SPRING_HOOKEAN = 0, BD_SPRING_FENE = 1 } bd_spring;
+
+/* System parameters.  The names follow the reference's globals
+ * (shear/src/Parameters.h:57-199) and Input.txt keys
+ * (shear/src/Initialization.c:157-174). */
+typedef struct {
+  int flow;           /* bd_flow */
+  int Nb, Nc;         /* beads per chain, chains */
+  double L;           /* cubic box edge */
+  double box_volume;  /* 0 -> L^3 (used by the k-space mobility sum) */
+  double edot;        /* strain rate (flowrate) */
+  double dt;          /* time step */
+  int spring;         /* bd_spring */
+  double kappas, qmax, kappab, epsilon;
+  /* Reference-compatible force-law switches (0 = reference behaviour):
+   * shear_kappas_override: 0 -> kappas forced to 200 in the shear tree
+   * (shear/src/main26.c:544) as the reference does; 1 -> use kappas. */
+  int shear_kappas_override;
+  double lambda_b, lambda_d; /* Bjerrum and Debye lengths */
+  int Ncharges;
+  double barrier, barrier2;  /* adjacent / non-adjacent hop barriers */
+  int MStep;                 /* charge-hop sweep period */
+  int nt_avg;                /* lookup-table lattice frames */
+  double bin_size;           /* lookup-table bin edge */
+  int srpy;                  /* mobility rebuild period; 0 -> 100 */
+  int sbins;                 /* CA-TEA strain bins; 0 -> 20 */
+  double strain_ss;          /* CA-TEA steady-state strain; 0 -> 10 */
+  int max_neighbors;         /* neighbour-row cap; 0 -> 256 */
+  long seed;                 /* ran1 seed (fixSeed=1: 830062920 shear, 981272199 ext) */
+} bd_params;
+
+typedef struct bd_ctx bd_ctx;
+
+/* State of the reference's ran1/gasdev generator
+ * (shear/src/Initialization.c:601-634, shear/src/main26.c:515-540). */
+typedef struct {
+  long idum, idum2, iy;
+  long iv[32];
+  int iset;
+  float gset;
+} bd_ran1_state;
+
+/* ---- context ------------------------------------------------------------
+ * replaces Initialization()/allocate() (shear/src/Initialization.c:3-23,
+ * 318-457): allocates device state for N = Nb*Nc beads. */
+int bd_create(const bd_params *p, bd_ctx **out);
+int bd_destroy(bd_ctx *ctx);
+const char *bd_status_string(int status);
+int bd_sync(bd_ctx *ctx);
+/* Device bytes currently held by the context. */
+size_t bd_device_bytes(const bd_ctx *ctx);
+
+/* ---- state transfer (the reference's global arrays) --------------------- */
+int bd_upload_positions(bd_ctx *ctx, const double *rx, const double *ry, const double *rz);
+int bd_download_positions(bd_ctx *ctx, double *rx, double *ry, double *rz);
+int bd_upload_displacements(bd_ctx *ctx, const double *dxv, const double *dyv, const double *dzv);
+int bd_download_displacements(bd_ctx *ctx, double *dxv, double *dyv, double *dzv);
+int bd_upload_forces(bd_ctx *ctx, const double *fx, const double *fy, const double *fz);
+int bd_download_forces(bd_ctx *ctx, double *fx, double *fy, double *fz);
+/* tauxx, tauyy, tauxy virial accumulators (shear/src/Parameters.h:98,138) */
+int bd_download_stress(bd_ctx *ctx, double *out3);
+int bd_reset_stress(bd_ctx *ctx);
+int bd_upload_noise(bd_ctx *ctx, const double *R);
+int bd_download_noise(bd_ctx *ctx, double *R);
+/* Charge_track (bead of each charge); sets Charge[] flags to 1 there
+ * (shear/src/main26.c:490-506). */
+int bd_set_charges(bd_ctx *ctx, const int *track, int ncharges);
+int bd_download_charges(bd_ctx *ctx, int *track, int *old, int *flags);
+int bd_set_rng(bd_ctx *ctx, const bd_ran1_state *s);
+int bd_get_rng(bd_ctx *ctx, bd_ran1_state *s);
+/* One lattice frame (nt < nt_avg) of the far-field lookup table read from
+ * mm/G*.txt by initEwald (shear/src/Initialization.c:497-520): num_bins
+ * row-major 3x3 tensors.  The tensors must be symmetric. */
+int bd_load_grid(bd_ctx *ctx, int nt, const double *D9);
+/* Lookup-grid geometry as initLattice derives it
+ * (shear/src/Initialization.c:281-295): nbx nby nbz nhx nhy nhz num_bins. */
+int bd_grid_shape(const bd_ctx *ctx, int *out7);
+/* CA-TEA parameters of one strain bin (bp[sbin], C[sbin][3 Nb]) read from
+ * decomp/DC*.txt (shear/src/Initialization.c:528-536). */
+int bd_set_tea(bd_ctx *ctx, int sbin, double beta, const double *c3nb);
+
+/* ---- step-loop routines (reference name in brackets) -------------------- */
+int bd_set_time(bd_ctx *ctx, unsigned long t, unsigned long tstart);
+int bd_update_lattice(bd_ctx *ctx, unsigned long t);   /* [updateLattice] main26.c:1382 */
+/* L1x L1y L2x L2y L1xp L1yp L2xp L2yp detL tp */
+int bd_get_lattice(const bd_ctx *ctx, double *out10);
+int bd_apply_pbc(bd_ctx *ctx);                         /* [applyPBC] main26.c:1409 */
+int bd_transform_coords(bd_ctx *ctx);                  /* [transformCoords] main14.c:1514 */
+int bd_inverse_coords(bd_ctx *ctx);                    /* [inverseCoords] main14.c:1525 */
+int bd_reset_force(bd_ctx *ctx);                       /* [resetForce] main26.c:509 */
+int bd_build_neighbors(bd_ctx *ctx);                   /* [verletlist] main26.c:682 */
+int bd_check_verlet(bd_ctx *ctx);                      /* [checkVerlet] main26.c:858 */
+/* Half list as verletlist stores it: counts[N], rows[N*maxnb] ascending. */
+int bd_download_neighbors(bd_ctx *ctx, int *counts, int *rows, int maxnb);
+int bd_bond_force(bd_ctx *ctx);                        /* [bondforce] main26.c:541 */
+int bd_ev_force(bd_ctx *ctx);                          /* [LJforce] main26.c:619 */
+int bd_coulomb_force(bd_ctx *ctx);                     /* [coulombForce] main26.c:1891 */
+int bd_get_noise(bd_ctx *ctx);                         /* [getNoise] main26.c:708 */
+int bd_calc_hi(bd_ctx *ctx);                           /* [calcHI] main26.c:1530 */
+/* Dense reference layout 9 N^2 (upper blocks and diagonal entries of the
+ * diagonal blocks filled, as calcHI leaves them). */
+int bd_download_mobility(bd_ctx *ctx, double *M9);
+int bd_update_hi(bd_ctx *ctx);                         /* [updateHI] main26.c:745 */
+int bd_update_fd(bd_ctx *ctx);                         /* [updateFD] main26.c:731 */
+int bd_charge_hop(bd_ctx *ctx);                        /* [chargeHop] main26.c:1926 */
+/* Per-charge outcome of the last sweep: (0 skipped,1 accepted,2 rejected),
+ * target bead, move kind; 3 ints per charge. */
+int bd_download_hop_log(bd_ctx *ctx, int *log3);
+
+/* One reference-mode hydrodynamic step (the body of the step loop,
+ * shear/src/main26.c:65-151, extensional/src/main14.c:68-171, without file
+ * output), repeated nsteps times from step t0. */
+int bd_step_reference(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

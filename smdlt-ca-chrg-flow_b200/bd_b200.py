@@ -1,0 +1,354 @@
+"""Python binding of the bd_b200 C ABI (include/bd_b200.h).
+
+A thin ctypes layer over ``libbd_b200.so``: every method calls one exported C
+function and raises :class:`BDError` on a non-zero status.  The library is
+the CUDA implementation; there is no CPU path behind this module, and loading
+fails loudly when the shared library has not been built.
+
+Method names follow the reference's step-loop routines
+(shear/src/main.h:7-65): ``bond_force`` is bondforce, ``ev_force`` is
+LJforce, ``coulomb_force`` is coulombForce, ``build_neighbors`` is verletlist,
+``calc_hi``/``update_hi``/``update_fd``/``charge_hop`` are calcHI, updateHI,
+updateFD and chargeHop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "libbd_b200.so")
+INCLUDE = os.path.join(ROOT, "include")
+SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+FLOW_SHEAR, FLOW_EXT = 0, 1
+SPRING_HOOKEAN, SPRING_FENE = 0, 1
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libbd_b200.so for sm_100a with nvcc (in-tree)."""
+    srcs = [os.path.join(PKG, "csrc", s) for s in SOURCES]
+    cmd = ["nvcc", "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+           f"-I{INCLUDE}", "-o", LIB, *srcs]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+class BDError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        msg = _lib().bd_status_string(status).decode() if _LIB else str(status)
+        super().__init__(f"{where}: {msg} (status {status})")
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("flow", C.c_int), ("Nb", C.c_int), ("Nc", C.c_int), ("L", C.c_double),
+        ("box_volume", C.c_double), ("edot", C.c_double), ("dt", C.c_double),
+        ("spring", C.c_int), ("kappas", C.c_double), ("qmax", C.c_double),
+        ("kappab", C.c_double), ("epsilon", C.c_double), ("shear_kappas_override", C.c_int),
+        ("lambda_b", C.c_double), ("lambda_d", C.c_double), ("Ncharges", C.c_int),
+        ("barrier", C.c_double), ("barrier2", C.c_double), ("MStep", C.c_int),
+        ("nt_avg", C.c_int), ("bin_size", C.c_double), ("srpy", C.c_int), ("sbins", C.c_int),
+        ("strain_ss", C.c_double), ("max_neighbors", C.c_int), ("seed", C.c_long),
+    ]
+
+
+class Ran1State(C.Structure):
+    _fields_ = [("idum", C.c_long), ("idum2", C.c_long), ("iy", C.c_long),
+                ("iv", C.c_long * 32), ("iset", C.c_int), ("gset", C.c_float)]
+
+    def state_words(self) -> np.ndarray:
+        g = np.float32(self.gset).view(np.int32)
+        return np.array([self.idum, self.idum2, self.iy, *self.iv, self.iset, int(g)],
+                        dtype=np.int64)
+
+
+_LIB = None
+
+
+def _lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB):
+            raise OSError(f"{LIB} is not built; run __graft_entry__.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB)
+        vp = C.c_void_p
+        L.bd_status_string.restype = C.c_char_p
+        L.bd_status_string.argtypes = [C.c_int]
+        L.bd_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+        L.bd_destroy.argtypes = [vp]
+        L.bd_sync.argtypes = [vp]
+        L.bd_device_bytes.argtypes = [vp]
+        L.bd_device_bytes.restype = C.c_size_t
+        for n in ("bd_upload_positions", "bd_download_positions", "bd_upload_displacements",
+                  "bd_download_displacements", "bd_upload_forces", "bd_download_forces"):
+            getattr(L, n).argtypes = [vp, _dp, _dp, _dp]
+        L.bd_download_stress.argtypes = [vp, _dp]
+        L.bd_reset_stress.argtypes = [vp]
+        L.bd_upload_noise.argtypes = [vp, _dp]
+        L.bd_download_noise.argtypes = [vp, _dp]
+        L.bd_set_charges.argtypes = [vp, _ip, C.c_int]
+        L.bd_download_charges.argtypes = [vp, _ip, _ip, _ip]
+        L.bd_set_rng.argtypes = [vp, C.POINTER(Ran1State)]
+        L.bd_get_rng.argtypes = [vp, C.POINTER(Ran1State)]
+        L.bd_load_grid.argtypes = [vp, C.c_int, _dp]
+        L.bd_grid_shape.argtypes = [vp, _ip]
+        L.bd_set_tea.argtypes = [vp, C.c_int, C.c_double, _dp]
+        L.bd_set_time.argtypes = [vp, C.c_ulong, C.c_ulong]
+        L.bd_update_lattice.argtypes = [vp, C.c_ulong]
+        L.bd_get_lattice.argtypes = [vp, _dp]
+        for n in ("bd_apply_pbc", "bd_transform_coords", "bd_inverse_coords", "bd_reset_force",
+                  "bd_build_neighbors", "bd_check_verlet", "bd_bond_force", "bd_ev_force",
+                  "bd_coulomb_force", "bd_get_noise", "bd_calc_hi", "bd_update_hi",
+                  "bd_update_fd", "bd_charge_hop"):
+            getattr(L, n).argtypes = [vp]
+        L.bd_download_neighbors.argtypes = [vp, _ip, _ip, C.c_int]
+        L.bd_download_mobility.argtypes = [vp, _dp]
+        L.bd_download_hop_log.argtypes = [vp, _ip]
+        L.bd_step_reference.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
+        _LIB = L
+    return _LIB
+
+
+def exported_symbols() -> list[str]:
+    """Names declared in include/bd_b200.h (for the ABI export test)."""
+    import re
+    txt = open(os.path.join(INCLUDE, "bd_b200.h")).read()
+    return sorted(set(re.findall(r"\b(bd_[a-z0-9_]+)\s*\(", txt)))
+
+
+def _chk(status: int, where: str) -> None:
+    if status != 0:
+        raise BDError(status, where)
+
+
+def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3.0, kappab=0.0,
+                epsilon=1.0, lambda_b=2.0, lambda_d=5.0, Ncharges=0, barrier=3.0, barrier2=3.0,
+                MStep=100, nt_avg=8, bin_size=2.0, srpy=100, sbins=20, strain_ss=10.0,
+                max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0) -> Params:
+    p = Params()
+    p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
+    p.box_volume = box_volume
+    p.spring = SPRING_FENE if spring == "FENE" else SPRING_HOOKEAN
+    p.kappas, p.qmax, p.kappab, p.epsilon = kappas, qmax, kappab, epsilon
+    p.shear_kappas_override = shear_kappas_override
+    p.lambda_b, p.lambda_d, p.Ncharges = lambda_b, lambda_d, Ncharges
+    p.barrier, p.barrier2, p.MStep = barrier, barrier2, MStep
+    p.nt_avg, p.bin_size, p.srpy, p.sbins, p.strain_ss = nt_avg, bin_size, srpy, sbins, strain_ss
+    p.max_neighbors = max_neighbors
+    p.seed = (830062920 if flow == FLOW_SHEAR else 981272199) if seed is None else seed
+    return p
+
+
+class Context:
+    """Device-resident system; one CUDA stream per context."""
+
+    def __init__(self, params: Params):
+        self.L = _lib()
+        self.p = params
+        self.N = params.Nb * params.Nc
+        h = C.c_void_p()
+        _chk(self.L.bd_create(C.byref(params), C.byref(h)), "bd_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _call(self, name, *args):
+        _chk(getattr(self.L, name)(self.h, *args), name)
+
+    # state transfer
+    def set_positions(self, x, y, z):
+        self._call("bd_upload_positions", *(np.ascontiguousarray(a, np.float64) for a in (x, y, z)))
+
+    def positions(self):
+        a = [np.zeros(self.N) for _ in range(3)]
+        self._call("bd_download_positions", *a)
+        return a
+
+    def set_displacements(self, x, y, z):
+        self._call("bd_upload_displacements", *(np.ascontiguousarray(a, np.float64) for a in (x, y, z)))
+
+    def displacements(self):
+        a = [np.zeros(self.N) for _ in range(3)]
+        self._call("bd_download_displacements", *a)
+        return np.stack(a)
+
+    def set_forces(self, x, y, z):
+        self._call("bd_upload_forces", *(np.ascontiguousarray(a, np.float64) for a in (x, y, z)))
+
+    def forces(self):
+        a = [np.zeros(self.N) for _ in range(3)]
+        self._call("bd_download_forces", *a)
+        return np.stack(a)
+
+    def stress(self):
+        o = np.zeros(3)
+        self._call("bd_download_stress", o)
+        return o
+
+    def set_noise(self, R):
+        self._call("bd_upload_noise", np.ascontiguousarray(R, np.float64))
+
+    def noise(self):
+        o = np.zeros(3 * self.N)
+        self._call("bd_download_noise", o)
+        return o
+
+    def set_charges(self, track):
+        t = np.ascontiguousarray(track, np.int32)
+        self._call("bd_set_charges", t, len(t))
+        self.nch = len(t)
+
+    def charges(self):
+        n = getattr(self, "nch", 0)
+        tr, old = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
+        fl = np.zeros(self.N, np.int32)
+        self._call("bd_download_charges", tr, old, fl)
+        return tr[:n], old[:n], fl
+
+    def set_rng(self, state: Ran1State):
+        self._call("bd_set_rng", C.byref(state))
+
+    def rng(self) -> Ran1State:
+        s = Ran1State()
+        self._call("bd_get_rng", C.byref(s))
+        return s
+
+    def grid_shape(self):
+        o = np.zeros(7, np.int32)
+        self._call("bd_grid_shape", o)
+        return o
+
+    def load_grid(self, nt, D9):
+        self._call("bd_load_grid", int(nt), np.ascontiguousarray(D9, np.float64))
+
+    def set_tea(self, sbin, beta, c3nb):
+        self._call("bd_set_tea", int(sbin), float(beta), np.ascontiguousarray(c3nb, np.float64))
+
+    # step-loop routines
+    def set_time(self, t, tstart=0):
+        self._call("bd_set_time", int(t), int(tstart))
+
+    def update_lattice(self, t):
+        self._call("bd_update_lattice", int(t))
+
+    def lattice(self):
+        o = np.zeros(10)
+        self._call("bd_get_lattice", o)
+        return o
+
+    def neighbors(self, maxnb=256):
+        cnt = np.zeros(self.N, np.int32)
+        rows = np.zeros((self.N, maxnb), np.int32)
+        self._call("bd_download_neighbors", cnt, rows, maxnb)
+        return cnt, rows
+
+    def mobility(self):
+        o = np.zeros(9 * self.N * self.N)
+        self._call("bd_download_mobility", o)
+        return o
+
+    def hop_log(self):
+        n = getattr(self, "nch", 0)
+        o = np.zeros(3 * max(n, 1), np.int32)
+        self._call("bd_download_hop_log", o)
+        return o.reshape(-1, 3)[:n]
+
+    def step_reference(self, t0, nsteps, with_hop=True):
+        self._call("bd_step_reference", int(t0), int(nsteps), int(bool(with_hop)))
+
+    def sync(self):
+        self._call("bd_sync")
+
+    def device_bytes(self) -> int:
+        return int(self.L.bd_device_bytes(self.h))
+
+
+for _n in ("apply_pbc", "transform_coords", "inverse_coords", "reset_force", "build_neighbors",
+           "check_verlet", "bond_force", "ev_force", "coulomb_force", "get_noise", "calc_hi",
+           "update_hi", "update_fd", "charge_hop"):
+    setattr(Context, _n, (lambda name: lambda self: self._call("bd_" + name))(_n))
+
+
+# ---------------------------------------------------------------------------
+# synthetic inputs
+
+
+def random_chains(Nb, Nc, L, seed, bond=2.0, min_sep=0.0, max_tries=200):
+    """Seeded random-walk chains of bond length ``bond`` in a cubic box of edge L
+    centred at the origin, returned as three float64 arrays.  With min_sep > 0
+    each new bead is redrawn (up to max_tries) until it is at least min_sep from
+    every earlier bead, like the reference's own initialiser
+    (shear/src/main26.c:437-457)."""
+    rng = np.random.default_rng(seed)
+    N = Nb * Nc
+    r = np.zeros((N, 3))
+    for c in range(Nc):
+        for b in range(Nb):
+            a = c * Nb + b
+            for _ in range(max_tries):
+                if b == 0:
+                    p = rng.uniform(-L / 2, L / 2, 3)
+                else:
+                    v = rng.normal(size=3)
+                    p = r[a - 1] + bond * v / np.linalg.norm(v)
+                if min_sep <= 0 or a == 0:
+                    break
+                d = r[:a] - p
+                d -= L * np.round(d / L)
+                if np.min(np.einsum("ij,ij->i", d, d)) >= min_sep * min_sep:
+                    break
+            r[a] = p
+    return [np.ascontiguousarray(r[:, k]) for k in range(3)]
+
+
+def lab_frame(flow, x, y):
+    """Rotate chains generated in a cubic box into the lab frame of the flow.
+
+    In extension the t = 0 cell is the cube rotated by theta = atan(L1y/L1x)
+    = 31.7 degrees, so chains built with cubic periodicity are rotated by theta
+    as the reference does after building them (extensional/src/main14.c:483-490).
+    Shear needs no rotation."""
+    if flow == FLOW_SHEAR:
+        return x, y
+    th = np.deg2rad(90.0 - (45.0 + 31.7))
+    l1x, l1y = np.cos(th) + np.sin(th), -np.sin(th) + np.cos(th)
+    t = np.arctan(l1y / l1x)
+    c, s = np.cos(t), np.sin(t)
+    return np.ascontiguousarray(x * c - y * s), np.ascontiguousarray(x * s + y * c)
+
+
+def random_charges(Nb, Nc, frac, seed):
+    """A seeded random subset of each chain's beads (frac of them) as bead indices."""
+    rng = np.random.default_rng(seed)
+    out = []
+    k = int(round(frac * Nb))
+    for c in range(Nc):
+        out.extend(sorted(c * Nb + rng.choice(Nb, size=k, replace=False)))
+    return np.array(out, np.int32)

@@ -1,0 +1,100 @@
+// Context layout shared by the bd_b200 translation units.
+//
+// Device memory layout (all FP64 unless noted):
+//   positions rx, ry, rz          SoA, N each (the reference's globals)
+//   forces fx, fy, fz             SoA
+//   displacement since last neighbour build dxv, dyv, dzv
+//   noise R                       3N, interleaved x,y,z per bead (as R[])
+//   neighbour rows                N x max_neighbors int32, full list sorted
+//                                 ascending; half list = entries > i
+//   mobility tiles                packed upper triangle of 32x32-bead tiles,
+//                                 each tile 6 x 32 x 32 (xx xy xz yy yz zz)
+//   lookup grid                   nt_avg x num_bins x 6
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "bd_internal.cuh"
+
+struct bd_ctx {
+  bd_params p;
+  int N, Nb, Nc;
+  cudaStream_t stream;
+  int device;
+
+  // derived constants
+  double rv, r2cut, rnew, qmax2, kappa_d, boxvol, kappas_eff;
+  int tp, srpy, sbins, maxnb;
+  double strain_ss, strain_interval;
+  // lookup grid geometry (initLattice, shear/src/Initialization.c:281-295)
+  int nbx, nby, nbz, nhx, nhy, nhz, nbins;
+  double bsx, bsy, bsz;
+
+  // step state (host-side mirror)
+  unsigned long t, tstart;
+  double strain;
+  bd::Lat lat;
+
+  // device state
+  double *rx, *ry, *rz, *fx, *fy, *fz, *dxv, *dyv, *dzv, *R;
+  double *stress;  // 3
+  int *err;        // error bits
+  int *flag;       // [0] neighbour rebuild due
+  int nch;
+  int *track, *old, *cflags, *hoplog;  // charges
+  double *q;                           // bead charge values (0/1 in reference mode)
+  double *dE;                          // charge-hop energy scratch
+  bd::Ran1 *rng;
+
+  // neighbours
+  int *nb_count, *nb_rows, *nb_half;
+  int *cell_of, *cell_count, *cell_start, *cell_beads, *cell_cursor;
+  int ncell_cap;
+
+  // mobility (packed symmetric tiles)
+  int NT;
+  size_t ntiles;
+  double *Mt;
+  int *tileI;  // tile row index of each packed tile
+  double *grid;
+  int grid_loaded_mask;
+  int *near_pairs, *near_count;
+  size_t near_cap;
+  double *kvec;
+  int kvec_cap, nk;
+  double Dtr[3];
+  bool hi_built;
+  double *rowpart, *colpart;  // matvec partial sums (scratch)
+  double *U, *W;              // M F and off-diagonal M R
+  double *Ctab;               // (sbins+1) x 3 Nb
+  std::vector<double> btab;
+  double bt;
+  int sbin;
+
+  size_t bytes;
+};
+
+namespace bd {
+
+int set_error_from_bits(int bits);
+int check(bd_ctx* c);                 // synchronise and fold device error bits
+int launch_ok(bd_ctx* c);             // report an asynchronous launch error
+void host_lattice(bd_ctx* c, unsigned long t, Lat* out);
+void rotate_coords(bd_ctx* c, int inverse);  // transformCoords (0) / inverseCoords (1)
+
+// neighbours
+int build_neighbors(bd_ctx* c, bool force);
+int alloc_neighbors(bd_ctx* c);
+
+// mobility
+int alloc_mobility(bd_ctx* c);
+int calc_hi(bd_ctx* c);
+int update_hi(bd_ctx* c);
+int download_mobility(bd_ctx* c, double* M9);
+
+// charge hopping
+int charge_hop(bd_ctx* c);
+
+}  // namespace bd

@@ -1,0 +1,663 @@
+// Dense hybrid Rotne-Prager-Yamakawa mobility (reference mode) and the TEA
+// Brownian displacement.
+//
+// Storage.  M is symmetric with symmetric 3x3 blocks, so only the upper
+// triangle of 32x32-bead tiles is stored, six unique components per block,
+// component-major inside a tile: tile(I,J), I <= J, at packed index
+// I*NT - I*(I-1)/2 + (J-I), element (c, il, jl) at c*1024 + il*32 + jl.
+// A warp reading one (c, il) row reads 256 contiguous bytes.  The diagonal
+// blocks are the reference's uniform self term Dtr (calcHI writes only their
+// diagonal entries, shear/src/main26.c:1687-1692) and are kept as 3 scalars.
+//
+// Build (calcHI, shear/src/main26.c:1530-1806).  A far pass evaluates the
+// minimum image over the (nx,ny) images for every pair (getNIDbin), copies
+// the lookup tensor for pairs at 12 or more, and appends nearer pairs to a
+// list with one atomic per warp.  A near pass gives each listed pair a warp
+// whose lanes split the real-space image sum and the k-space cosine sum.
+// The k-vectors, their coefficients and Dtr are generated on the host with
+// the reference's loop bounds and arithmetic.
+//
+// Matvec.  One CTA per tile applies the block to both the tile's rows and its
+// columns (block symmetry) for two right-hand sides at once, and writes the
+// two partial sums to scratch; a two-level reduction sums them per bead in a
+// fixed order, so results are deterministic without atomics.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bd_ctx.cuh"
+
+using namespace bd;
+
+#define CU(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
+  } while (0)
+
+static const int kRedSplit = 16;  // column-range splits of the matvec reduction
+
+struct Ewald {
+  double alpha, alpha2, alpha3, alpha5, alpha7, rce, rtpi;
+  int nmax, nt, nk;
+};
+
+__device__ __forceinline__ long long tile_off(int I, int NT) {
+  return (long long)I * NT - (long long)I * (I - 1) / 2;
+}
+
+// Real-space Beenakker RPY terms for one image at squared distance rr
+// (shear/src/main26.c:1727-1741), with the overlap form for r <= 2.
+__device__ __forceinline__ void rpy_real(const Ewald& e, double rr, double& t1, double& t2) {
+  double r = sqrt(rr), C1, C2, C3, C4;
+  double a = e.alpha, a3 = e.alpha3, a5 = e.alpha5, a7 = e.alpha7;
+  if (r > 2.0) {
+    C1 = 0.75 / r + 0.5 / (r * rr);
+    C2 = 4.0 * a7 * rr * rr + 3.0 * a3 * rr - 20.0 * a5 * rr - 4.5 * a + 14.0 * a3 + a / rr;
+    C3 = 0.75 / r - 1.5 / (r * rr);
+    C4 = -4.0 * a7 * rr * rr - 3.0 * a3 * rr + 16.0 * a5 * rr + 1.5 * a - 2.0 * a3 - 3.0 * a / rr;
+  } else {
+    C1 = 1.0 - 0.28125 * r;
+    C2 = 64.0 * a7 + 12.0 * a3 - 80.0 * a5 - 4.5 * a + 14.0 * a3 + 0.25 * a;
+    C3 = 0.09375 * r;
+    C4 = -64.0 * a7 - 12.0 * a3 + 64.0 * a5 + 1.5 * a - 2.0 * a3 - 0.75 * a;
+  }
+  double ec = erfc(a * r), ex = exp(-e.alpha2 * rr) / e.rtpi;
+  t1 = C1 * ec + C2 * ex;
+  t2 = C3 * ec + C4 * ex;
+}
+
+__global__ void __launch_bounds__(256) k_hi_far(Lat l, Ewald ew, const double* __restrict__ rx,
+                                                const double* __restrict__ ry,
+                                                const double* __restrict__ rz, int N, int NT,
+                                                const int* __restrict__ tileI,
+                                                const double* __restrict__ grid, int nbx,
+                                                int nby, int nbz, int nhx, int nhy, int nhz,
+                                                double bsx, double bsy, double bsz, int nbins,
+                                                double* Mt, int2* near, int* near_count,
+                                                long long near_cap, int* err) {
+  long long tile = blockIdx.x;
+  int I = tileI[tile];
+  int J = I + (int)(tile - tile_off(I, NT));
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* tb = Mt + tile * 6144;
+  const double* gt = grid + (size_t)ew.nt * nbins * 6;
+  for (int q = 0; q < 4; q++) {
+    int il = w + 8 * q;
+    int i = I * 32 + il, j = J * 32 + lane;
+    bool pair = (i < j) && (j < N);
+    bool is_near = false;
+    double m[6] = {0, 0, 0, 0, 0, 0};
+    if (pair) {
+      double vx, vy, vz;
+      // getNIDbin(j, i) (shear/src/main26.c:1709)
+      min_image_bin(l, subx(rx[j], rx[i]), subx(ry[j], ry[i]), subx(rz[j], rz[i]), vx, vy, vz);
+      double d = sqrt(rr3(vx, vy, vz));
+      if (d < 12.0) {
+        is_near = true;
+      } else {
+        // binij(i, j) uses getNIDbin(j, i) as well (shear/src/main26.c:1518-1529)
+        // the flattened index is used as the reference computes it: a bin
+        // just off the table on one axis aliases to a neighbouring table row
+        int bx = (int)(round(vx / bsx) + nhx), by = (int)(round(vy / bsy) + nhy);
+        int bz = (int)(round(vz / bsz) + nhz);
+        long long b = (long long)nby * nbz * bx + (long long)nbz * by + bz;
+        if (b < 0 || b >= nbins) {
+          atomicOr(err, ERRB_GRID_RANGE);
+        } else {
+          const double* g = gt + (size_t)b * 6;
+          for (int a = 0; a < 6; a++) m[a] = g[a];
+        }
+      }
+    }
+    unsigned bal = __ballot_sync(0xffffffffu, is_near);
+    if (bal) {
+      int base = 0;
+      int leader = __ffs(bal) - 1;
+      if (lane == leader) base = atomicAdd(near_count, __popc(bal));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (is_near) {
+        long long k = base + __popc(bal & ((1u << lane) - 1));
+        if (k < near_cap)
+          near[k] = make_int2(i, j);
+        else
+          atomicOr(err, ERRB_NBR_OVERFLOW);
+      }
+    }
+    for (int a = 0; a < 6; a++) tb[a * 1024 + il * 32 + lane] = m[a];
+  }
+}
+
+// kvec rows: rkx rky rkz m00 m01 m02 m11 m12 m22
+__device__ __forceinline__ void near_pair(const Lat& l, const Ewald& ew,
+                                          const double* __restrict__ rx,
+                                          const double* __restrict__ ry,
+                                          const double* __restrict__ rz, int NT, int2 ij,
+                                          const double* __restrict__ kvec, double* Mt, int lane);
+
+// Grid-stride over the near-pair list, one warp per pair.
+__global__ void __launch_bounds__(256) k_hi_near(Lat l, Ewald ew, const double* __restrict__ rx,
+                                                 const double* __restrict__ ry,
+                                                 const double* __restrict__ rz, int NT,
+                                                 const int2* __restrict__ near,
+                                                 const int* __restrict__ near_count,
+                                                 long long near_cap,
+                                                 const double* __restrict__ kvec, double* Mt) {
+  int lane = threadIdx.x & 31;
+  long long np = min((long long)*near_count, near_cap);
+  long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw)
+    near_pair(l, ew, rx, ry, rz, NT, near[p], kvec, Mt, lane);
+}
+
+__device__ __forceinline__ void near_pair(const Lat& l, const Ewald& ew,
+                                          const double* __restrict__ rx,
+                                          const double* __restrict__ ry,
+                                          const double* __restrict__ rz, int NT, int2 ij,
+                                          const double* __restrict__ kvec, double* Mt, int lane) {
+  int i = ij.x, j = ij.y;
+  double rxi, ryi, rxj, ryj;
+  if (l.flow == 0) {
+    rxi = rx[i];
+    ryi = ry[i];
+    rxj = rx[j];
+    ryj = ry[j];
+  } else {
+    // positions are held in the rotated frame; calcHI rotates them back
+    // (extensional/src/main14.c:1720-1726)
+    rxi = rx[i] * l.cth - ry[i] * l.sth;
+    ryi = rx[i] * l.sth + ry[i] * l.cth;
+    rxj = rx[j] * l.cth - ry[j] * l.sth;
+    ryj = rx[j] * l.sth + ry[j] * l.cth;
+  }
+  double dxo = rxj - rxi, dyo = ryj - ryi, dzo = rz[j] - rz[i];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int side = 2 * ew.nmax + 1, nimg = side * side * side;
+  for (int m = lane; m < nimg; m += 32) {
+    int nz = m % side - ew.nmax, ny = (m / side) % side - ew.nmax, nx = m / (side * side) - ew.nmax;
+    double dx = dxo + nx * l.L1x + ny * l.L2x;
+    double dy = dyo + nx * l.L1y + ny * l.L2y;
+    double dz = dzo + nz * l.L;
+    double rr = dx * dx + dy * dy + dz * dz;
+    if (sqrt(rr) < ew.rce) {
+      double t1, t2;
+      rpy_real(ew, rr, t1, t2);
+      acc[0] += t1 + t2 * dx * dx / rr;
+      acc[1] += t2 * dx * dy / rr;
+      acc[2] += t2 * dx * dz / rr;
+      acc[3] += t1 + t2 * dy * dy / rr;
+      acc[4] += t2 * dy * dz / rr;
+      acc[5] += t1 + t2 * dz * dz / rr;
+    }
+  }
+  for (int c = lane; c < ew.nk; c += 32) {
+    const double* kv = kvec + 9 * c;
+    double ck = cos(kv[0] * dxo + kv[1] * dyo + kv[2] * dzo);
+    acc[0] += kv[3] * ck;
+    acc[1] += kv[4] * ck;
+    acc[2] += kv[5] * ck;
+    acc[3] += kv[6] * ck;
+    acc[4] += kv[7] * ck;
+    acc[5] += kv[8] * ck;
+  }
+  for (int a = 0; a < 6; a++)
+    for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
+  if (lane == 0) {
+    int I = i >> 5, J = j >> 5;
+    double* tb = Mt + (tile_off(I, NT) + (J - I)) * 6144;
+    int e = (i & 31) * 32 + (j & 31);
+    for (int a = 0; a < 6; a++) tb[a * 1024 + e] = acc[a];
+  }
+}
+
+// Input vector with component pointers and stride: x_c(i) = p[c][i*stride].
+struct VecIn {
+  const double* p[3];
+  int stride;
+};
+
+__device__ __forceinline__ double vin(const VecIn& v, int c, int i) {
+  return v.p[c][(size_t)i * v.stride];
+}
+
+// Partial products of one packed tile with two right-hand sides.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sym_matvec2(const T* __restrict__ Mt,
+                                                     const int* __restrict__ tileI, int NT, int N,
+                                                     VecIn v0, VecIn v1, double* rowpart,
+                                                     double* colpart) {
+  long long tile = blockIdx.x;
+  int I = tileI[tile];
+  int J = I + (int)(tile - tile_off(I, NT));
+  __shared__ double xI[2][3][32], xJ[2][3][32], racc[2][3][32];
+  __shared__ double cacc[8][6][32];
+  int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid < 192) {
+    int r = tid / 96, c = (tid / 32) % 3, k = tid & 31;
+    int i = I * 32 + k, j = J * 32 + k;
+    const VecIn& v = r ? v1 : v0;
+    xI[r][c][k] = i < N ? vin(v, c, i) : 0.0;
+    xJ[r][c][k] = j < N ? vin(v, c, j) : 0.0;
+  }
+  const T* tb = Mt + tile * 6144;
+  double m[4][6];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    int il = w + 8 * q;
+#pragma unroll
+    for (int a = 0; a < 6; a++) m[q][a] = (double)tb[a * 1024 + il * 32 + lane];
+  }
+  __syncthreads();
+  double cs[2][3] = {{0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    int il = w + 8 * q;
+    bool valid = (I != J) || (il < lane);
+    double m0 = valid ? m[q][0] : 0.0, m1 = valid ? m[q][1] : 0.0, m2 = valid ? m[q][2] : 0.0;
+    double m3 = valid ? m[q][3] : 0.0, m4 = valid ? m[q][4] : 0.0, m5 = valid ? m[q][5] : 0.0;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      double x0 = xJ[r][0][lane], x1 = xJ[r][1][lane], x2 = xJ[r][2][lane];
+      double ra = m0 * x0 + m1 * x1 + m2 * x2;
+      double rb = m1 * x0 + m3 * x1 + m4 * x2;
+      double rc = m2 * x0 + m4 * x1 + m5 * x2;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ra += __shfl_xor_sync(0xffffffffu, ra, o);
+        rb += __shfl_xor_sync(0xffffffffu, rb, o);
+        rc += __shfl_xor_sync(0xffffffffu, rc, o);
+      }
+      if (lane == 0) {
+        racc[r][0][il] = ra;
+        racc[r][1][il] = rb;
+        racc[r][2][il] = rc;
+      }
+      double y0 = xI[r][0][il], y1 = xI[r][1][il], y2 = xI[r][2][il];
+      cs[r][0] += m0 * y0 + m1 * y1 + m2 * y2;
+      cs[r][1] += m1 * y0 + m3 * y1 + m4 * y2;
+      cs[r][2] += m2 * y0 + m4 * y1 + m5 * y2;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2; r++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) cacc[w][r * 3 + a][lane] = cs[r][a];
+  __syncthreads();
+  if (tid < 192) {
+    int ra = tid / 32, k = tid & 31;
+    double s = 0;
+#pragma unroll
+    for (int ww = 0; ww < 8; ww++) s += cacc[ww][ra][k];
+    colpart[tile * 192 + tid] = s;
+    rowpart[tile * 192 + tid] = racc[ra / 3][ra % 3][k];
+  }
+}
+
+// First reduction level: block (K, s) sums its share of the row partials of
+// tiles (K, J >= K) and the column partials of tiles (I <= K, K).
+__global__ void k_matvec_reduce1(const double* __restrict__ rowpart,
+                                 const double* __restrict__ colpart, int NT, double* part) {
+  int K = blockIdx.x, s = blockIdx.y, e = threadIdx.x;  // e < 192
+  double acc = 0;
+  for (int J = K + s; J < NT; J += kRedSplit) acc += rowpart[(tile_off(K, NT) + (J - K)) * 192 + e];
+  for (int I = s; I <= K; I += kRedSplit) acc += colpart[(tile_off(I, NT) + (K - I)) * 192 + e];
+  part[((size_t)K * kRedSplit + s) * 192 + e] = acc;
+}
+
+// Second level: Y[r][a][K*32+k] = sum over splits.
+__global__ void k_matvec_reduce2(const double* __restrict__ part, int NT, double* Y0, double* Y1) {
+  int K = blockIdx.x, e = threadIdx.x;
+  double acc = 0;
+  for (int s = 0; s < kRedSplit; s++) acc += part[((size_t)K * kRedSplit + s) * 192 + e];
+  int r = e / 96, a = (e / 32) % 3, k = e & 31;
+  double* Y = r ? Y1 : Y0;
+  Y[(size_t)a * NT * 32 + K * 32 + k] = acc;
+}
+
+// TEA displacement and position update (updateHI, shear/src/main26.c:787-855;
+// extensional/src/main14.c:825-893).  U = sum_{j != i} M_ij F_j and
+// W = sum_{j != i} M_ij R_j; the diagonal block contributes
+// Dtr_a (F_a + p C_a R_a), beta applying only off the diagonal.
+__global__ void k_tea_update(int flow, double* rx, double* ry, double* rz, double* dxv,
+                             double* dyv, double* dzv, const double* __restrict__ fx,
+                             const double* __restrict__ fy, const double* __restrict__ fz,
+                             const double* __restrict__ R, const double* __restrict__ U,
+                             const double* __restrict__ W, int NTp, const double* __restrict__ Ct,
+                             int Nb, int N, double dt, double edot, double p, double bt,
+                             double D0, double D1, double D2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int b = i % Nb;
+  double F[3] = {fx[i], fy[i], fz[i]};
+  double Dg[3] = {D0, D1, D2};
+  double du[3];
+  for (int a = 0; a < 3; a++) {
+    double C = Ct[3 * b + a];
+    double Ra = R[3 * i + a];
+    du[a] = dt * (U[(size_t)a * NTp + i] + p * bt * C * W[(size_t)a * NTp + i]) +
+            dt * (Dg[a] * (F[a] + p * C * Ra));
+  }
+  if (flow == 0) {
+    du[0] += dt * edot * ry[i];
+  } else {
+    du[0] += dt * edot * rx[i];
+    du[1] -= dt * edot * ry[i];
+  }
+  dxv[i] += du[0];
+  rx[i] += du[0];
+  dyv[i] += du[1];
+  ry[i] += du[1];
+  dzv[i] += du[2];
+  rz[i] += du[2];
+}
+
+namespace bd {
+
+int alloc_mobility(bd_ctx* c) {
+  int N = c->N;
+  c->NT = (N + 31) / 32;
+  c->ntiles = (size_t)c->NT * (c->NT + 1) / 2;
+  size_t gsz = (size_t)c->p.nt_avg * c->nbins * 6;
+  CU(cudaMalloc(&c->grid, 8 * gsz));
+  CU(cudaMemsetAsync(c->grid, 0, 8 * gsz, c->stream));
+  CU(cudaMalloc(&c->Ctab, 8 * (size_t)(c->sbins + 1) * 3 * c->Nb));
+  CU(cudaMemsetAsync(c->Ctab, 0, 8 * (size_t)(c->sbins + 1) * 3 * c->Nb, c->stream));
+  c->bytes += 8 * gsz + 8 * (size_t)(c->sbins + 1) * 3 * c->Nb;
+  return BD_OK;
+}
+
+// Tile storage, tile-row table, near-pair list and matvec scratch are
+// allocated on the first mobility build (they are O(N^2)).
+static int ensure_tiles(bd_ctx* c) {
+  if (c->Mt) return BD_OK;
+  size_t nt = c->ntiles;
+  if (cudaMalloc(&c->Mt, 8 * nt * 6144) != cudaSuccess) return BD_ERR_OOM;
+  std::vector<int> ti(nt);
+  size_t k = 0;
+  for (int I = 0; I < c->NT; I++)
+    for (int J = I; J < c->NT; J++) ti[k++] = I;
+  CU(cudaMalloc(&c->tileI, 4 * nt));
+  CU(cudaMemcpy(c->tileI, ti.data(), 4 * nt, cudaMemcpyHostToDevice));
+  long long N = c->N;
+  c->near_cap = std::min<long long>(N * (N - 1) / 2 + 1, 512 * N);
+  CU(cudaMalloc(&c->near_pairs, 8 * c->near_cap));
+  CU(cudaMalloc(&c->near_count, 16));
+  CU(cudaMalloc(&c->rowpart, 8 * nt * 192));
+  CU(cudaMalloc(&c->colpart, 8 * nt * 192 + 8 * (size_t)c->NT * kRedSplit * 192));
+  CU(cudaMalloc(&c->U, 8 * 3 * (size_t)c->NT * 32));
+  CU(cudaMalloc(&c->W, 8 * 3 * (size_t)c->NT * 32));
+  c->bytes += 8 * nt * 6144 + 4 * nt + 8 * c->near_cap + 16 + 16 * nt * 192 +
+              8 * (size_t)c->NT * kRedSplit * 192 + 48 * (size_t)c->NT * 32;
+  return BD_OK;
+}
+
+// Ewald parameters, k-vector list with coefficients M2, and the self term Dtr
+// of calcHI (shear/src/main26.c:1536-1686; ext k-vectors of the rotated
+// reciprocal lattice, extensional/src/main14.c:1582-1588), generated with
+// the reference's loop structure and arithmetic.
+static void hi_setup(bd_ctx* c, const Lat& l, Ewald* ew, std::vector<double>* kv, double Dtr[3]) {
+  double L = l.L, boxvol = c->boxvol;
+  int treal = l.treal, tp = c->tp, nmax;
+  double rce, M_HI = 4.0;
+  if (treal <= tp / 2) {
+    rce = 1.0 * l.L2yp;
+    nmax = 1;
+  } else {
+    rce = 2.0 * l.L2yp;
+    nmax = 2;
+  }
+  double tf = (double)treal / tp;
+  int nt = (int)round(tf * c->p.nt_avg) % c->p.nt_avg;
+  double alpha = M_HI / rce, rkcut = 2.0 * M_HI * M_HI / rce;
+  double rkkcut = rkcut * rkcut, rtpi = sqrt(M_PI);
+  double alpha2 = alpha * alpha, alpha3 = alpha2 * alpha, alpha4 = alpha2 * alpha2;
+  double alpha5 = alpha4 * alpha, alpha7 = alpha4 * alpha2 * alpha;
+  double selfconst = 1 - 6 / rtpi * alpha + 40 / (3 * rtpi) * alpha3;
+  double L1[2] = {l.L1x, l.L1y}, L2[2] = {l.L2x, l.L2y};
+  int kxmax = ceil(rkcut * l.detL / (M_PI * 2.0 * L * L2[1]));
+  int kymax = ceil(rkcut * l.detL / (M_PI * 2.0 * L * L1[0]));
+  int kzmax = ceil(rkcut * L / (M_PI * 2.0));
+  int nyw = 2 * kymax + 1;
+  std::vector<int> kyup(kxmax + 2, 0), kylo(kxmax + 2, 0);
+  std::vector<int> kzup((size_t)(kxmax + 2) * nyw, 0), kzlo((size_t)(kxmax + 2) * nyw, 0);
+  double kcoeff = (l.flow == 0) ? M_PI * 2.0 : M_PI * 2.0 / l.detL;
+  auto kvec2 = [&](int kx, int ky, double& rkx, double& rky) {
+    if (l.flow == 0) {
+      rky = kcoeff * (kx - ky * (L2[0] / L1[0])) / L2[1];
+      rkx = kcoeff * ky / L1[0];
+    } else {
+      rkx = kcoeff * L * (kx * L2[1] - ky * L1[1]);
+      rky = kcoeff * L * (-kx * L2[0] + ky * L1[0]);
+    }
+  };
+  for (int kx = 0; kx < kxmax + 1; kx++) {
+    int ylo = 0, yup = 0;
+    for (int ky = -kymax; ky < kymax + 1; ky++) {
+      double rkx, rky;
+      kvec2(kx, ky, rkx, rky);
+      double rkxy = rkx * rkx + rky * rky;
+      int zlo = 0, zup = 0;
+      for (int kz = -kzmax; kz < kzmax + 1; kz++) {
+        double rkz = kz * M_PI * 2.0 / L, rkk = rkxy + rkz * rkz;
+        if (rkk < rkkcut && zlo == 0) {
+          kzlo[nyw * kx + ky + kymax] = kz;
+          zlo = 1;
+        }
+        if (rkk > rkkcut && zlo == 1 && zup == 0) {
+          kzup[nyw * kx + ky + kymax] = kz - 1;
+          zup = 1;
+        }
+      }
+      if (rkxy < rkkcut && ylo == 0) {
+        kylo[kx] = ky;
+        ylo = 1;
+      }
+      if (rkxy > rkkcut && ylo == 1 && yup == 0) {
+        kyup[kx] = ky - 1;
+        yup = 1;
+      }
+    }
+  }
+  {
+    // same scan as the reference; the arrays carry one spare zero row so the
+    // scan and the kxmax increment below stay inside them
+    int kx = 0, rows = kxmax + 2;
+    while (kx < rows && kyup[kx] != -kymax &&
+           kx <= (int)(rkcut * l.detL / (M_PI * 2.0 * L * l.L2yp))) {
+      kxmax = kx;
+      kx++;
+    }
+  }
+  kxmax++;
+  kv->clear();
+  for (int kx = 0; kx < kxmax + 1 && kx < (int)kylo.size(); kx++)
+    for (int ky = kylo[kx]; ky < kyup[kx] + 1; ky++) {
+      double rkx, rky;
+      kvec2(kx, ky, rkx, rky);
+      double rkxy = rkx * rkx + rky * rky;
+      for (int kz = kzlo[nyw * kx + ky + kymax]; kz < kzup[nyw * kx + ky + kymax] + 1; kz++) {
+        double rkz = kz * M_PI * 2.0 / L, rkk = rkxy + rkz * rkz;
+        double m2 = 2.0 * (1.0 - rkk / 3.0) * (1.0 + rkk / (4.0 * alpha2) + rkk * rkk / (8.0 * alpha4)) * 6.0 * M_PI / rkk * exp(-rkk / (4.0 * alpha2));
+        double row[9] = {rkx,
+                         rky,
+                         rkz,
+                         m2 * (1 - rkx * rkx / rkk) / boxvol,
+                         m2 * (-rkx * rky / rkk) / boxvol,
+                         m2 * (-rkx * rkz / rkk) / boxvol,
+                         m2 * (1 - rky * rky / rkk) / boxvol,
+                         m2 * (-rky * rkz / rkk) / boxvol,
+                         m2 * (1 - rkz * rkz / rkk) / boxvol};
+        kv->insert(kv->end(), row, row + 9);
+      }
+    }
+  {
+    int cnt = 0;
+    for (int ky = kylo[0]; ky < kyup[0] + 1; ky++)
+      for (int kz = kzlo[ky + kymax]; kz < kzup[ky + kymax] + 1; kz++) {
+        for (int a = 3; a < 9; a++) (*kv)[9 * cnt + a] /= 2.0;
+        if (ky == 0 && kz == 0)
+          for (int a = 3; a < 9; a++) (*kv)[9 * cnt + a] = 0.0;
+        cnt++;
+      }
+  }
+  int nk = (int)(kv->size() / 9);
+  Dtr[0] = Dtr[1] = Dtr[2] = selfconst;
+  for (int k = 0; k < nk; k++) {
+    Dtr[0] += (*kv)[9 * k + 3];
+    Dtr[1] += (*kv)[9 * k + 6];
+    Dtr[2] += (*kv)[9 * k + 8];
+  }
+  // self images with all three indices non-zero, yy projection added to zz
+  // (shear/src/main26.c:1667-1686)
+  for (int nx = -nmax; nx < nmax + 1; nx++)
+    for (int ny = -nmax; ny < nmax + 1; ny++)
+      for (int nz = -nmax; nz < nmax + 1; nz++)
+        if (nx != 0 && ny != 0 && nz != 0) {
+          double dx = nx * L1[0] + ny * L2[0], dy = nx * L1[1] + ny * L2[1], dz = nz * L;
+          double rr = dx * dx + dy * dy + dz * dz, r = sqrt(rr);
+          double C1 = 0.75 / r + 0.5 / (r * rr);
+          double C2 = 4.0 * alpha7 * rr * rr + 3.0 * alpha3 * rr - 20.0 * alpha5 * rr - 4.5 * alpha + 14.0 * alpha3 + alpha / rr;
+          double C3 = 0.75 / r - 1.5 / (r * rr);
+          double C4 = -4.0 * alpha7 * rr * rr - 3.0 * alpha3 * rr + 16.0 * alpha5 * rr + 1.5 * alpha - 2.0 * alpha3 - 3.0 * alpha / rr;
+          double t1 = C1 * erfc(alpha * r) + C2 * exp(-alpha2 * rr) / rtpi;
+          double t2 = C3 * erfc(alpha * r) + C4 * exp(-alpha2 * rr) / rtpi;
+          Dtr[0] += t1 + t2 * dx * dx / rr;
+          Dtr[1] += t1 + t2 * dy * dy / rr;
+          Dtr[2] += t1 + t2 * dy * dy / rr;
+        }
+  ew->alpha = alpha;
+  ew->alpha2 = alpha2;
+  ew->alpha3 = alpha3;
+  ew->alpha5 = alpha5;
+  ew->alpha7 = alpha7;
+  ew->rce = rce;
+  ew->rtpi = rtpi;
+  ew->nmax = nmax;
+  ew->nt = nt;
+  ew->nk = nk;
+}
+
+static Lat step_lat(bd_ctx* c) {
+  Lat l = c->lat;
+  int treal = (int)(c->t % (unsigned long)c->tp);
+  l.treal = treal;
+  l.nmax = (treal <= c->tp / 2) ? 1 : 2;
+  l.delx = c->p.edot * treal * c->p.dt;
+  return l;
+}
+
+int calc_hi(bd_ctx* c) {
+  int s;
+  if ((s = ensure_tiles(c)) != BD_OK) return s;
+  Lat l = step_lat(c);
+  Ewald ew;
+  std::vector<double> kv;
+  hi_setup(c, l, &ew, &kv, c->Dtr);
+  if ((int)kv.size() / 9 > c->kvec_cap) {
+    if (c->kvec) cudaFree(c->kvec);
+    c->kvec_cap = (int)kv.size() / 9 + 64;
+    CU(cudaMalloc(&c->kvec, 8 * 9 * (size_t)c->kvec_cap));
+  }
+  c->nk = ew.nk;
+  if (!kv.empty())
+    CU(cudaMemcpyAsync(c->kvec, kv.data(), 8 * kv.size(), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaMemsetAsync(c->near_count, 0, 4, c->stream));
+  k_hi_far<<<(unsigned)c->ntiles, 256, 0, c->stream>>>(
+      l, ew, c->rx, c->ry, c->rz, c->N, c->NT, c->tileI, c->grid, c->nbx, c->nby, c->nbz, c->nhx,
+      c->nhy, c->nhz, c->bsx, c->bsy, c->bsz, c->nbins, c->Mt, (int2*)c->near_pairs,
+      c->near_count, (long long)c->near_cap, c->err);
+  k_hi_near<<<148 * 8, 256, 0, c->stream>>>(l, ew, c->rx, c->ry, c->rz, c->NT,
+                                                     (const int2*)c->near_pairs, c->near_count,
+                                                     (long long)c->near_cap, c->kvec, c->Mt);
+  c->hi_built = true;
+  return launch_ok(c);
+}
+
+// y0 = M_off v0, y1 = M_off v1 over the packed tiles (off-diagonal blocks).
+static int sym_matvec2(bd_ctx* c, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1) {
+  k_sym_matvec2<double><<<(unsigned)c->ntiles, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N,
+                                                                     v0, v1, c->rowpart,
+                                                                     c->colpart);
+  double* part = c->colpart + c->ntiles * 192;
+  k_matvec_reduce1<<<dim3(c->NT, kRedSplit), 192, 0, c->stream>>>(c->rowpart, c->colpart, c->NT,
+                                                                  part);
+  k_matvec_reduce2<<<c->NT, 192, 0, c->stream>>>(part, c->NT, Y0, Y1);
+  return launch_ok(c);
+}
+
+int update_hi(bd_ctx* c) {
+  int s;
+  if (c->t % (unsigned long)c->srpy == 0 || c->t == c->tstart) {
+    if ((s = calc_hi(c)) != BD_OK) return s;
+    int sb = (int)floor(c->strain / c->strain_interval);
+    if (sb > c->sbins) sb = c->sbins;
+    if (sb < 0) sb = 0;
+    c->sbin = sb;
+    c->bt = c->btab[sb];
+  }
+  if (!c->hi_built) return BD_ERR_STATE;
+  if (c->p.flow == BD_FLOW_EXT) rotate_coords(c, 1);
+  VecIn vf = {{c->fx, c->fy, c->fz}, 1};
+  VecIn vr = {{c->R, c->R + 1, c->R + 2}, 3};
+  if ((s = sym_matvec2(c, vf, vr, c->U, c->W)) != BD_OK) return s;
+  double p = sqrt(2.0 / c->p.dt);
+  k_tea_update<<<(c->N + 255) / 256, 256, 0, c->stream>>>(
+      c->p.flow, c->rx, c->ry, c->rz, c->dxv, c->dyv, c->dzv, c->fx, c->fy, c->fz, c->R, c->U,
+      c->W, c->NT * 32, c->Ctab + (size_t)c->sbin * 3 * c->Nb, c->Nb, c->N, c->p.dt, c->p.edot,
+      p, c->bt, c->Dtr[0], c->Dtr[1], c->Dtr[2]);
+  return launch_ok(c);
+}
+
+int download_mobility(bd_ctx* c, double* M9) {
+  if (!c->hi_built) return BD_ERR_STATE;
+  int N = c->N, NT = c->NT;
+  std::vector<double> h(c->ntiles * 6144);
+  CU(cudaMemcpyAsync(h.data(), c->Mt, 8 * h.size(), cudaMemcpyDeviceToHost, c->stream));
+  int s = check(c);
+  if (s) return s;
+  memset(M9, 0, sizeof(double) * 9 * (size_t)N * N);
+  static const int comp[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+  size_t t = 0;
+  for (int I = 0; I < NT; I++)
+    for (int J = I; J < NT; J++, t++) {
+      const double* tb = h.data() + t * 6144;
+      for (int il = 0; il < 32; il++)
+        for (int jl = 0; jl < 32; jl++) {
+          int i = I * 32 + il, j = J * 32 + jl;
+          if (i >= j || j >= N) continue;
+          double* blk = M9 + (size_t)9 * N * i + 9 * (size_t)j;
+          for (int a = 0; a < 9; a++) blk[a] = tb[comp[a] * 1024 + il * 32 + jl];
+        }
+    }
+  for (int i = 0; i < N; i++) {
+    double* blk = M9 + (size_t)9 * N * i + 9 * (size_t)i;
+    blk[0] = c->Dtr[0];
+    blk[4] = c->Dtr[1];
+    blk[8] = c->Dtr[2];
+  }
+  return BD_OK;
+}
+
+}  // namespace bd
+
+extern "C" int bd_load_grid(bd_ctx* c, int nt, const double* D9) {
+  if (!c || !D9 || nt < 0 || nt >= c->p.nt_avg) return BD_ERR_ARG;
+  std::vector<double> g((size_t)c->nbins * 6);
+  for (int b = 0; b < c->nbins; b++) {
+    const double* d = D9 + 9 * (size_t)b;
+    if (d[1] != d[3] || d[2] != d[6] || d[5] != d[7]) return BD_ERR_ASYMMETRIC;
+    double* o = g.data() + 6 * (size_t)b;
+    o[0] = d[0];
+    o[1] = d[1];
+    o[2] = d[2];
+    o[3] = d[4];
+    o[4] = d[5];
+    o[5] = d[8];
+  }
+  CU(cudaMemcpyAsync(c->grid + (size_t)nt * c->nbins * 6, g.data(), 8 * g.size(),
+                     cudaMemcpyHostToDevice, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return BD_OK;
+}
