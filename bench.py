@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the Brownian-dynamics step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1|c0]
+
+A "step" is one pass of the hydrodynamic step loop over the whole system:
+lattice update, periodic wrap, neighbour check (and rebuild when due),
+spring + excluded-volume + screened-Coulomb forces, Brownian noise,
+mobility rebuild every srpy=100 steps, Brownian displacement, and a
+charge-hop sweep every MStep=100 steps.  The metric is bead-steps/s,
+whole-job (sum over GPUs).
+
+Default workload (c1): planar extension with Kraynik-Reinelt boundaries,
+80 chains x 100 beads (8000 beads), box 60a, Wi = 2, dt = 5e-4, FENE k=30
+Q0=3, WCA, 50% charged, charge hop every 100 steps.  Inputs are seeded
+synthetic chains.  The path timed is the reference-mode step (dense hybrid
+Rotne-Prager-Yamakawa mobility + conformationally averaged TEA noise) with
+Philox Gaussians.
+
+--impl reference times the reference's own CPU code (compiled from its sources
+into oracle/_ref/) on this host's cores for the same workload.
+
+One process per GPU (torchrun for N > 1); the path does not shard, so each
+rank advances its own independent replica ("replicas only"); timing is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "smdlt-ca-chrg-flow_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "bead-steps/s on 1 B200 at 1e-6 Lanczos tol: learned-precond FP32 vs plain FP64"
+
+# Relaxation time for Wi = edot * tau: the reference's notebooks quote
+# tau = 175 for 50-bead chains; Zimm scaling tau ~ Nb^(3 nu), nu = 0.588.
+def tau_estimate(Nb):
+    return 175.0 * (Nb / 50.0) ** (3 * 0.588)
+
+
+WORKLOADS = {
+    "c1": dict(name="ext KRBC 80x100 beads (8000), box 60, Wi 2, 50% charged, hop/100 steps",
+               flow=1, Nb=100, Nc=80, L=60.0, Wi=2.0, dt=5e-4, frac=0.5),
+    # half of c1 at the same density, for profiling captures
+    "c1s": dict(name="ext KRBC 40x100 beads (4000), box 47.6, Wi 2, 50% charged, hop/100 steps",
+                flow=1, Nb=100, Nc=40, L=60.0 * 0.5 ** (1 / 3), Wi=2.0, dt=5e-4, frac=0.5),
+    # the shear tree forces kappas = 200 (shear/src/main26.c:544); its own
+    # Input.txt pairs that with a Hookean spring of rest length 2 and eps = 0.1
+    "c0": dict(name="shear LE 20x25 beads (500), box 30, Wi 1, 50% charged, hop/100 steps",
+               flow=0, Nb=25, Nc=20, L=30.0, Wi=1.0, dt=5e-4, frac=0.5,
+               force=dict(spring="Hookean", kappas=200.0, qmax=2.0, epsilon=0.1)),
+}
+COMMON = dict(spring="FENE", kappas=30.0, qmax=3.0, epsilon=1.0, lambda_b=2.0, lambda_d=5.0,
+              barrier=3.0, barrier2=3.0, MStep=100, nt_avg=8, bin_size=2.0, srpy=100)
+
+
+def force_params(w):
+    kw = dict(COMMON)
+    kw.update(w.get("force", {}))
+    return kw
+
+
+def edot_of(w):
+    return w["Wi"] / tau_estimate(w["Nb"])
+
+
+def synth_inputs(w, seed):
+    """Seeded chains, charges, far-field table and TEA parameters."""
+    import bd_b200 as B
+    x, y, z = B.random_chains(w["Nb"], w["Nc"], w["L"], seed, bond=2.0, min_sep=1.8)
+    x, y = B.lab_frame(w["flow"], x, y)
+    q = B.random_charges(w["Nb"], w["Nc"], w["frac"], seed + 1)
+    r = np.random.default_rng(seed + 2)
+    beta = r.uniform(0.3, 0.6, 21)
+    C = r.uniform(0.8, 1.0, (21, 3 * w["Nb"]))
+    return x, y, z, q, beta, C
+
+
+def grid_table(nt_avg, nbins, seed):
+    g = np.random.default_rng(seed).normal(scale=1e-3, size=(nt_avg, nbins, 3, 3))
+    g = 0.5 * (g + np.swapaxes(g, -1, -2))
+    return np.ascontiguousarray(g.reshape(nt_avg, nbins * 9))
+
+
+# ---------------------------------------------------------------------------
+# the reference on the host cores
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def time_reference(w, steps, warmup, threads):
+    """Per-step wall time of the reference's own routines (oracle/_ref) on the
+    workload: plain steps at full size, plus the amortised mobility rebuild
+    (timed once at full size) and charge-hop sweep.  The reference's sweep is
+    O(Ncharges N^2) (~10 min at 8000 beads), so it is timed on a system with
+    the same density, chain length and charge fraction but 1/8 of the beads
+    and scaled by N^3 (labelled in the sample string)."""
+    import oracle as O
+    if not O.ref_available(w["flow"]):
+        return None
+    edot = edot_of(w)
+    N = w["Nb"] * w["Nc"]
+    x, y, z, q, beta, C = synth_inputs(w, 1234)
+    kw = force_params(w)
+    kw.pop("srpy")
+    ref = O.RefSim(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
+                   threads=threads, **kw)
+    nbins = int(ref.bins()[6])
+    G = grid_table(COMMON["nt_avg"], nbins, 7)
+    for nt in range(COMMON["nt_avg"]):
+        ref.set_grid(nt, np.ascontiguousarray(G[nt]))
+    for sb in range(21):
+        ref.set_tea(sb, float(beta[sb]), np.ascontiguousarray(C[sb]))
+    ref.set_pos(x, y, z)
+    ref.set_charges(q, len(q))
+    ref.set_tstart(0)
+    ref.begin_iteration()
+    ref.step_hi(0, 0)  # t == tstart: builds M
+    for t in range(1, 1 + warmup):
+        ref.step_hi(t, 1)
+    t0 = ref.wtime()
+    for t in range(1 + warmup, 1 + warmup + steps):
+        ref.step_hi(t, 1)
+    t_plain = (ref.wtime() - t0) / steps
+    t0 = ref.wtime()
+    ref.calc_hi()
+    t_hi = ref.wtime() - t0
+    # charge-hop sweep on the 1/8 system (same density: box edge halved)
+    ws = dict(w, Nc=max(1, w["Nc"] // 8), L=w["L"] / 2)
+    xs, ys, zs, qs, _, _ = synth_inputs(ws, 99)
+    Ns = ws["Nb"] * ws["Nc"]
+    del ref
+    refs = O.RefSim(w["flow"], ws["Nb"], ws["Nc"], ws["L"], edot, w["dt"], Ncharges=len(qs),
+                    threads=threads, **kw)
+    refs.set_pos(xs, ys, zs)
+    refs.set_charges(qs, len(qs))
+    refs.update_lattice(0)
+    refs.set_t(0)
+    if w["flow"] == 1:
+        refs.transform()
+    refs.apply_pbc()
+    t0 = refs.wtime()
+    refs.charge_hop()
+    t_sweep_s = refs.wtime() - t0
+    t_sweep = t_sweep_s * (N / Ns) ** 3
+    per_step = t_plain + t_hi / COMMON["srpy"] + t_sweep / COMMON["MStep"]
+    sample = (f"reference routines on {threads} host threads: {steps} full-size steps "
+              f"({t_plain*1e3:.1f} ms each) + mobility rebuild at full size "
+              f"({t_hi:.2f} s, amortised over {COMMON['srpy']} steps) + one charge-hop sweep "
+              f"timed at {Ns} beads ({t_sweep_s:.2f} s) scaled by (N/{Ns})^3 to "
+              f"{t_sweep:.0f} s, amortised over {COMMON['MStep']} steps")
+    return dict(per_step=per_step, value=N / per_step, sample=sample, threads=threads,
+                components={"plain_step_s": t_plain, "mobility_build_s": t_hi,
+                            "hop_sweep_s_scaled": t_sweep, "hop_sweep_s_sampled": t_sweep_s,
+                            "hop_sample_beads": Ns})
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out = ""
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in (self.out or "").splitlines():
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our path
+
+
+def build_context(w, seed, device_noise="philox"):
+    import bd_b200 as B
+    edot = edot_of(w)
+    x, y, z, q, beta, C = synth_inputs(w, seed)
+    p = B.make_params(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
+                      noise=device_noise, philox_seed=seed, **force_params(w))
+    c = B.Context(p)
+    nbins = int(c.grid_shape()[6])
+    G = grid_table(COMMON["nt_avg"], nbins, 7)
+    for nt in range(COMMON["nt_avg"]):
+        c.load_grid(nt, G[nt])
+    for sb in range(21):
+        c.set_tea(sb, beta[sb], C[sb])
+    c.set_positions(x, y, z)
+    c.set_charges(q)
+    c.set_time(0, 0)
+    c.update_lattice(0)
+    c.transform_coords()
+    c.apply_pbc()
+    c.build_neighbors()
+    c.inverse_coords()
+    return c
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    w = WORKLOADS[args.workload]
+    N = w["Nb"] * w["Nc"]
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    c = build_context(w, 1000 + rank)
+    K, W = args.steps, args.warmup
+    c.step_reference(0, W, True)
+    c.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    c.profile(True)
+    n0 = c.launches()
+    with ClockSampler(dev) as clk:
+        c.step_reference(W, K, True)
+        c.sync()
+    launches = c.launches() - n0
+    step_ms, _ = c.profile_read(c.PROF_STEP)
+    mv_ms, mv_n = c.profile_read(c.PROF_MATVEC)
+    hi_ms, hi_n = c.profile_read(c.PROF_HI_BUILD)
+    hop_ms, hop_n = c.profile_read(c.PROF_HOP)
+    f_ms, f_n = c.profile_read(c.PROF_FORCES)
+    c.profile(False)
+    t_max = step_ms
+    if dist:
+        tt = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * N * K / (t_max / 1e3)
+
+    # end to end through the C ABI with pinned host buffers: upload the
+    # positions, one step, download the positions, every step
+    Ke = max(1, min(K, args.e2e_steps))
+    hb = [torch.empty(N, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    hx = c.positions()
+    for a, b in zip(hb, hx):
+        a[:] = b
+    c.sync()
+    t0 = time.perf_counter()
+    for t in range(W + K, W + K + Ke):
+        c.set_positions(*hb)
+        c.step_reference(t, 1, True)
+        out = c.positions()
+        for a, b in zip(hb, out):
+            a[:] = b
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": world * N * Ke / e2e_s, "unit": "bead-steps/s",
+           "h2d_bytes_per_step": 3 * 8 * N, "d2h_bytes_per_step": 3 * 8 * N, "steps": Ke}
+
+    # roofline of the dominant kernel: packed symmetric mobility product,
+    # algorithmic bytes = 6 FP64 per off-diagonal block of the upper triangle
+    # + two right-hand sides in and two partial outputs
+    alg_bytes = 48.0 * N * (N - 1) / 2 + 4 * 3 * N * 8
+    avg_ms = mv_ms / max(mv_n, 1)
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    peak, kind = peaks()
+    roof = {"kernel": "k_sym_matvec2<double>", "bound": "hbm", "achieved": achieved,
+            "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+            "launches": mv_n}
+    breakdown = {"matvec_ms": mv_ms, "mobility_build_ms": hi_ms, "mobility_builds": hi_n,
+                 "hop_sweep_ms": hop_ms, "hop_sweeps": hop_n, "forces_ms": f_ms,
+                 "step_total_ms": step_ms}
+    clocks = clk.summary()
+    line = {"metric": METRIC, "value": value, "unit": "bead-steps/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": t_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["name"], "beads": N, "path": "reference mode: dense hybrid "
+                       "RPY mobility (Ewald near field + lookup far field) + CA-TEA noise, "
+                       "Philox Gaussians, sequential charge-hop sweep",
+                       "edot": edot_of(w), "tau_estimate": tau_estimate(w["Nb"]),
+                       "l2": "inputs larger than L2 (packed mobility 1.5 GB)",
+                       "parallelism": "replicas only" if world > 1 else "single GPU"},
+            "roofline": roof, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
+            "breakdown": breakdown}
+    c.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    w = WORKLOADS[args.workload]
+    N = w["Nb"] * w["Nc"]
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        th = host_threads()
+        r = time_reference(w, steps=min(args.steps, 10), warmup=min(args.warmup, 1), threads=th)
+        if r is None:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "reference library oracle/_ref not built here"}))
+            return
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"],
+                "unit": "bead-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["per_step"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": w["name"], "beads": N},
+                "cpu_baseline": {"value": r["value"], "unit": "bead-steps/s", "cores": th,
+                                 "kind": "reference", "sample": r["sample"]},
+                "components": r["components"],
+                "e2e": {"value": r["value"], "unit": "bead-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = run_ours(args, rank, world, dist)
+        if rank == 0 and not args.no_cpu_baseline:
+            r = time_reference(w, steps=5, warmup=1, threads=host_threads())
+            if r is not None:
+                line["cpu_baseline"] = {"value": r["value"], "unit": "bead-steps/s",
+                                        "cores": r["threads"], "kind": "reference",
+                                        "sample": r["sample"]}
+        if rank == 0:
+            print(json.dumps(line))
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -47,6 +47,10 @@ typedef enum {
 } bd_status;
 
 typedef enum { BD_FLOW_SHEAR = 0, BD_FLOW_EXT = 1 } bd_flow;
+/* Brownian noise source for bd_get_noise: the reference's sequential
+ * ran1/gasdev stream (bit-identical, one device thread) or counter-based
+ * Philox4x32-10 Gaussians (parallel; the production source). */
+typedef enum { BD_NOISE_RAN1 = 0, BD_NOISE_PHILOX = 1 } bd_noise;
 typedef enum { BD_SPRING_HOOKEAN = 0, BD_SPRING_FENE = 1 } bd_spring;
 
 /* System parameters.  The names follow the reference's globals
@@ -76,6 +80,8 @@ typedef struct {
   double strain_ss;          /* CA-TEA steady-state strain; 0 -> 10 */
   int max_neighbors;         /* neighbour-row cap; 0 -> 256 */
   long seed;                 /* ran1 seed (fixSeed=1: 830062920 shear, 981272199 ext) */
+  int noise;                 /* bd_noise */
+  unsigned long long philox_seed;
 } bd_params;
 
 typedef struct bd_ctx bd_ctx;
@@ -155,6 +161,22 @@ int bd_charge_hop(bd_ctx *ctx);                        /* [chargeHop] main26.c:1
 /* Per-charge outcome of the last sweep: (0 skipped,1 accepted,2 rejected),
  * target bead, move kind; 3 ints per charge. */
 int bd_download_hop_log(bd_ctx *ctx, int *log3);
+
+/* ---- measurement -----------------------------------------------------
+ * Device time of selected kernels, measured with CUDA events recorded on
+ * the context's stream around each launch while profiling is enabled. */
+enum {
+  BD_PROF_MATVEC = 0,   /* packed symmetric mobility product (2 right-hand sides) */
+  BD_PROF_HI_BUILD = 1, /* mobility build (far + near passes) */
+  BD_PROF_HOP = 2,      /* charge-hop sweep kernel */
+  BD_PROF_FORCES = 3,   /* bond + excluded-volume + electrostatic kernels */
+  BD_PROF_STEP = 4,     /* one whole bd_step_reference call */
+  BD_PROF_SLOTS = 8
+};
+int bd_profile_enable(bd_ctx *ctx, int on); /* clears the accumulated events */
+int bd_profile_read(bd_ctx *ctx, int slot, double *total_ms, long *count);
+/* Number of kernels the library has launched on this context. */
+long long bd_launch_count(const bd_ctx *ctx);
 
 /* One reference-mode hydrodynamic step (the body of the step loop,
  * shear/src/main26.c:65-151, extensional/src/main14.c:68-171, without file

@@ -30,6 +30,7 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 FLOW_SHEAR, FLOW_EXT = 0, 1
+NOISE_RAN1, NOISE_PHILOX = 0, 1
 SPRING_HOOKEAN, SPRING_FENE = 0, 1
 
 
@@ -61,6 +62,7 @@ class Params(C.Structure):
         ("barrier", C.c_double), ("barrier2", C.c_double), ("MStep", C.c_int),
         ("nt_avg", C.c_int), ("bin_size", C.c_double), ("srpy", C.c_int), ("sbins", C.c_int),
         ("strain_ss", C.c_double), ("max_neighbors", C.c_int), ("seed", C.c_long),
+        ("noise", C.c_int), ("philox_seed", C.c_ulonglong),
     ]
 
 
@@ -117,6 +119,10 @@ def _lib() -> C.CDLL:
         L.bd_download_mobility.argtypes = [vp, _dp]
         L.bd_download_hop_log.argtypes = [vp, _ip]
         L.bd_step_reference.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
+        L.bd_profile_enable.argtypes = [vp, C.c_int]
+        L.bd_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+        L.bd_launch_count.argtypes = [vp]
+        L.bd_launch_count.restype = C.c_longlong
         _LIB = L
     return _LIB
 
@@ -136,7 +142,8 @@ def _chk(status: int, where: str) -> None:
 def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3.0, kappab=0.0,
                 epsilon=1.0, lambda_b=2.0, lambda_d=5.0, Ncharges=0, barrier=3.0, barrier2=3.0,
                 MStep=100, nt_avg=8, bin_size=2.0, srpy=100, sbins=20, strain_ss=10.0,
-                max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0) -> Params:
+                max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0,
+                noise="ran1", philox_seed=20261203) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
     p.box_volume = box_volume
@@ -148,6 +155,8 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
     p.nt_avg, p.bin_size, p.srpy, p.sbins, p.strain_ss = nt_avg, bin_size, srpy, sbins, strain_ss
     p.max_neighbors = max_neighbors
     p.seed = (830062920 if flow == FLOW_SHEAR else 981272199) if seed is None else seed
+    p.noise = NOISE_PHILOX if noise == "philox" else NOISE_RAN1
+    p.philox_seed = philox_seed
     return p
 
 
@@ -286,6 +295,19 @@ class Context:
     def sync(self):
         self._call("bd_sync")
 
+    PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP = 0, 1, 2, 3, 4
+
+    def profile(self, on=True):
+        self._call("bd_profile_enable", int(bool(on)))
+
+    def profile_read(self, slot):
+        ms, n = C.c_double(), C.c_long()
+        self._call("bd_profile_read", int(slot), C.byref(ms), C.byref(n))
+        return ms.value, n.value
+
+    def launches(self) -> int:
+        return int(self.L.bd_launch_count(self.h))
+
     def device_bytes(self) -> int:
         return int(self.L.bd_device_bytes(self.h))
 
@@ -300,31 +322,64 @@ for _n in ("apply_pbc", "transform_coords", "inverse_coords", "reset_force", "bu
 # synthetic inputs
 
 
-def random_chains(Nb, Nc, L, seed, bond=2.0, min_sep=0.0, max_tries=200):
+def random_chains(Nb, Nc, L, seed, bond=2.0, min_sep=0.0, max_tries=200, max_restarts=200):
     """Seeded random-walk chains of bond length ``bond`` in a cubic box of edge L
-    centred at the origin, returned as three float64 arrays.  With min_sep > 0
-    each new bead is redrawn (up to max_tries) until it is at least min_sep from
-    every earlier bead, like the reference's own initialiser
-    (shear/src/main26.c:437-457)."""
+    centred at the origin, returned as three float64 arrays (unwrapped along
+    each chain).  With min_sep > 0 every bead keeps at least min_sep from all
+    earlier beads under cubic periodicity: a bead is redrawn up to max_tries
+    times, and a chain that gets stuck is regrown from a new start, as the
+    reference's own initialiser does (shear/src/main26.c:398-474)."""
     rng = np.random.default_rng(seed)
     N = Nb * Nc
     r = np.zeros((N, 3))
+    cell = max(min_sep, 1e-9)
+    nc = max(1, int(np.floor(L / cell)))
+    grid: dict = {}
+
+    def key(p):
+        q = np.floor((p - L * np.round(p / L) + L / 2) / L * nc).astype(int) % nc
+        return int(q[0]), int(q[1]), int(q[2])
+
+    def clear(p):
+        if min_sep <= 0:
+            return True
+        kx, ky, kz = key(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for b in grid.get(((kx + dx) % nc, (ky + dy) % nc, (kz + dz) % nc), ()):
+                        d = r[b] - p
+                        d -= L * np.round(d / L)
+                        if d @ d < min_sep * min_sep:
+                            return False
+        return True
+
     for c in range(Nc):
-        for b in range(Nb):
-            a = c * Nb + b
-            for _ in range(max_tries):
-                if b == 0:
-                    p = rng.uniform(-L / 2, L / 2, 3)
+        for _ in range(max_restarts):
+            placed = []
+            ok = True
+            for b in range(Nb):
+                a = c * Nb + b
+                for _ in range(max_tries):
+                    if b == 0:
+                        p = rng.uniform(-L / 2, L / 2, 3)
+                    else:
+                        v = rng.normal(size=3)
+                        p = r[a - 1] + bond * v / np.linalg.norm(v)
+                    if clear(p):
+                        break
                 else:
-                    v = rng.normal(size=3)
-                    p = r[a - 1] + bond * v / np.linalg.norm(v)
-                if min_sep <= 0 or a == 0:
+                    ok = False
                     break
-                d = r[:a] - p
-                d -= L * np.round(d / L)
-                if np.min(np.einsum("ij,ij->i", d, d)) >= min_sep * min_sep:
-                    break
-            r[a] = p
+                r[a] = p
+                grid.setdefault(key(p), []).append(a)
+                placed.append(a)
+            if ok:
+                break
+            for a in placed:
+                grid[key(r[a])].remove(a)
+        else:
+            raise RuntimeError("could not place chain %d without overlaps" % c)
     return [np.ascontiguousarray(r[:, k]) for k in range(3)]
 
 

@@ -448,6 +448,38 @@ __device__ float gasdev_dev(Ran1& g) {
   return g.gset;
 }
 
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11): ten rounds of two 32x32->64 multiplies with a Weyl key
+// schedule.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(M0, ctr.x), lo0 = M0 * ctr.x;
+    uint32_t hi1 = __umulhi(M1, ctr.z), lo1 = M1 * ctr.z;
+    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
+    key.x += W0;
+    key.y += W1;
+  }
+  return ctr;
+}
+
+// Gaussian noise from Philox: counter (pair index, step, stream), key = seed;
+// two 53-bit uniforms per draw, Box-Muller (u1 in (0,1]) for two deviates.
+__global__ void k_noise_philox(double* R, int n, unsigned long long seed, unsigned long long step) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * k >= n) return;
+  uint4 c = make_uint4((uint32_t)k, (uint32_t)step, (uint32_t)(step >> 32), 0x42445f42u);
+  uint4 x = philox4x32_10(c, make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  const double s53 = 1.0 / 9007199254740992.0;
+  double u1 = ((double)(((unsigned long long)(x.x >> 5) << 26) | (x.y >> 6)) + 1.0) * s53;
+  double u2 = (double)(((unsigned long long)(x.z >> 5) << 26) | (x.w >> 6)) * s53;
+  double r = sqrt(-2.0 * log(u1)), sn, cs;
+  sincospi(2.0 * u2, &sn, &cs);
+  R[2 * k] = r * cs;
+  if (2 * k + 1 < n) R[2 * k + 1] = r * sn;
+}
+
 // getNoise with the reference's generator (shear/src/main26.c:708-713).  The
 // generator is a sequential chain, so one thread draws all 3N deviates; the
 // shuffle table lives in shared memory.
@@ -643,10 +675,37 @@ int bd_destroy(bd_ctx* c) {
                   c->Ctab};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  prof_clear(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return BD_OK;
 }
+
+int bd_profile_enable(bd_ctx* c, int on) {
+  if (!c) return BD_ERR_ARG;
+  CU(cudaStreamSynchronize(c->stream));
+  prof_clear(c);
+  c->prof_on = on != 0;
+  return BD_OK;
+}
+
+int bd_profile_read(bd_ctx* c, int slot, double* total_ms, long* count) {
+  if (!c || slot < 0 || slot >= BD_PROF_SLOTS || !total_ms || !count) return BD_ERR_ARG;
+  CU(cudaStreamSynchronize(c->stream));
+  double tot = 0;
+  auto& a = c->prof_ev[slot][0];
+  auto& b = c->prof_ev[slot][1];
+  for (size_t k = 0; k < a.size() && k < b.size(); k++) {
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, a[k], b[k]));
+    tot += ms;
+  }
+  *total_ms = tot;
+  *count = (long)std::min(a.size(), b.size());
+  return BD_OK;
+}
+
+long long bd_launch_count(const bd_ctx* c) { return c ? c->launches : 0; }
 
 int bd_sync(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
@@ -845,6 +904,7 @@ static Lat kernel_lat(bd_ctx* c) {
 
 int bd_apply_pbc(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
+  c->launches++;
   k_apply_pbc<<<nblk(c->N, 256), 256, 0, c->stream>>>(kernel_lat(c), c->rx, c->ry, c->rz, c->N);
   return launch_ok(c);
 }
@@ -852,6 +912,7 @@ int bd_apply_pbc(bd_ctx* c) {
 int bd_transform_coords(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
   if (c->p.flow != BD_FLOW_EXT) return BD_OK;
+  c->launches++;
   k_rotate<<<nblk(c->N, 256), 256, 0, c->stream>>>(c->lat, c->rx, c->ry, c->N, 0);
   return launch_ok(c);
 }
@@ -859,12 +920,14 @@ int bd_transform_coords(bd_ctx* c) {
 int bd_inverse_coords(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
   if (c->p.flow != BD_FLOW_EXT) return BD_OK;
+  c->launches++;
   k_rotate<<<nblk(c->N, 256), 256, 0, c->stream>>>(c->lat, c->rx, c->ry, c->N, 1);
   return launch_ok(c);
 }
 
 int bd_reset_force(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
+  c->launches++;
   k_zero3<<<nblk(c->N, 256), 256, 0, c->stream>>>(c->fx, c->fy, c->fz, c->N);
   CU(cudaMemsetAsync(c->stress, 0, 24, c->stream));
   return launch_ok(c);
@@ -872,6 +935,7 @@ int bd_reset_force(bd_ctx* c) {
 
 int bd_bond_force(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
+  c->launches++;
   k_bond<<<nblk(c->N, 128), 128, 0, c->stream>>>(kernel_lat(c), c->rx, c->ry, c->rz, c->fx, c->fy,
                                                   c->fz, c->N, c->Nb, c->p.spring, c->kappas_eff,
                                                   c->p.qmax, c->qmax2, c->p.kappab, c->stress,
@@ -881,6 +945,7 @@ int bd_bond_force(bd_ctx* c) {
 
 int bd_ev_force(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
+  c->launches++;
   k_ev<<<nblk(c->N, 128), 128, 0, c->stream>>>(kernel_lat(c), c->rx, c->ry, c->rz, c->fx, c->fy,
                                                 c->fz, c->N, c->nb_count, c->nb_rows, c->maxnb,
                                                 c->r2cut, c->p.epsilon, c->stress);
@@ -891,8 +956,10 @@ int bd_coulomb_force(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
   if (c->nch < 2) return BD_OK;
   double4* cq = (double4*)c->dE;
+  c->launches++;
   k_gather_charges<<<nblk(c->nch, 256), 256, 0, c->stream>>>(c->rx, c->ry, c->rz, c->q, c->track,
                                                              c->nch, cq);
+  c->launches++;
   k_coulomb<<<nblk(c->nch * 32, 256), 256, 0, c->stream>>>(kernel_lat(c), cq, c->track, c->nch,
                                                            c->fx, c->fy, c->fz, c->p.lambda_b,
                                                            c->kappa_d);
@@ -901,12 +968,20 @@ int bd_coulomb_force(bd_ctx* c) {
 
 int bd_get_noise(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
-  k_gasdev_seq<<<1, 32, 0, c->stream>>>(c->rng, c->R, 3 * c->N);
+  c->launches++;
+  if (c->p.noise == BD_NOISE_PHILOX) {
+    int n = 3 * c->N, pairs = (n + 1) / 2;
+    k_noise_philox<<<nblk(pairs, 256), 256, 0, c->stream>>>(c->R, n, c->p.philox_seed,
+                                                            c->noise_draws++);
+  } else {
+    k_gasdev_seq<<<1, 32, 0, c->stream>>>(c->rng, c->R, 3 * c->N);
+  }
   return launch_ok(c);
 }
 
 int bd_update_fd(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
+  c->launches++;
   k_update_fd<<<nblk(c->N, 256), 256, 0, c->stream>>>(c->p.flow, c->rx, c->ry, c->rz, c->dxv,
                                                       c->dyv, c->dzv, c->fx, c->fy, c->fz, c->R,
                                                       c->N, c->p.dt, c->p.edot,
@@ -959,6 +1034,7 @@ int bd_step_reference(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
   if (!c || nsteps < 0) return BD_ERR_ARG;
   int s;
   bool ext = c->p.flow == BD_FLOW_EXT;
+  prof_begin(c, BD_PROF_STEP);
   for (int n = 0; n < nsteps; n++) {
     unsigned long t = t0 + (unsigned long)n;
     c->t = t;
@@ -972,9 +1048,11 @@ int bd_step_reference(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
     if (ext && (s = bd_transform_coords(c))) return s;
     if ((s = bd_apply_pbc(c))) return s;
     if ((s = build_neighbors(c, false))) return s;
+    prof_begin(c, BD_PROF_FORCES);
     if ((s = bd_bond_force(c))) return s;
     if ((s = bd_ev_force(c))) return s;
     if ((s = bd_coulomb_force(c))) return s;
+    prof_end(c, BD_PROF_FORCES);
     if ((s = bd_get_noise(c))) return s;
     if ((s = update_hi(c))) return s;
     if (with_hop) {
@@ -985,6 +1063,7 @@ int bd_step_reference(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
       if (ext && (s = bd_inverse_coords(c))) return s;
     }
   }
+  prof_end(c, BD_PROF_STEP);
   return check(c);
 }
 
@@ -992,7 +1071,31 @@ int bd_step_reference(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
 
 namespace bd {
 void rotate_coords(bd_ctx* c, int inverse) {
+  c->launches++;
   k_rotate<<<nblk(c->N, 256), 256, 0, c->stream>>>(c->lat, c->rx, c->ry, c->N, inverse);
 }
 }  // namespace bd
 
+namespace bd {
+void prof_begin(bd_ctx* c, int slot) {
+  if (!c->prof_on) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, c->stream);
+  c->prof_ev[slot][0].push_back(e);
+}
+void prof_end(bd_ctx* c, int slot) {
+  if (!c->prof_on) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, c->stream);
+  c->prof_ev[slot][1].push_back(e);
+}
+void prof_clear(bd_ctx* c) {
+  for (int s = 0; s < BD_PROF_SLOTS; s++)
+    for (int k = 0; k < 2; k++) {
+      for (cudaEvent_t e : c->prof_ev[s][k]) cudaEventDestroy(e);
+      c->prof_ev[s][k].clear();
+    }
+}
+}  // namespace bd

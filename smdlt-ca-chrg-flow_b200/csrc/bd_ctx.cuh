@@ -47,6 +47,7 @@ struct bd_ctx {
   double *q;                           // bead charge values (0/1 in reference mode)
   double *dE;                          // charge-hop energy scratch
   bd::Ran1 *rng;
+  unsigned long long noise_draws;  // Philox counter: one per bd_get_noise call
 
   // neighbours
   int *nb_count, *nb_rows, *nb_half;
@@ -74,9 +75,18 @@ struct bd_ctx {
   int sbin;
 
   size_t bytes;
+
+  // profiling: CUDA events around selected kernels on the context's stream
+  bool prof_on;
+  std::vector<cudaEvent_t> prof_ev[BD_PROF_SLOTS][2];
+  long long launches;  // kernels launched by the library
 };
 
 namespace bd {
+
+void prof_begin(bd_ctx* c, int slot);
+void prof_end(bd_ctx* c, int slot);
+void prof_clear(bd_ctx* c);
 
 int set_error_from_bits(int bits);
 int check(bd_ctx* c);                 // synchronise and fold device error bits

@@ -244,17 +244,25 @@ int charge_hop(bd_ctx* c) {
   int treal = (int)(c->t % (unsigned long)c->tp);
   l.treal = treal;
   l.delx = c->p.edot * treal * c->p.dt;
+  c->launches++;
   k_charge_values<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->q, c->track, nch, qk);
+  c->launches++;
   k_gather_charges_mc<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->rx, c->ry, c->rz, c->q, c->track,
                                                              nch, cq);
+  c->launches++;
   k_dh_energy_rows<<<(nch * 32 + 255) / 256, 256, 0, c->stream>>>(l, cq, nch, c->p.lambda_b,
                                                                    c->kappa_d, rowsum);
   cudaFuncSetAttribute(k_charge_hop, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  prof_begin(c, BD_PROF_HOP);
+  c->launches++;
   k_charge_hop<<<1, kHopThreads, smem, c->stream>>>(l, c->rx, c->ry, c->rz, N, c->Nb, nch,
                                                     c->track, c->old, qk, rowsum, c->rng,
                                                     c->p.lambda_b, c->kappa_d, c->p.barrier,
                                                     c->p.barrier2, c->hoplog);
+  prof_end(c, BD_PROF_HOP);
+  c->launches++;
   k_clear_charges<<<(N + 255) / 256, 256, 0, c->stream>>>(c->cflags, c->q, N);
+  c->launches++;
   k_scatter_charges<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->track, qk, nch, c->cflags, c->q);
   return launch_ok(c);
 }

@@ -564,25 +564,34 @@ int calc_hi(bd_ctx* c) {
   if (!kv.empty())
     CU(cudaMemcpyAsync(c->kvec, kv.data(), 8 * kv.size(), cudaMemcpyHostToDevice, c->stream));
   CU(cudaMemsetAsync(c->near_count, 0, 4, c->stream));
+  prof_begin(c, BD_PROF_HI_BUILD);
+  c->launches++;
   k_hi_far<<<(unsigned)c->ntiles, 256, 0, c->stream>>>(
       l, ew, c->rx, c->ry, c->rz, c->N, c->NT, c->tileI, c->grid, c->nbx, c->nby, c->nbz, c->nhx,
       c->nhy, c->nhz, c->bsx, c->bsy, c->bsz, c->nbins, c->Mt, (int2*)c->near_pairs,
       c->near_count, (long long)c->near_cap, c->err);
+  c->launches++;
   k_hi_near<<<148 * 8, 256, 0, c->stream>>>(l, ew, c->rx, c->ry, c->rz, c->NT,
                                                      (const int2*)c->near_pairs, c->near_count,
                                                      (long long)c->near_cap, c->kvec, c->Mt);
+  prof_end(c, BD_PROF_HI_BUILD);
   c->hi_built = true;
   return launch_ok(c);
 }
 
 // y0 = M_off v0, y1 = M_off v1 over the packed tiles (off-diagonal blocks).
 static int sym_matvec2(bd_ctx* c, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1) {
+  prof_begin(c, BD_PROF_MATVEC);
+  c->launches++;
   k_sym_matvec2<double><<<(unsigned)c->ntiles, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N,
                                                                      v0, v1, c->rowpart,
                                                                      c->colpart);
+  prof_end(c, BD_PROF_MATVEC);
   double* part = c->colpart + c->ntiles * 192;
+  c->launches++;
   k_matvec_reduce1<<<dim3(c->NT, kRedSplit), 192, 0, c->stream>>>(c->rowpart, c->colpart, c->NT,
                                                                   part);
+  c->launches++;
   k_matvec_reduce2<<<c->NT, 192, 0, c->stream>>>(part, c->NT, Y0, Y1);
   return launch_ok(c);
 }
@@ -603,6 +612,7 @@ int update_hi(bd_ctx* c) {
   VecIn vr = {{c->R, c->R + 1, c->R + 2}, 3};
   if ((s = sym_matvec2(c, vf, vr, c->U, c->W)) != BD_OK) return s;
   double p = sqrt(2.0 / c->p.dt);
+  c->launches++;
   k_tea_update<<<(c->N + 255) / 256, 256, 0, c->stream>>>(
       c->p.flow, c->rx, c->ry, c->rz, c->dxv, c->dyv, c->dzv, c->fx, c->fy, c->fz, c->R, c->U,
       c->W, c->NT * 32, c->Ctab + (size_t)c->sbin * 3 * c->Nb, c->Nb, c->N, c->p.dt, c->p.edot,

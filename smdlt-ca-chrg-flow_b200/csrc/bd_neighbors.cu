@@ -226,22 +226,30 @@ int build_neighbors(bd_ctx* c, bool force) {
   int treal = (int)(c->t % (unsigned long)c->tp);
   l.treal = treal;
   l.delx = c->p.edot * treal * c->p.dt;
-  if (force)
+  if (force) {
+    c->launches++;
     k_set_flag<<<1, 1, 0, c->stream>>>(c->flag, 1);
-  else
+  } else {
+    c->launches++;
     k_check_verlet<<<nblk(N, 256), 256, 0, c->stream>>>(c->dxv, c->dyv, c->dzv, N, c->rnew,
                                                           c->flag);
+  }
   CellGeom g = cell_geom(c, l);
+  c->launches++;
   k_cell_count<<<nblk(N, 256), 256, 0, c->stream>>>(c->flag, g, c->rx, c->ry, c->rz, N,
                                                     c->cell_of, c->cell_count);
+  c->launches++;
   k_cell_scan<<<1, 1024, 0, c->stream>>>(c->flag, g.ncell, c->cell_count, c->cell_start,
                                          c->cell_cursor);
+  c->launches++;
   k_cell_fill<<<nblk(N, 256), 256, 0, c->stream>>>(c->flag, c->cell_of, c->cell_start,
                                                    c->cell_cursor, c->cell_beads, N);
+  c->launches++;
   k_nbr_rows<<<nblk(N, 128), 128, 0, c->stream>>>(c->flag, g, l, c->rx, c->ry, c->rz, N,
                                                   c->cell_of, c->cell_start, c->cell_beads,
                                                   c->rv, c->maxnb, c->nb_count, c->nb_rows,
                                                   c->nb_half, c->dxv, c->dyv, c->dzv, c->err);
+  c->launches++;
   k_set_flag<<<1, 1, 0, c->stream>>>(c->flag, 0);
   return launch_ok(c);
 }
