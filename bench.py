@@ -88,10 +88,15 @@ def synth_inputs(w, seed):
     return x, y, z, q, beta, C
 
 
-def grid_table(nt_avg, nbins, seed):
-    g = np.random.default_rng(seed).normal(scale=1e-3, size=(nt_avg, nbins, 3, 3))
-    g = 0.5 * (g + np.swapaxes(g, -1, -2))
-    return np.ascontiguousarray(g.reshape(nt_avg, nbins * 9))
+def grid_table_host(w):
+    """The far-field lookup table for the reference arm, computed on the host
+    by the oracle's restatement of gridHI (pinned bit-exact to the reference's
+    gridHI program); the GPU arm builds the same table with bd_build_grid."""
+    import oracle as O
+    o = O.Oracle(w["flow"], w["Nb"], w["Nc"], w["L"], edot_of(w), w["dt"],
+                 nt_avg=COMMON["nt_avg"], bin_size=COMMON["bin_size"])
+    D, _ = o.grid(0.001, w["L"] ** 3)
+    return D
 
 
 # ---------------------------------------------------------------------------
@@ -122,8 +127,7 @@ def time_reference(w, steps, warmup, threads):
     kw.pop("srpy")
     ref = O.RefSim(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
                    threads=threads, **kw)
-    nbins = int(ref.bins()[6])
-    G = grid_table(COMMON["nt_avg"], nbins, 7)
+    G = grid_table_host(w)
     for nt in range(COMMON["nt_avg"]):
         ref.set_grid(nt, np.ascontiguousarray(G[nt]))
     for sb in range(21):
@@ -237,10 +241,7 @@ def build_context(w, seed, device_noise="philox"):
     p = B.make_params(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
                       noise=device_noise, philox_seed=seed, **force_params(w))
     c = B.Context(p)
-    nbins = int(c.grid_shape()[6])
-    G = grid_table(COMMON["nt_avg"], nbins, 7)
-    for nt in range(COMMON["nt_avg"]):
-        c.load_grid(nt, G[nt])
+    c.build_grid(0.001)
     for sb in range(21):
         c.set_tea(sb, beta[sb], C[sb])
     c.set_positions(x, y, z)

@@ -127,6 +127,13 @@ int bd_get_rng(bd_ctx *ctx, bd_ran1_state *s);
  * mm/G*.txt by initEwald (shear/src/Initialization.c:497-520): num_bins
  * row-major 3x3 tensors.  The tensors must be symmetric. */
 int bd_load_grid(bd_ctx *ctx, int nt, const double *D9);
+/* Builds all nt_avg frames of the lookup table on the device, as the
+ * reference's separate gridHI program does (shear/src/gridHI.c:3-278),
+ * instead of reading mm/G*.txt.  grid_dt is gridHI's own time step (it
+ * hard-codes 0.001, shear/src/gridHI.c:288; 0 selects that).  Fails with
+ * BD_ERR_STATE if gridHI's bin geometry differs from the simulation's. */
+int bd_build_grid(bd_ctx *ctx, double grid_dt);
+int bd_download_grid(bd_ctx *ctx, int nt, double *D9);
 /* Lookup-grid geometry as initLattice derives it
  * (shear/src/Initialization.c:281-295): nbx nby nbz nhx nhy nhz num_bins. */
 int bd_grid_shape(const bd_ctx *ctx, int *out7);

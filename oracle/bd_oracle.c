@@ -81,6 +81,7 @@ void bdo_init(bdo_sys *s, int flow, int Nb, int Nc, double L, double edot,
     xmax = p0[2][0] * exp(edot * treal * dt);
   }
   zmax = L / 2;
+  s->bin_size = bin_size;
   s->bsx = bin_size;
   s->bsy = bin_size;
   s->bsz = bin_size;
@@ -426,35 +427,15 @@ int bdo_check_verlet(const bdo_sys *s, const double *dxv, const double *dyv,
 
 /* ---- hydrodynamic mobility ---------------------------------------------- */
 
-/* calcHI: dense 3N x 3N Rotne-Prager-Yamakawa mobility with Beenakker's Ewald
- * split (shear/src/main26.c:1530-1806, extensional/src/main14.c:1548-1824).
- * Pairs whose minimum image is closer than 12 get the explicit real-space
- * image sum plus the explicit k-space cosine sum; other pairs copy the
- * lookup-table tensor of their displacement bin.  grid holds nt_avg frames of
- * nbins 3x3 tensors.  M is row-major 9 N^2 (block (i,j) at 9N i + 9 j);
- * only the upper blocks and the diagonal entries of the diagonal blocks are
- * written, as in the reference. */
-void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
-                 const double *rz, const double *grid, double *M) {
-  int N = s->N;
-  double L = s->L, boxvol = L * L * L;
-  int treal = (int)(s->t % (unsigned long)s->tp);
-  double rce, M_HI = 4.0;
-  int nmax;
-  if (treal <= s->tp / 2) {
-    rce = 1.0 * s->L2yp;
-    nmax = 1;
-  } else {
-    rce = 2.0 * s->L2yp;
-    nmax = 2;
-  }
-  double tf = (double)treal / s->tp;
-  int nt = (int)round(tf * s->nt_avg) % s->nt_avg;
-  double alpha = M_HI / rce, rkcut = 2.0 * M_HI * M_HI / rce;
-  double rkkcut = rkcut * rkcut, rtpi = sqrt(M_PI);
-  double alpha2 = alpha * alpha, alpha3 = alpha2 * alpha, alpha4 = alpha2 * alpha2;
-  double alpha5 = alpha4 * alpha, alpha7 = alpha4 * alpha2 * alpha;
-  double selfconst = 1 - 6 / rtpi * alpha + 40 / (3 * rtpi) * alpha3;
+/* Wave vectors of the k-space mobility sum and their 3x3 coefficients
+ * (shear/src/main26.c:1557-1652; ext reciprocal of the rotated lattice,
+ * extensional/src/main14.c:1575-1670; identical loops in gridHI.c:38-144),
+ * including the reference's bound scans, the halving of the kx = 0 plane and
+ * the zeroed k = 0 term.  Returns nk and malloc'd M2[9 nk], kv[3 nk]. */
+static void kvectors(const bdo_sys *s, double boxvol, double rkkcut, double rkcut,
+                     double alpha2, double alpha4, int *nk_out, double **M2_out,
+                     double **kv_out) {
+  double L = s->L;
   const double *L1 = s->L1, *L2 = s->L2;
   int kxmax = ceil(rkcut * s->detL / (M_PI * 2.0 * L * L2[1]));
   int kymax = ceil(rkcut * s->detL / (M_PI * 2.0 * L * L1[0]));
@@ -553,6 +534,48 @@ void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
         c++;
       }
   }
+  free(kyup);
+  free(kylo);
+  free(kzup);
+  free(kzlo);
+  *nk_out = nk;
+  *M2_out = M2;
+  *kv_out = kv;
+}
+
+/* calcHI: dense 3N x 3N Rotne-Prager-Yamakawa mobility with Beenakker's Ewald
+ * split (shear/src/main26.c:1530-1806, extensional/src/main14.c:1548-1824).
+ * Pairs whose minimum image is closer than 12 get the explicit real-space
+ * image sum plus the explicit k-space cosine sum; other pairs copy the
+ * lookup-table tensor of their displacement bin.  grid holds nt_avg frames of
+ * nbins 3x3 tensors.  M is row-major 9 N^2 (block (i,j) at 9N i + 9 j);
+ * only the upper blocks and the diagonal entries of the diagonal blocks are
+ * written, as in the reference. */
+void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
+                 const double *rz, const double *grid, double *M) {
+  int N = s->N;
+  double L = s->L, boxvol = L * L * L;
+  int treal = (int)(s->t % (unsigned long)s->tp);
+  double rce, M_HI = 4.0;
+  int nmax;
+  if (treal <= s->tp / 2) {
+    rce = 1.0 * s->L2yp;
+    nmax = 1;
+  } else {
+    rce = 2.0 * s->L2yp;
+    nmax = 2;
+  }
+  double tf = (double)treal / s->tp;
+  int nt = (int)round(tf * s->nt_avg) % s->nt_avg;
+  double alpha = M_HI / rce, rkcut = 2.0 * M_HI * M_HI / rce;
+  double rkkcut = rkcut * rkcut, rtpi = sqrt(M_PI);
+  double alpha2 = alpha * alpha, alpha3 = alpha2 * alpha, alpha4 = alpha2 * alpha2;
+  double alpha5 = alpha4 * alpha, alpha7 = alpha4 * alpha2 * alpha;
+  double selfconst = 1 - 6 / rtpi * alpha + 40 / (3 * rtpi) * alpha3;
+  const double *L1 = s->L1, *L2 = s->L2;
+  int nk;
+  double *M2, *kv;
+  kvectors(s, boxvol, rkkcut, rkcut, alpha2, alpha4, &nk, &M2, &kv);
   double Dtr[3] = {selfconst, selfconst, selfconst};
   for (int c = 0; c < nk; c++) {
     Dtr[0] += M2[9 * c];
@@ -654,12 +677,149 @@ void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
       }
     }
   }
-  free(kyup);
-  free(kylo);
-  free(kzup);
-  free(kzlo);
   free(M2);
   free(kv);
+}
+
+/* gridHI: the far-field lookup table, nt_avg lattice frames of the full
+ * Ewald-summed RPY tensor at every bin centre (shear/src/gridHI.c:13-246,
+ * extensional/src/gridHI.c:13-239).  gridHI runs with its own time step
+ * (dt = 0.001, shear/src/gridHI.c:288) for the period and the bin geometry,
+ * takes frame nt at t = nt*tp/nt_avg, uses M_HI = 6, no self term, and
+ * evaluates the origin bin at (0.6, 0.6, 0.6).  D receives nt_avg x nbins
+ * row-major 3x3 tensors on gridHI's bin geometry, which is returned in
+ * geom[]: nbx nby nbz nhx nhy nhz nbins origin. */
+/* gridHI's period and bin geometry from its own time step
+ * (shear/src/gridHI.c:367-432): geom = nbx nby nbz nhx nhy nhz nbins origin. */
+static void grid_geom(bdo_sys *s, double grid_dt, int *geom) {
+  double L = s->L, edot = s->edot;
+  s->dt = grid_dt;
+  s->tp = (int)(EPK / edot / grid_dt);
+  double th = 90.0 - (45.0 + (s->flow == 0 ? 0.0 : 31.7));
+  th *= M_PI / 180;
+  double p0x2 = sqrt(2) / 2 * L * cos(th), p0y1 = -sqrt(2) / 2 * L * cos(th);
+  double xmax, ymax, zmax = L / 2;
+  int treal = s->tp;
+  if (s->flow == 0) {
+    ymax = L / 2;
+    xmax = L / 2 * edot * treal * grid_dt;
+  } else {
+    ymax = -p0y1;
+    xmax = p0x2 * exp(edot * treal * grid_dt);
+  }
+  s->bsx = s->bsy = s->bsz = s->bin_size;
+  s->nbx = 2 * ceil(xmax / s->bsx) + 1;
+  s->bsx = xmax / ((s->nbx - 1) / 2);
+  s->nhx = (s->nbx - 1) / 2;
+  s->nby = 2 * ceil(ymax / s->bsy) + 1;
+  s->bsy = ymax / ((s->nby - 1) / 2);
+  s->nhy = (s->nby - 1) / 2;
+  s->nbz = 2 * ceil(zmax / s->bsz) + 1;
+  s->bsz = zmax / ((s->nbz - 1) / 2);
+  s->nhz = (s->nbz - 1) / 2;
+  s->nbins = s->nbx * s->nby * s->nbz;
+  geom[0] = s->nbx;
+  geom[1] = s->nby;
+  geom[2] = s->nbz;
+  geom[3] = s->nhx;
+  geom[4] = s->nhy;
+  geom[5] = s->nhz;
+  geom[6] = s->nbins;
+  geom[7] = s->nhx * s->nby * s->nbz + s->nhy * s->nbz + s->nhz;
+}
+
+void bdo_grid_geom(const bdo_sys *s0, double grid_dt, int *geom) {
+  bdo_sys s = *s0;
+  grid_geom(&s, grid_dt, geom);
+}
+
+void bdo_grid(const bdo_sys *s0, double grid_dt, double boxvol, double *D, int *geom) {
+  bdo_sys s = *s0;
+  double L = s.L;
+  grid_geom(&s, grid_dt, geom);
+  int origin = geom[7];
+  double rtpi = sqrt(M_PI);
+  for (int nt = 0; nt < s.nt_avg; nt++) {
+    unsigned long t = (unsigned long)(nt * s.tp / s.nt_avg);
+    bdo_lattice(&s, t);
+    int treal = (int)(t % (unsigned long)s.tp), nmax;
+    double rce;
+    if (treal <= s.tp / 2) {
+      rce = s.L2yp;
+      nmax = 1;
+    } else {
+      rce = 2.0 * s.L2yp;
+      nmax = 2;
+    }
+    double M_HI = 6.0;
+    double alpha = M_HI / rce, rkcut = 2.0 * M_HI * M_HI / rce, rkkcut = rkcut * rkcut;
+    double alpha2 = alpha * alpha, alpha3 = alpha2 * alpha, alpha4 = alpha2 * alpha2;
+    double alpha5 = alpha4 * alpha, alpha7 = alpha4 * alpha2 * alpha;
+    int nk;
+    double *M2, *kv;
+    kvectors(&s, boxvol, rkkcut, rkcut, alpha2, alpha4, &nk, &M2, &kv);
+    /* bins are independent: spread them over the host threads */
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int b = 0; b < s.nbins; b++) {
+      double dr[3];
+      if (b != origin) {
+        int bb = b;
+        int bx = bb / (s.nby * s.nbz);
+        bb -= bx * s.nby * s.nbz;
+        bx -= s.nhx;
+        int by = bb / s.nbz;
+        bb -= by * s.nbz;
+        by -= s.nhy;
+        int bz = bb - s.nhz;
+        dr[0] = bx * s.bsx;
+        dr[1] = by * s.bsy;
+        dr[2] = bz * s.bsz;
+      } else {
+        dr[0] = dr[1] = dr[2] = 0.6;
+      }
+      double Dt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int nx = -nmax; nx < nmax + 1; nx++)
+        for (int ny = -nmax; ny < nmax + 1; ny++)
+          for (int nz = -nmax; nz < nmax + 1; nz++) {
+            double dx = dr[0] + nx * s.L1[0] + ny * s.L2[0];
+            double dy = dr[1] + nx * s.L1[1] + ny * s.L2[1];
+            double dz = dr[2] + nz * L;
+            double rr = dx * dx + dy * dy + dz * dz, r = sqrt(rr);
+            if (r < rce) {
+              double C1, C2, C3, C4;
+              if (r > 2.0) {
+                C1 = 0.75 / r + 0.5 / (r * rr);
+                C2 = 4.0 * alpha7 * rr * rr + 3.0 * alpha3 * rr - 20.0 * alpha5 * rr - 4.5 * alpha + 14.0 * alpha3 + alpha / rr;
+                C3 = 0.75 / r - 1.5 / (r * rr);
+                C4 = -4.0 * alpha7 * rr * rr - 3.0 * alpha3 * rr + 16.0 * alpha5 * rr + 1.5 * alpha - 2.0 * alpha3 - 3.0 * alpha / rr;
+              } else {
+                C1 = 1.0 - 0.28125 * r;
+                C2 = 64.0 * alpha7 + 12.0 * alpha3 - 80.0 * alpha5 - 4.5 * alpha + 14.0 * alpha3 + 0.25 * alpha;
+                C3 = 0.09375 * r;
+                C4 = -64.0 * alpha7 - 12.0 * alpha3 + 64.0 * alpha5 + 1.5 * alpha - 2.0 * alpha3 - 0.75 * alpha;
+              }
+              double t1 = C1 * erfc(alpha * r) + C2 * exp(-alpha2 * rr) / rtpi;
+              double t2 = C3 * erfc(alpha * r) + C4 * exp(-alpha2 * rr) / rtpi;
+              Dt[0] += t1 + t2 * dx * dx / rr;
+              Dt[1] += t2 * dx * dy / rr;
+              Dt[2] += t2 * dx * dz / rr;
+              Dt[3] += t2 * dx * dy / rr;
+              Dt[4] += t1 + t2 * dy * dy / rr;
+              Dt[5] += t2 * dy * dz / rr;
+              Dt[6] += t2 * dx * dz / rr;
+              Dt[7] += t2 * dy * dz / rr;
+              Dt[8] += t1 + t2 * dz * dz / rr;
+            }
+          }
+      for (int c = 0; c < nk; c++) {
+        double ck = cos(kv[3 * c] * dr[0] + kv[3 * c + 1] * dr[1] + kv[3 * c + 2] * dr[2]);
+        for (int a = 0; a < 9; a++) Dt[a] += M2[9 * c + a] * ck;
+      }
+      memcpy(D + ((size_t)nt * s.nbins + b) * 9, Dt, 9 * sizeof(double));
+    }
+    free(M2);
+    free(kv);
+  }
 }
 
 /* updateHI: TEA Brownian displacement dt M (F + sqrt(2/dt) beta C R) plus the

@@ -48,6 +48,7 @@ class Sys(C.Structure):
         ("nt_avg", C.c_int), ("nbx", C.c_int), ("nby", C.c_int), ("nbz", C.c_int),
         ("nhx", C.c_int), ("nhy", C.c_int), ("nhz", C.c_int), ("nbins", C.c_int),
         ("bsx", C.c_double), ("bsy", C.c_double), ("bsz", C.c_double),
+        ("bin_size", C.c_double),
     ]
 
 
@@ -87,6 +88,8 @@ def lib() -> C.CDLL:
         L.bdo_verlet.argtypes = [sp, _dp, _dp, _dp, _ip, _ip, C.c_int]
         L.bdo_check_verlet.argtypes = [sp, _dp, _dp, _dp]
         L.bdo_calc_hi.argtypes = [sp, _dp, _dp, _dp, _dp, _dp]
+        L.bdo_grid.argtypes = [sp, C.c_double, C.c_double, _dp, _ip]
+        L.bdo_grid_geom.argtypes = [sp, C.c_double, _ip]
         L.bdo_update_hi.argtypes = [sp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                     C.c_double, _dp]
         L.bdo_update_fd.argtypes = [sp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -153,6 +156,15 @@ class Oracle:
         M = np.zeros(9 * self.N * self.N)
         lib().bdo_calc_hi(C.byref(self.s), x, y, z, np.ascontiguousarray(grid, dtype=np.float64), M)
         return M
+
+    def grid(self, grid_dt=0.001, box_volume=None):
+        """gridHI's table: (D[nt_avg, nbins*9], geom[8]) on gridHI's bin geometry."""
+        bv = self.s.L ** 3 if box_volume is None else box_volume
+        geom = np.zeros(8, np.int32)
+        lib().bdo_grid_geom(C.byref(self.s), grid_dt, geom)
+        D = np.zeros(self.s.nt_avg * int(geom[6]) * 9)
+        lib().bdo_grid(C.byref(self.s), grid_dt, bv, D, geom)
+        return D.reshape(self.s.nt_avg, -1), geom
 
     def update_hi(self, x, y, z, dv, f, R, M, beta, Ct):
         lib().bdo_update_hi(C.byref(self.s), x, y, z, dv[0], dv[1], dv[2], f[0], f[1], f[2],
@@ -372,3 +384,34 @@ class OracleSim:
             o.charge_hop(self.x, self.y, self.z, self.track, self.old, self.rng)
             if ext:
                 o.rotate(self.x, self.y, 1)
+
+
+def ref_grid(flow, Nb, Nc, c_norm, edot, nt_avg, bin_size, workdir):
+    """Runs the reference's gridHI main (one per process) in workdir and
+    returns (D[nt_avg, nbins*9], bins[8], geom[7]) from its globals."""
+    path = os.path.join(HERE, "_ref", "libref_grid_shear.so" if flow == 0 else "libref_grid_ext.so")
+    lib_ = C.CDLL(path, mode=C.RTLD_LOCAL)
+    os.makedirs(os.path.join(workdir, "mm"), exist_ok=True)
+    cwd = os.getcwd()
+    os.chdir(workdir)
+    try:
+        argv = ["gridHI", "-c", repr(c_norm), "-b", str(Nb), "-a", str(Nc), "-f", repr(edot),
+                "-s", str(nt_avg), "-g", repr(bin_size), "-n", "1"]
+        arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+        lib_.grid_main.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
+        lib_.grid_main(len(argv), arr)
+    finally:
+        os.chdir(cwd)
+    bins = np.zeros(8, np.int32)
+    lib_.hg_bins.argtypes = [_ip]
+    lib_.hg_bins(bins)
+    geom = np.zeros(7)
+    lib_.hg_geom.argtypes = [_dp]
+    lib_.hg_geom(geom)
+    lib_.hg_D.argtypes = [C.c_int, _dp]
+    D = np.zeros((nt_avg, int(bins[6]) * 9))
+    for nt in range(nt_avg):
+        row = np.zeros(int(bins[6]) * 9)
+        lib_.hg_D(nt, row)
+        D[nt] = row
+    return D, bins, geom

@@ -106,6 +106,8 @@ def _lib() -> C.CDLL:
         L.bd_get_rng.argtypes = [vp, C.POINTER(Ran1State)]
         L.bd_load_grid.argtypes = [vp, C.c_int, _dp]
         L.bd_grid_shape.argtypes = [vp, _ip]
+        L.bd_build_grid.argtypes = [vp, C.c_double]
+        L.bd_download_grid.argtypes = [vp, C.c_int, _dp]
         L.bd_set_tea.argtypes = [vp, C.c_int, C.c_double, _dp]
         L.bd_set_time.argtypes = [vp, C.c_ulong, C.c_ulong]
         L.bd_update_lattice.argtypes = [vp, C.c_ulong]
@@ -256,6 +258,14 @@ class Context:
 
     def load_grid(self, nt, D9):
         self._call("bd_load_grid", int(nt), np.ascontiguousarray(D9, np.float64))
+
+    def build_grid(self, grid_dt=0.001):
+        self._call("bd_build_grid", float(grid_dt))
+
+    def grid(self, nt):
+        o = np.zeros(int(self.grid_shape()[6]) * 9)
+        self._call("bd_download_grid", int(nt), o)
+        return o
 
     def set_tea(self, sbin, beta, c3nb):
         self._call("bd_set_tea", int(sbin), float(beta), np.ascontiguousarray(c3nb, np.float64))

@@ -68,12 +68,16 @@ static void corners0(int flow, double L, double p0[3][2]) {
 // 1426-1450), evaluated on the host with the C library so that every kernel
 // sees the reference's lattice bit for bit.
 void host_lattice(bd_ctx* c, unsigned long t, Lat* out) {
+  host_lattice_at(c, t, c->p.dt, c->tp, out);
+}
+
+void host_lattice_at(bd_ctx* c, unsigned long t, double dt, int tp, Lat* out) {
   Lat l;
   memset(&l, 0, sizeof(l));
   double L = c->p.L, p0[3][2], pt[3][2];
   corners0(c->p.flow, L, p0);
-  int treal = (int)(t % (unsigned long)c->tp);
-  double edot = c->p.edot, dt = c->p.dt;
+  int treal = (int)(t % (unsigned long)tp);
+  double edot = c->p.edot;
   if (c->p.flow == 0) {
     for (int a = 0; a < 3; a++) {
       pt[a][1] = p0[a][1];
@@ -87,8 +91,8 @@ void host_lattice(bd_ctx* c, unsigned long t, Lat* out) {
   }
   l.flow = c->p.flow;
   l.treal = treal;
-  l.tp = c->tp;
-  l.nmax = (treal <= c->tp / 2) ? 1 : 2;
+  l.tp = tp;
+  l.nmax = (treal <= tp / 2) ? 1 : 2;
   l.L = L;
   l.L1x = pt[2][0] - pt[1][0];
   l.L1y = pt[2][1] - pt[1][1];

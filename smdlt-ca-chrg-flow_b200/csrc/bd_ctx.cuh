@@ -92,6 +92,7 @@ int set_error_from_bits(int bits);
 int check(bd_ctx* c);                 // synchronise and fold device error bits
 int launch_ok(bd_ctx* c);             // report an asynchronous launch error
 void host_lattice(bd_ctx* c, unsigned long t, Lat* out);
+void host_lattice_at(bd_ctx* c, unsigned long t, double dt, int tp, Lat* out);
 void rotate_coords(bd_ctx* c, int inverse);  // transformCoords (0) / inverseCoords (1)
 
 // neighbours

@@ -131,6 +131,43 @@ __global__ void __launch_bounds__(256) k_hi_far(Lat l, Ewald ew, const double* _
 }
 
 // kvec rows: rkx rky rkz m00 m01 m02 m11 m12 m22
+// Lane share of the Ewald-summed RPY tensor at raw displacement (dxo,dyo,dzo):
+// real-space images within rce (shear/src/main26.c:1722-1763) and the
+// k-space cosine sum (shear/src/main26.c:1764-1788); lanes stride over both.
+__device__ __forceinline__ void ewald6(const Lat& l, const Ewald& ew, double dxo, double dyo,
+                                       double dzo, const double* __restrict__ kvec, int lane,
+                                       double acc[6]) {
+  for (int a = 0; a < 6; a++) acc[a] = 0.0;
+  int side = 2 * ew.nmax + 1, nimg = side * side * side;
+  for (int m = lane; m < nimg; m += 32) {
+    int nz = m % side - ew.nmax, ny = (m / side) % side - ew.nmax, nx = m / (side * side) - ew.nmax;
+    double dx = dxo + nx * l.L1x + ny * l.L2x;
+    double dy = dyo + nx * l.L1y + ny * l.L2y;
+    double dz = dzo + nz * l.L;
+    double rr = dx * dx + dy * dy + dz * dz;
+    if (sqrt(rr) < ew.rce) {
+      double t1, t2;
+      rpy_real(ew, rr, t1, t2);
+      acc[0] += t1 + t2 * dx * dx / rr;
+      acc[1] += t2 * dx * dy / rr;
+      acc[2] += t2 * dx * dz / rr;
+      acc[3] += t1 + t2 * dy * dy / rr;
+      acc[4] += t2 * dy * dz / rr;
+      acc[5] += t1 + t2 * dz * dz / rr;
+    }
+  }
+  for (int c = lane; c < ew.nk; c += 32) {
+    const double* kv = kvec + 9 * c;
+    double ck = cos(kv[0] * dxo + kv[1] * dyo + kv[2] * dzo);
+    acc[0] += kv[3] * ck;
+    acc[1] += kv[4] * ck;
+    acc[2] += kv[5] * ck;
+    acc[3] += kv[6] * ck;
+    acc[4] += kv[7] * ck;
+    acc[5] += kv[8] * ck;
+  }
+}
+
 __device__ __forceinline__ void near_pair(const Lat& l, const Ewald& ew,
                                           const double* __restrict__ rx,
                                           const double* __restrict__ ry,
@@ -173,35 +210,8 @@ __device__ __forceinline__ void near_pair(const Lat& l, const Ewald& ew,
     ryj = rx[j] * l.sth + ry[j] * l.cth;
   }
   double dxo = rxj - rxi, dyo = ryj - ryi, dzo = rz[j] - rz[i];
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  int side = 2 * ew.nmax + 1, nimg = side * side * side;
-  for (int m = lane; m < nimg; m += 32) {
-    int nz = m % side - ew.nmax, ny = (m / side) % side - ew.nmax, nx = m / (side * side) - ew.nmax;
-    double dx = dxo + nx * l.L1x + ny * l.L2x;
-    double dy = dyo + nx * l.L1y + ny * l.L2y;
-    double dz = dzo + nz * l.L;
-    double rr = dx * dx + dy * dy + dz * dz;
-    if (sqrt(rr) < ew.rce) {
-      double t1, t2;
-      rpy_real(ew, rr, t1, t2);
-      acc[0] += t1 + t2 * dx * dx / rr;
-      acc[1] += t2 * dx * dy / rr;
-      acc[2] += t2 * dx * dz / rr;
-      acc[3] += t1 + t2 * dy * dy / rr;
-      acc[4] += t2 * dy * dz / rr;
-      acc[5] += t1 + t2 * dz * dz / rr;
-    }
-  }
-  for (int c = lane; c < ew.nk; c += 32) {
-    const double* kv = kvec + 9 * c;
-    double ck = cos(kv[0] * dxo + kv[1] * dyo + kv[2] * dzo);
-    acc[0] += kv[3] * ck;
-    acc[1] += kv[4] * ck;
-    acc[2] += kv[5] * ck;
-    acc[3] += kv[6] * ck;
-    acc[4] += kv[7] * ck;
-    acc[5] += kv[8] * ck;
-  }
+  double acc[6];
+  ewald6(l, ew, dxo, dyo, dzo, kvec, lane, acc);
   for (int a = 0; a < 6; a++)
     for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
   if (lane == 0) {
@@ -209,6 +219,36 @@ __device__ __forceinline__ void near_pair(const Lat& l, const Ewald& ew,
     double* tb = Mt + (tile_off(I, NT) + (J - I)) * 6144;
     int e = (i & 31) * 32 + (j & 31);
     for (int a = 0; a < 6; a++) tb[a * 1024 + e] = acc[a];
+  }
+}
+
+// gridHI (shear/src/gridHI.c:145-240): one warp per bin of one lattice frame;
+// the bin centre is the displacement, except the origin bin at (0.6,0.6,0.6).
+__global__ void __launch_bounds__(256) k_grid_bins(Lat l, Ewald ew,
+                                                   const double* __restrict__ kvec, int nbins,
+                                                   int nby, int nbz, int nhx, int nhy, int nhz,
+                                                   double bsx, double bsy, double bsz,
+                                                   int origin, double* out) {
+  int lane = threadIdx.x & 31;
+  int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbins; b += nw) {
+    double dx, dy, dz;
+    if (b != origin) {
+      int bb = b, bx = bb / (nby * nbz);
+      bb -= bx * nby * nbz;
+      int by = bb / nbz, bz = bb - by * nbz;
+      dx = (bx - nhx) * bsx;
+      dy = (by - nhy) * bsy;
+      dz = (bz - nhz) * bsz;
+    } else {
+      dx = dy = dz = 0.6;
+    }
+    double acc[6];
+    ewald6(l, ew, dx, dy, dz, kvec, lane, acc);
+    for (int a = 0; a < 6; a++)
+      for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
+    if (lane == 0)
+      for (int a = 0; a < 6; a++) out[(size_t)b * 6 + a] = acc[a];
   }
 }
 
@@ -397,10 +437,12 @@ static int ensure_tiles(bd_ctx* c) {
 // of calcHI (shear/src/main26.c:1536-1686; ext k-vectors of the rotated
 // reciprocal lattice, extensional/src/main14.c:1582-1588), generated with
 // the reference's loop structure and arithmetic.
-static void hi_setup(bd_ctx* c, const Lat& l, Ewald* ew, std::vector<double>* kv, double Dtr[3]) {
+static void hi_setup(bd_ctx* c, const Lat& l, Ewald* ew, std::vector<double>* kv, double Dtr[3],
+                     double M_HI = 4.0, int tp = 0) {
   double L = l.L, boxvol = c->boxvol;
-  int treal = l.treal, tp = c->tp, nmax;
-  double rce, M_HI = 4.0;
+  if (tp == 0) tp = c->tp;
+  int treal = l.treal, nmax;
+  double rce;
   if (treal <= tp / 2) {
     rce = 1.0 * l.L2yp;
     nmax = 1;
@@ -651,6 +693,76 @@ int download_mobility(bd_ctx* c, double* M9) {
 }
 
 }  // namespace bd
+
+// gridHI's main (shear/src/gridHI.c:3-278) on the device: the period and bin
+// geometry follow gridHI's own time step, frame nt is taken at
+// t = nt*tp/nt_avg, and the Ewald split uses M_HI = 6.
+extern "C" int bd_build_grid(bd_ctx* c, double grid_dt) {
+  if (!c) return BD_ERR_ARG;
+  if (grid_dt <= 0) grid_dt = 0.001;
+  double L = c->p.L, edot = c->p.edot;
+  int tp = (int)(0.9624 / edot / grid_dt);
+  if (tp < 1) return BD_ERR_ARG;
+  double th = (90.0 - (45.0 + (c->p.flow == 0 ? 0.0 : 31.7))) * (M_PI / 180);
+  double xmax, ymax, zmax = L / 2;
+  if (c->p.flow == 0) {
+    ymax = L / 2;
+    xmax = L / 2 * edot * tp * grid_dt;
+  } else {
+    ymax = -(-sqrt(2) / 2 * L * cos(th));
+    xmax = (sqrt(2) / 2 * L * cos(th)) * exp(edot * tp * grid_dt);
+  }
+  double bs = c->p.bin_size, bsx = bs, bsy = bs, bsz = bs;
+  int nbx = 2 * ceil(xmax / bsx) + 1;
+  bsx = xmax / ((nbx - 1) / 2);
+  int nhx = (nbx - 1) / 2;
+  int nby = 2 * ceil(ymax / bsy) + 1;
+  bsy = ymax / ((nby - 1) / 2);
+  int nhy = (nby - 1) / 2;
+  int nbz = 2 * ceil(zmax / bsz) + 1;
+  bsz = zmax / ((nbz - 1) / 2);
+  int nhz = (nbz - 1) / 2;
+  int nbins = nbx * nby * nbz;
+  if (nbins != c->nbins || nbx != c->nbx || nby != c->nby) return BD_ERR_STATE;
+  int origin = nhx * nby * nbz + nhy * nbz + nhz;
+  for (int nt = 0; nt < c->p.nt_avg; nt++) {
+    unsigned long t = (unsigned long)(nt * tp / c->p.nt_avg);
+    Lat l;
+    host_lattice_at(c, t, grid_dt, tp, &l);
+    Ewald ew;
+    std::vector<double> kv;
+    double unused[3];
+    hi_setup(c, l, &ew, &kv, unused, 6.0, tp);
+    if ((int)kv.size() / 9 > c->kvec_cap) {
+      CU(cudaStreamSynchronize(c->stream));
+      if (c->kvec) cudaFree(c->kvec);
+      c->kvec_cap = (int)kv.size() / 9 + 64;
+      CU(cudaMalloc(&c->kvec, 8 * 9 * (size_t)c->kvec_cap));
+    }
+    if (!kv.empty())
+      CU(cudaMemcpyAsync(c->kvec, kv.data(), 8 * kv.size(), cudaMemcpyHostToDevice, c->stream));
+    c->launches++;
+    k_grid_bins<<<148 * 4, 256, 0, c->stream>>>(l, ew, c->kvec, nbins, nby, nbz, nhx, nhy, nhz, bsx,
+                                                bsy, bsz, origin,
+                                                c->grid + (size_t)nt * nbins * 6);
+    // the host vector kv is reused next frame: wait for the copy to finish
+    CU(cudaStreamSynchronize(c->stream));
+  }
+  return check(c);
+}
+
+extern "C" int bd_download_grid(bd_ctx* c, int nt, double* D9) {
+  if (!c || !D9 || nt < 0 || nt >= c->p.nt_avg) return BD_ERR_ARG;
+  std::vector<double> g((size_t)c->nbins * 6);
+  CU(cudaMemcpyAsync(g.data(), c->grid + (size_t)nt * c->nbins * 6, 8 * g.size(),
+                     cudaMemcpyDeviceToHost, c->stream));
+  int s = check(c);
+  if (s) return s;
+  static const int comp[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+  for (int b = 0; b < c->nbins; b++)
+    for (int a = 0; a < 9; a++) D9[(size_t)b * 9 + a] = g[(size_t)b * 6 + comp[a]];
+  return BD_OK;
+}
 
 extern "C" int bd_load_grid(bd_ctx* c, int nt, const double* D9) {
   if (!c || !D9 || nt < 0 || nt >= c->p.nt_avg) return BD_ERR_ARG;

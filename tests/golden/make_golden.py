@@ -233,6 +233,17 @@ def sc_step(flow, nsteps=4):
                 tracks=np.array(tracks), nsteps=np.array(nsteps))
 
 
+def sc_grid(flow):
+    """gridHI's table for a small box (2 lattice frames), from the reference's
+    own gridHI main run in a scratch directory."""
+    import tempfile
+    import oracle as O
+    c_norm, edot = 0.6, 0.5
+    D, bins, geom = O.ref_grid(flow, 8, 6, c_norm, edot, 2, 2.0, tempfile.mkdtemp())
+    return dict(D=D, bins=bins, geom=geom, c_norm=np.array(c_norm), edot=np.array(edot),
+                nt_avg=np.array(2), bin_size=np.array(2.0))
+
+
 SCENARIOS = {}
 for f in (0, 1):
     fl = "shear" if f == 0 else "ext"
@@ -240,6 +251,7 @@ for f in (0, 1):
     SCENARIOS[f"noise_{fl}"] = (sc_noise, (f,))
     SCENARIOS[f"hop_{fl}"] = (sc_hop, (f,))
     SCENARIOS[f"step_{fl}"] = (sc_step, (f,))
+    SCENARIOS[f"grid_{fl}"] = (sc_grid, (f,))
     for t in (0, 2900):
         SCENARIOS[f"forces_{fl}_{t}"] = (sc_forces, (f, t))
         SCENARIOS[f"hi_{fl}_{t}"] = (sc_hi, (f, t))

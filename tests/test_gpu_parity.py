@@ -303,3 +303,28 @@ def test_charge_hop_vs_oracle_n500(flow):
         assert np.array_equal(c.hop_log(), log), sweep
         tr, od, _ = c.charges()
         assert np.array_equal(tr, track) and np.array_equal(od, old), sweep
+
+
+@pytest.mark.parametrize("name,flow", FLOWS)
+def test_grid_table_vs_reference(golden, name, flow):
+    g = golden(f"grid_{name}")
+    geom = g["geom"]
+    c = B.Context(B.make_params(flow, 8, 6, float(geom[0]), float(g["edot"]), 1e-3,
+                                nt_avg=int(g["nt_avg"]), bin_size=float(g["bin_size"]),
+                                box_volume=float(geom[1])))
+    c.build_grid(float(geom[5]))
+    for nt in range(int(g["nt_avg"])):
+        assert rel_err(c.grid(nt), g["D"][nt]) < TOL, nt
+
+
+@pytest.mark.parametrize("flow", [0, 1])
+def test_grid_table_vs_oracle_c1_geometry(flow):
+    """Box 30 at the bench's strain rate, all 8 frames, against the oracle."""
+    L, edot = 30.0, 3.37e-3
+    o = O.Oracle(flow, 25, 20, L, edot, 5e-4, nt_avg=8, bin_size=2.0)
+    D, bins = o.grid(0.001, L ** 3)
+    c = B.Context(B.make_params(flow, 25, 20, L, edot, 5e-4, nt_avg=8, bin_size=2.0))
+    c.build_grid(0.001)
+    assert np.array_equal(c.grid_shape()[:7], bins[:7])
+    for nt in range(8):
+        assert rel_err(c.grid(nt), D[nt]) < TOL, nt

@@ -164,3 +164,15 @@ def test_full_reference_steps(golden, name, flow):
         sim.step_hi(t, True)
         assert rel_err(np.stack([sim.x, sim.y, sim.z]), g["pos"][t]) < 1e-12, t
         assert np.array_equal(sim.track, g["tracks"][t]), t
+
+
+@pytest.mark.parametrize("name,flow", FLOWS)
+def test_grid_table(golden, name, flow):
+    """The restated gridHI against the reference's gridHI program."""
+    g = golden(f"grid_{name}")
+    geom = g["geom"]  # L box_volume bsx bsy bsz dt tp
+    o = O.Oracle(flow, 8, 6, float(geom[0]), float(g["edot"]), 5e-4, nt_avg=int(g["nt_avg"]),
+                 bin_size=float(g["bin_size"]))
+    D, bins = o.grid(float(geom[5]), float(geom[1]))
+    assert np.array_equal(bins, g["bins"])
+    assert np.array_equal(D, g["D"])
