@@ -234,14 +234,28 @@ class ClockSampler:
 # our path
 
 
-def build_context(w, seed, device_noise="philox"):
+PATHS = {
+    # north-star Brownian step: exact Ewald RPY mobility, Lanczos sqrt(M) z at
+    # tol 1e-6 with FP64 orthogonalisation; mobility tiles stored in FP32
+    # (products accumulated in FP64) or FP64
+    "lanczos32": dict(mobility="ewald", precision="fp32", step="lanczos", bytes_per_block=24),
+    "lanczos64": dict(mobility="ewald", precision="fp64", step="lanczos", bytes_per_block=48),
+    # the reference's own algorithm: hybrid mobility + CA-TEA displacement
+    "tea": dict(mobility="hybrid", precision="fp64", step="reference", bytes_per_block=48),
+}
+
+
+def build_context(w, seed, path="lanczos32", device_noise="philox"):
     import bd_b200 as B
     edot = edot_of(w)
     x, y, z, q, beta, C = synth_inputs(w, seed)
+    pp = PATHS[path]
     p = B.make_params(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
-                      noise=device_noise, philox_seed=seed, **force_params(w))
+                      noise=device_noise, philox_seed=seed, mobility=pp["mobility"],
+                      precision=pp["precision"], lanczos_tol=1e-6, **force_params(w))
     c = B.Context(p)
-    c.build_grid(0.001)
+    if pp["mobility"] == "hybrid":
+        c.build_grid(0.001)
     for sb in range(21):
         c.set_tea(sb, beta[sb], C[sb])
     c.set_positions(x, y, z)
@@ -263,88 +277,114 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def run_ours(args, rank, world, dist):
+def measure(w, path, K, W, rank, dist, e2e_steps):
+    """Times K steps of one path after W warm-up steps; returns a dict."""
     import torch
-    w = WORKLOADS[args.workload]
     N = w["Nb"] * w["Nc"]
-    dev = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(dev)
-    c = build_context(w, 1000 + rank)
-    K, W = args.steps, args.warmup
-    c.step_reference(0, W, True)
+    pp = PATHS[path]
+    c = build_context(w, 1000 + rank, path)
+    step = c.step_lanczos if pp["step"] == "lanczos" else c.step_reference
+    step(0, W, True)
     c.sync()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    lan0 = c.lanczos_stats()
     c.profile(True)
     n0 = c.launches()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
     with ClockSampler(dev) as clk:
-        c.step_reference(W, K, True)
+        step(W, K, True)
         c.sync()
     launches = c.launches() - n0
-    step_ms, _ = c.profile_read(c.PROF_STEP)
-    mv_ms, mv_n = c.profile_read(c.PROF_MATVEC)
-    hi_ms, hi_n = c.profile_read(c.PROF_HI_BUILD)
-    hop_ms, hop_n = c.profile_read(c.PROF_HOP)
-    f_ms, f_n = c.profile_read(c.PROF_FORCES)
+    prof = {k: c.profile_read(getattr(c, "PROF_" + k)) for k in
+            ("STEP", "MATVEC", "HI_BUILD", "HOP", "FORCES")}
     c.profile(False)
+    lan1 = c.lanczos_stats()
+    step_ms = prof["STEP"][0]
     t_max = step_ms
     if dist:
         tt = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_max = float(tt.item())
-    value = world * N * K / (t_max / 1e3)
-
     # end to end through the C ABI with pinned host buffers: upload the
     # positions, one step, download the positions, every step
-    Ke = max(1, min(K, args.e2e_steps))
+    Ke = max(1, min(K, e2e_steps))
     hb = [torch.empty(N, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
-    hx = c.positions()
-    for a, b in zip(hb, hx):
+    for a, b in zip(hb, c.positions()):
         a[:] = b
     c.sync()
     t0 = time.perf_counter()
     for t in range(W + K, W + K + Ke):
         c.set_positions(*hb)
-        c.step_reference(t, 1, True)
-        out = c.positions()
-        for a, b in zip(hb, out):
+        step(t, 1, True)
+        for a, b in zip(hb, c.positions()):
             a[:] = b
     e2e_s = time.perf_counter() - t0
     if dist:
         tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    e2e = {"value": world * N * Ke / e2e_s, "unit": "bead-steps/s",
-           "h2d_bytes_per_step": 3 * 8 * N, "d2h_bytes_per_step": 3 * 8 * N, "steps": Ke}
-
-    # roofline of the dominant kernel: packed symmetric mobility product,
-    # algorithmic bytes = 6 FP64 per off-diagonal block of the upper triangle
-    # + two right-hand sides in and two partial outputs
-    alg_bytes = 48.0 * N * (N - 1) / 2 + 4 * 3 * N * 8
+    mv_ms, mv_n = prof["MATVEC"]
+    alg_bytes = pp["bytes_per_block"] * N * (N - 1) / 2 + 4 * 3 * N * 8
     avg_ms = mv_ms / max(mv_n, 1)
-    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    peak, kind = peaks()
-    roof = {"kernel": "k_sym_matvec2<double>", "bound": "hbm", "achieved": achieved,
-            "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
-            "launches": mv_n}
-    breakdown = {"matvec_ms": mv_ms, "mobility_build_ms": hi_ms, "mobility_builds": hi_n,
-                 "hop_sweep_ms": hop_ms, "hop_sweeps": hop_n, "forces_ms": f_ms,
-                 "step_total_ms": step_ms}
-    clocks = clk.summary()
-    line = {"metric": METRIC, "value": value, "unit": "bead-steps/s", "n_gpus": world,
-            "steps": K, "warmup": W, "ms_per_step": t_max / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["name"], "beads": N, "path": "reference mode: dense hybrid "
-                       "RPY mobility (Ewald near field + lookup far field) + CA-TEA noise, "
-                       "Philox Gaussians, sequential charge-hop sweep",
-                       "edot": edot_of(w), "tau_estimate": tau_estimate(w["Nb"]),
-                       "l2": "inputs larger than L2 (packed mobility 1.5 GB)",
-                       "parallelism": "replicas only" if world > 1 else "single GPU"},
-            "roofline": roof, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
-            "breakdown": breakdown}
+    iters = lan1["iterations"] - lan0["iterations"]
+    calls = lan1["calls"] - lan0["calls"]
+    out = dict(path=path, t_max_ms=t_max, launches=launches, clocks=clk.summary(),
+               e2e_s=e2e_s, e2e_steps=Ke, matvec_ms=mv_ms, matvec_launches=mv_n,
+               matvec_avg_ms=avg_ms, alg_bytes=alg_bytes,
+               achieved_gbs=alg_bytes / (avg_ms / 1e3) / 1e9 if mv_n else None,
+               lanczos_iters_per_step=(iters / calls) if calls else None,
+               lanczos_maxed=lan1["maxed"] - lan0["maxed"],
+               breakdown={"mobility_build_ms": prof["HI_BUILD"][0], "mobility_builds": prof["HI_BUILD"][1],
+                          "hop_sweep_ms": prof["HOP"][0], "hop_sweeps": prof["HOP"][1],
+                          "forces_ms": prof["FORCES"][0], "matvec_ms": mv_ms,
+                          "step_total_ms": step_ms})
     c.close()
+    return out
+
+
+def run_ours(args, rank, world, dist):
+    w = WORKLOADS[args.workload]
+    N = w["Nb"] * w["Nc"]
+    K, W = args.steps, args.warmup
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps)
+    value = world * N * K / (main["t_max_ms"] / 1e3)
+    peak, kind = peaks()
+    roof = {"kernel": "k_sym_matvec<%s>" % ("float" if PATHS[args.path]["precision"] == "fp32"
+                                             else "double"),
+            "bound": "hbm", "achieved": main["achieved_gbs"], "peak": peak, "peak_kind": kind,
+            "unit": "GB/s", "frac": (main["achieved_gbs"] or 0) / peak, "traffic": None,
+            "alg_bytes_per_launch": main["alg_bytes"], "avg_launch_ms": main["matvec_avg_ms"],
+            "launches": main["matvec_launches"]}
+    e2e = {"value": world * N * main["e2e_steps"] / main["e2e_s"], "unit": "bead-steps/s",
+           "h2d_bytes_per_step": 3 * 8 * N, "d2h_bytes_per_step": 3 * 8 * N,
+           "steps": main["e2e_steps"]}
+    line = {"metric": METRIC, "value": value, "unit": "bead-steps/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": main["t_max_ms"] / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if PATHS[args.path]["precision"] == "fp32" else "f64",
+            "data": "synthetic",
+            "config": {"workload": w["name"], "beads": N, "path": args.path,
+                       "mobility": "Ewald-summed RPY, every pair (dense packed tiles)",
+                       "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation",
+                       "preconditioner": "none",
+                       "lanczos_iters_per_step": main["lanczos_iters_per_step"],
+                       "lanczos_fallbacks": main["lanczos_maxed"],
+                       "edot": edot_of(w), "tau_estimate": tau_estimate(w["Nb"]),
+                       "l2": "inputs larger than L2 (packed mobility tiles >> 126 MB)",
+                       "parallelism": "replicas only" if world > 1 else "single GPU"},
+            "roofline": roof, "e2e": e2e, "clocks": main["clocks"],
+            "gpu_launches": main["launches"], "breakdown": main["breakdown"]}
+    if args.compare and args.path != "lanczos64":
+        ref64 = measure(w, "lanczos64", K, W, rank, dist, 1)
+        line["plain_fp64"] = {"value": world * N * K / (ref64["t_max_ms"] / 1e3),
+                              "ms_per_step": ref64["t_max_ms"] / K,
+                              "lanczos_iters_per_step": ref64["lanczos_iters_per_step"],
+                              "matvec_gbs": ref64["achieved_gbs"]}
+        line["speedup_vs_plain_fp64"] = line["value"] / line["plain_fp64"]["value"]
     return line
 
 
@@ -357,6 +397,9 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--path", choices=sorted(PATHS), default="lanczos32")
+    ap.add_argument("--compare", type=int, default=1,
+                    help="also time the plain FP64 Krylov path (reported as plain_fp64)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

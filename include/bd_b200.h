@@ -51,6 +51,13 @@ typedef enum { BD_FLOW_SHEAR = 0, BD_FLOW_EXT = 1 } bd_flow;
  * ran1/gasdev stream (bit-identical, one device thread) or counter-based
  * Philox4x32-10 Gaussians (parallel; the production source). */
 typedef enum { BD_NOISE_RAN1 = 0, BD_NOISE_PHILOX = 1 } bd_noise;
+/* Pair mobility: the reference's hybrid (Ewald sum below a minimum-image
+ * distance of 12, lookup table beyond, shear/src/main26.c:1714-1794) or the
+ * Ewald sum for every pair. */
+typedef enum { BD_MOB_HYBRID = 0, BD_MOB_EWALD = 1 } bd_mobility_kind;
+/* Storage of the packed mobility tiles used by the products: FP64, or FP32
+ * with FP64 accumulation. */
+typedef enum { BD_PREC_FP64 = 0, BD_PREC_FP32 = 1 } bd_precision;
 typedef enum { BD_SPRING_HOOKEAN = 0, BD_SPRING_FENE = 1 } bd_spring;
 
 /* System parameters.  The names follow the reference's globals
@@ -82,6 +89,10 @@ typedef struct {
   long seed;                 /* ran1 seed (fixSeed=1: 830062920 shear, 981272199 ext) */
   int noise;                 /* bd_noise */
   unsigned long long philox_seed;
+  int mobility;              /* bd_mobility_kind */
+  int precision;             /* bd_precision */
+  double lanczos_tol;        /* relative change of sqrt(M) z between iterations; 0 -> 1e-6 */
+  int lanczos_max;           /* Krylov dimension cap; 0 -> 80 */
 } bd_params;
 
 typedef struct bd_ctx bd_ctx;
@@ -184,6 +195,25 @@ int bd_profile_enable(bd_ctx *ctx, int on); /* clears the accumulated events */
 int bd_profile_read(bd_ctx *ctx, int slot, double *total_ms, long *count);
 /* Number of kernels the library has launched on this context. */
 long long bd_launch_count(const bd_ctx *ctx);
+
+/* ---- Krylov Brownian displacement (no reference counterpart: the
+ * reference's noise is the conformationally averaged TEA approximation of
+ * updateHI, shear/src/main26.c:745-857) ----------------------------------- */
+/* out = M v for a host vector v[3N] (bead-interleaved), using the mobility of
+ * the last bd_calc_hi (diagonal blocks included). */
+int bd_mobility_apply(bd_ctx *ctx, const double *v, double *out);
+/* out = sqrt(M) z by Lanczos with full FP64 reorthogonalisation, stopped when
+ * the relative change between successive iterates is below lanczos_tol;
+ * *iters receives the Krylov dimension used. */
+int bd_lanczos_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
+/* calls, total Krylov iterations, calls that hit lanczos_max, negative Ritz
+ * values clamped (a hybrid mobility need not be positive definite) */
+int bd_lanczos_stats(bd_ctx *ctx, long *out4);
+/* One Brownian-dynamics step with the Krylov displacement
+ * dr = dt M F + sqrt(2 dt) M^(1/2) z + dt u(r): the reference's step order
+ * (lattice, PBC, neighbour check, forces, mobility rebuild every srpy steps,
+ * charge hop every MStep steps) with Philox z; repeated nsteps times. */
+int bd_step_lanczos(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 
 /* One reference-mode hydrodynamic step (the body of the step loop,
  * shear/src/main26.c:65-151, extensional/src/main14.c:68-171, without file

@@ -551,8 +551,25 @@ static void kvectors(const bdo_sys *s, double boxvol, double rkkcut, double rkcu
  * nbins 3x3 tensors.  M is row-major 9 N^2 (block (i,j) at 9N i + 9 j);
  * only the upper blocks and the diagonal entries of the diagonal blocks are
  * written, as in the reference. */
+static void calc_hi_impl(const bdo_sys *s, const double *rx, const double *ry,
+                         const double *rz, const double *grid, double *M, int all_pairs);
+
 void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
                  const double *rz, const double *grid, double *M) {
+  calc_hi_impl(s, rx, ry, rz, grid, M, 0);
+}
+
+/* The Ewald-summed RPY tensor for every pair (no lookup table) with the self
+ * term summed over every image but the origin and its zz entry from dz --
+ * the project's exact-mobility mode, which has no counterpart in the
+ * reference; it shares calcHI's Ewald split and sums. */
+void bdo_calc_hi_ewald(const bdo_sys *s, const double *rx, const double *ry,
+                       const double *rz, double *M) {
+  calc_hi_impl(s, rx, ry, rz, NULL, M, 1);
+}
+
+static void calc_hi_impl(const bdo_sys *s, const double *rx, const double *ry,
+                         const double *rz, const double *grid, double *M, int all_pairs) {
   int N = s->N;
   double L = s->L, boxvol = L * L * L;
   int treal = (int)(s->t % (unsigned long)s->tp);
@@ -587,7 +604,7 @@ void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
   for (int nx = -nmax; nx < nmax + 1; nx++)
     for (int ny = -nmax; ny < nmax + 1; ny++)
       for (int nz = -nmax; nz < nmax + 1; nz++)
-        if (nx != 0 && ny != 0 && nz != 0) {
+        if (all_pairs ? (nx != 0 || ny != 0 || nz != 0) : (nx != 0 && ny != 0 && nz != 0)) {
           double dx = nx * L1[0] + ny * L2[0], dy = nx * L1[1] + ny * L2[1], dz = nz * L;
           double rr = dx * dx + dy * dy + dz * dz, r = sqrt(rr);
           double C1 = 0.75 / r + 0.5 / (r * rr);
@@ -598,7 +615,7 @@ void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
           double t2 = C3 * erfc(alpha * r) + C4 * exp(-alpha2 * rr) / rtpi;
           Dtr[0] += t1 + t2 * dx * dx / rr;
           Dtr[1] += t1 + t2 * dy * dy / rr;
-          Dtr[2] += t1 + t2 * dy * dy / rr;
+          Dtr[2] += t1 + t2 * (all_pairs ? dz * dz : dy * dy) / rr;
         }
   for (int i = 0; i < N; i++) {
     size_t st = (size_t)9 * N * i + 9 * i;
@@ -628,7 +645,7 @@ void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
       double bm[3];
       bdo_nidbin(s, rx, ry, rz, j, i, bm);
       double dmin = sqrt(bm[0] * bm[0] + bm[1] * bm[1] + bm[2] * bm[2]);
-      if (dmin < 12.0) {
+      if (all_pairs || dmin < 12.0) {
         double Dt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         double dxo = rxj - rxi, dyo = ryj - ryi, dzo = rz[j] - rz[i];
         for (int nx = -nmax; nx < nmax + 1; nx++)

@@ -74,6 +74,8 @@ int bdo_check_verlet(const bdo_sys *s, const double *dxv, const double *dyv,
                      const double *dzv);
 void bdo_calc_hi(const bdo_sys *s, const double *rx, const double *ry,
                  const double *rz, const double *grid, double *M);
+void bdo_calc_hi_ewald(const bdo_sys *s, const double *rx, const double *ry,
+                       const double *rz, double *M);
 void bdo_grid_geom(const bdo_sys *s, double grid_dt, int *geom);
 void bdo_grid(const bdo_sys *s, double grid_dt, double boxvol, double *D, int *geom);
 void bdo_update_hi(const bdo_sys *s, double *rx, double *ry, double *rz,

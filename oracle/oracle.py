@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
         L.bdo_check_verlet.argtypes = [sp, _dp, _dp, _dp]
         L.bdo_calc_hi.argtypes = [sp, _dp, _dp, _dp, _dp, _dp]
         L.bdo_grid.argtypes = [sp, C.c_double, C.c_double, _dp, _ip]
+        L.bdo_calc_hi_ewald.argtypes = [sp, _dp, _dp, _dp, _dp]
         L.bdo_grid_geom.argtypes = [sp, C.c_double, _ip]
         L.bdo_update_hi.argtypes = [sp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                     C.c_double, _dp]
@@ -155,6 +156,11 @@ class Oracle:
     def calc_hi(self, x, y, z, grid):
         M = np.zeros(9 * self.N * self.N)
         lib().bdo_calc_hi(C.byref(self.s), x, y, z, np.ascontiguousarray(grid, dtype=np.float64), M)
+        return M
+
+    def calc_hi_ewald(self, x, y, z):
+        M = np.zeros(9 * self.N * self.N)
+        lib().bdo_calc_hi_ewald(C.byref(self.s), x, y, z, M)
         return M
 
     def grid(self, grid_dt=0.001, box_volume=None):
@@ -415,3 +421,24 @@ def ref_grid(flow, Nb, Nc, c_norm, edot, nt_avg, bin_size, workdir):
         lib_.hg_D(nt, row)
         D[nt] = row
     return D, bins, geom
+
+
+def full_mobility(M9, N):
+    """The symmetric 3N x 3N matrix from the reference layout (upper blocks and
+    the diagonal entries of the diagonal blocks filled): block (j, i) = block
+    (i, j), whose 3x3 blocks are symmetric."""
+    B = M9.reshape(N, N, 3, 3).copy()
+    iu = np.triu_indices(N, 1)
+    up = B[iu]
+    B[(iu[1], iu[0])] = up
+    for i in range(N):
+        d = np.diag(B[i, i]).copy()
+        B[i, i] = np.diag(d)
+    return B.transpose(0, 2, 1, 3).reshape(3 * N, 3 * N)
+
+
+def sqrtm_apply(Mfull, z):
+    """sqrt(M) z by a dense eigendecomposition (numpy eigh), negative
+    eigenvalues clamped to zero; also returns the smallest eigenvalue."""
+    w, Q = np.linalg.eigh(Mfull)
+    return Q @ (np.sqrt(np.clip(w, 0, None)) * (Q.T @ z)), float(w.min())

@@ -23,7 +23,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
-SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu"]
+SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -63,6 +63,8 @@ class Params(C.Structure):
         ("nt_avg", C.c_int), ("bin_size", C.c_double), ("srpy", C.c_int), ("sbins", C.c_int),
         ("strain_ss", C.c_double), ("max_neighbors", C.c_int), ("seed", C.c_long),
         ("noise", C.c_int), ("philox_seed", C.c_ulonglong),
+        ("mobility", C.c_int), ("precision", C.c_int), ("lanczos_tol", C.c_double),
+        ("lanczos_max", C.c_int),
     ]
 
 
@@ -121,6 +123,10 @@ def _lib() -> C.CDLL:
         L.bd_download_mobility.argtypes = [vp, _dp]
         L.bd_download_hop_log.argtypes = [vp, _ip]
         L.bd_step_reference.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
+        L.bd_mobility_apply.argtypes = [vp, _dp, _dp]
+        L.bd_lanczos_sqrt.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
+        L.bd_lanczos_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        L.bd_step_lanczos.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
         L.bd_profile_enable.argtypes = [vp, C.c_int]
         L.bd_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
         L.bd_launch_count.argtypes = [vp]
@@ -145,7 +151,8 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
                 epsilon=1.0, lambda_b=2.0, lambda_d=5.0, Ncharges=0, barrier=3.0, barrier2=3.0,
                 MStep=100, nt_avg=8, bin_size=2.0, srpy=100, sbins=20, strain_ss=10.0,
                 max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0,
-                noise="ran1", philox_seed=20261203) -> Params:
+                noise="ran1", philox_seed=20261203, mobility="hybrid", precision="fp64",
+                lanczos_tol=1e-6, lanczos_max=80) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
     p.box_volume = box_volume
@@ -159,6 +166,9 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
     p.seed = (830062920 if flow == FLOW_SHEAR else 981272199) if seed is None else seed
     p.noise = NOISE_PHILOX if noise == "philox" else NOISE_RAN1
     p.philox_seed = philox_seed
+    p.mobility = 1 if mobility == "ewald" else 0
+    p.precision = 1 if precision == "fp32" else 0
+    p.lanczos_tol, p.lanczos_max = lanczos_tol, lanczos_max
     return p
 
 
@@ -298,6 +308,25 @@ class Context:
         o = np.zeros(3 * max(n, 1), np.int32)
         self._call("bd_download_hop_log", o)
         return o.reshape(-1, 3)[:n]
+
+    def mobility_apply(self, v):
+        out = np.zeros(3 * self.N)
+        self._call("bd_mobility_apply", np.ascontiguousarray(v, np.float64), out)
+        return out
+
+    def lanczos_sqrt(self, z):
+        out = np.zeros(3 * self.N)
+        it = C.c_int()
+        self._call("bd_lanczos_sqrt", np.ascontiguousarray(z, np.float64), out, C.byref(it))
+        return out, it.value
+
+    def lanczos_stats(self):
+        o = np.zeros(4, np.int64)
+        self._call("bd_lanczos_stats", o)
+        return dict(calls=int(o[0]), iterations=int(o[1]), maxed=int(o[2]), negative=int(o[3]))
+
+    def step_lanczos(self, t0, nsteps, with_hop=True):
+        self._call("bd_step_lanczos", int(t0), int(nsteps), int(bool(with_hop)))
 
     def step_reference(self, t0, nsteps, with_hop=True):
         self._call("bd_step_reference", int(t0), int(nsteps), int(bool(with_hop)))

@@ -582,6 +582,11 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   c->strain_ss = p->strain_ss > 0 ? p->strain_ss : 10.0;
   c->strain_interval = c->strain_ss / c->sbins;
   c->maxnb = p->max_neighbors > 0 ? p->max_neighbors : 256;
+  if (p->lanczos_max > 120 || p->mobility < 0 || p->mobility > 1 || p->precision < 0 ||
+      p->precision > 1) {
+    bd_destroy(c);
+    return BD_ERR_ARG;
+  }
   // lookup-grid geometry (initLattice, shear/src/Initialization.c:244-295,
   // extensional/src/Initialization.c:252-285)
   {
@@ -676,7 +681,7 @@ int bd_destroy(bd_ctx* c) {
                   c->dE, c->rng, c->nb_count, c->nb_rows, c->nb_half, c->cell_of, c->cell_count,
                   c->cell_start, c->cell_beads, c->cell_cursor, c->Mt, c->tileI, c->grid,
                   c->near_pairs, c->near_count, c->kvec, c->rowpart, c->colpart, c->U, c->W,
-                  c->Ctab};
+                  c->Ctab, c->Mt32, c->LV, c->Lw, c->Lpart, c->Lh, c->Lsc, c->Lc, c->MF, c->Yz};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   prof_clear(c);

@@ -58,6 +58,7 @@ struct bd_ctx {
   int NT;
   size_t ntiles;
   double *Mt;
+  float *Mt32;   // FP32 copy of the tiles (BD_PREC_FP32), products accumulated in FP64
   int *tileI;  // tile row index of each packed tile
   double *grid;
   int grid_loaded_mask;
@@ -73,6 +74,20 @@ struct bd_ctx {
   std::vector<double> btab;
   double bt;
   int sbin;
+
+  // Krylov (Lanczos) square root
+  int lmax;
+  double ltol;
+  double *LV;     // (lmax+1) basis vectors, each 3 x NTp SoA (component-major, padded)
+  double *Lw;     // work vector, 3 x NTp
+  double *Lpart;  // per-block partial dots, (lmax+1) x kDotBlocks
+  double *Lh;     // dot results, lmax+1
+  double *Lsc;    // device scalars: [0] beta, [1] 1/beta
+  double *Lc;     // Ritz combination coefficients, lmax+1
+  double *MF;     // M F, 3 x NTp
+  double *Yz;     // sqrt(M) z, 3 x NTp
+  long long lan_calls, lan_iters, lan_maxed, lan_negative;
+  int lan_last;
 
   size_t bytes;
 
@@ -104,8 +119,18 @@ int alloc_mobility(bd_ctx* c);
 int calc_hi(bd_ctx* c);
 int update_hi(bd_ctx* c);
 int download_mobility(bd_ctx* c, double* M9);
+struct VecIn {
+  const double* p[3];  // component pointers: x_c(i) = p[c][i*stride]
+  int stride;
+};
+int sym_matvec(bd_ctx* c, int R, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1,
+               bool addiag);
 
 // charge hopping
 int charge_hop(bd_ctx* c);
+
+// Krylov square root
+int alloc_lanczos(bd_ctx* c);
+int lanczos_sqrt(bd_ctx* c, const double* zdev_interleaved, bool with_force, int* iters);
 
 }  // namespace bd

@@ -1,0 +1,416 @@
+// Krylov (Lanczos) square root of the mobility and the Brownian step built
+// on it.
+//
+// The reference draws its Brownian displacement with the conformationally
+// averaged truncated-expansion approximation (updateHI,
+// shear/src/main26.c:745-857).  This path computes sqrt(M) z itself:
+// Lanczos on M from v_1 = z/|z| with full reorthogonalisation in FP64
+// (classical Gram-Schmidt, applied twice), T_m = V_m^T M V_m tridiagonal,
+// sqrt(M) z ~= |z| V_m T_m^(1/2) e_1, stopped when the relative change of the
+// iterate between successive m is below the tolerance (the criterion of Ando,
+// Chow and Skolnick, J. Chem. Phys. 137, 064106 (2012)).  T_m^(1/2) e_1 comes
+// from an eigen-decomposition of T_m on the host by the implicit symmetric QR
+// iteration with Wilkinson shifts (Golub and Van Loan, Matrix Computations,
+// section 8.3).  Vectors live on the device in component-major SoA with the
+// tile padding (3 x NTp); every reduction is a fixed-order two-level sum.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bd_ctx.cuh"
+
+using namespace bd;
+
+#define CU(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
+  } while (0)
+
+static const int kDotBlocks = 148;  // one CTA per SM for the vector reductions
+
+// partial[k][b] = sum over block b's chunk of V_k . w   (grid: kDotBlocks x nv)
+__global__ void __launch_bounds__(256) k_multidot(const double* __restrict__ V, size_t vstride,
+                                                  const double* __restrict__ w, int n,
+                                                  double* part) {
+  int k = blockIdx.y;
+  const double* v = V + (size_t)k * vstride;
+  double s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += v[i] * w[i];
+  __shared__ double sh[8];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sh[q];
+    part[(size_t)k * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// out[k] (+)= sum_b part[k][b]; with acc the result is added to out.
+__global__ void k_reduce_parts(const double* __restrict__ part, int nblk, int nv, double* out,
+                               int acc) {
+  int k = threadIdx.x;
+  if (k >= nv) return;
+  double s = 0;
+  for (int b = 0; b < nblk; b++) s += part[(size_t)k * nblk + b];
+  out[k] = acc ? out[k] + s : s;
+}
+
+// w -= sum_{k < nv} h[k] V_k
+__global__ void k_sub_combo(const double* __restrict__ V, size_t vstride,
+                            const double* __restrict__ h, int nv, double* w, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int k = 0; k < nv; k++) s += h[k] * V[(size_t)k * vstride + i];
+    w[i] -= s;
+  }
+}
+
+// sc[0] = sqrt(sum of part) = |w|, sc[1] = 1/|w|
+__global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc) {
+  if (threadIdx.x) return;
+  double s = 0;
+  for (int b = 0; b < nblk; b++) s += part[b];
+  sc[0] = sqrt(s);
+  sc[1] = sc[0] > 0 ? 1.0 / sc[0] : 0.0;
+}
+
+__global__ void k_scale_into(const double* __restrict__ w, const double* __restrict__ sc,
+                             double* v, int n) {
+  double f = sc[1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i] = w[i] * f;
+}
+
+// v (SoA, padded) = z (bead-interleaved) / |z|; padding entries are zero
+__global__ void k_interleaved_to_soa(const double* __restrict__ z, const double* __restrict__ sc,
+                                     double* v, int N, int NTp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NTp) return;
+  double f = sc[1];
+  for (int a = 0; a < 3; a++) v[(size_t)a * NTp + i] = i < N ? z[3 * i + a] * f : 0.0;
+}
+
+// y = scale * sum_k c[k] V_k
+__global__ void k_combo(const double* __restrict__ V, size_t vstride,
+                        const double* __restrict__ c, int nv, double scale, double* y, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int k = 0; k < nv; k++) s += c[k] * V[(size_t)k * vstride + i];
+    y[i] = scale * s;
+  }
+}
+
+// |z|^2 partials over the bead-interleaved noise
+__global__ void __launch_bounds__(256) k_sumsq(const double* __restrict__ z, int n, double* part) {
+  double s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += z[i] * z[i];
+  __shared__ double sh[8];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sh[q];
+    part[blockIdx.x] = t;
+  }
+}
+
+// Brownian step with the Krylov displacement: dr = dt M F + sqrt(2 dt) y
+// + dt u(r), u = edot (y, 0, 0) in shear, edot (x, -y, 0) in extension
+// (the flow terms of updateHI, shear/src/main26.c:846-847,
+// extensional/src/main14.c:885-886); also accumulates dxv for the Verlet check.
+__global__ void k_krylov_update(int flow, double* rx, double* ry, double* rz, double* dxv,
+                                double* dyv, double* dzv, const double* __restrict__ MF,
+                                const double* __restrict__ Y, int NTp, int N, double dt,
+                                double edot, double sq2dt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double du[3];
+  for (int a = 0; a < 3; a++) du[a] = dt * MF[(size_t)a * NTp + i] + sq2dt * Y[(size_t)a * NTp + i];
+  if (flow == 0) {
+    du[0] += dt * edot * ry[i];
+  } else {
+    du[0] += dt * edot * rx[i];
+    du[1] -= dt * edot * ry[i];
+  }
+  dxv[i] += du[0];
+  rx[i] += du[0];
+  dyv[i] += du[1];
+  ry[i] += du[1];
+  dzv[i] += du[2];
+  rz[i] += du[2];
+}
+
+// ---------------------------------------------------------------------------
+// host: symmetric tridiagonal eigen-decomposition
+
+// Implicit symmetric QR with Wilkinson shifts on T = tridiag(e, d, e)
+// (Golub & Van Loan, Alg. 8.3.2/8.3.3).  d[n] diagonal, e[n-1] off-diagonal;
+// on return d holds the eigenvalues and Z (n x n, Z[i*n+k] = component i of
+// eigenvector k) the orthonormal eigenvectors.
+static void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e,
+                        std::vector<double>& Z) {
+  Z.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) Z[(size_t)i * n + i] = 1.0;
+  if (n == 1) return;
+  e.resize(n, 0.0);
+  int hi = n - 1, guard = 0;
+  while (hi > 0 && guard < 60 * n) {
+    guard++;
+    // deflate negligible off-diagonals
+    for (int i = 0; i < hi; i++)
+      if (fabs(e[i]) <= 1e-15 * (fabs(d[i]) + fabs(d[i + 1]))) e[i] = 0.0;
+    while (hi > 0 && e[hi - 1] == 0.0) hi--;
+    if (hi == 0) break;
+    int lo = hi - 1;
+    while (lo > 0 && e[lo - 1] != 0.0) lo--;
+    // Wilkinson shift from the trailing 2x2 block
+    double dd = 0.5 * (d[hi - 1] - d[hi]);
+    double b2 = e[hi - 1] * e[hi - 1];
+    double mu = d[hi] - b2 / (dd + (dd >= 0 ? 1.0 : -1.0) * sqrt(dd * dd + b2));
+    double x = d[lo] - mu, z = e[lo], bulge = 0.0;
+    for (int k = lo; k < hi; k++) {
+      double r = hypot(x, z);
+      double cs = r > 0 ? x / r : 1.0, sn = r > 0 ? -z / r : 0.0;
+      if (k > lo) e[k - 1] = r;
+      double a = d[k], b = e[k], c2 = d[k + 1];
+      // R^T T R on rows/columns k, k+1 with R = [[cs, sn], [-sn, cs]]
+      d[k] = cs * cs * a - 2 * cs * sn * b + sn * sn * c2;
+      d[k + 1] = sn * sn * a + 2 * cs * sn * b + cs * cs * c2;
+      e[k] = cs * sn * a + (cs * cs - sn * sn) * b - cs * sn * c2;
+      if (k + 1 < hi) {
+        bulge = -sn * e[k + 1];
+        e[k + 1] = cs * e[k + 1];
+        x = e[k];
+        z = bulge;
+      }
+      for (int i = 0; i < n; i++) {
+        double zk = Z[(size_t)i * n + k], zk1 = Z[(size_t)i * n + k + 1];
+        Z[(size_t)i * n + k] = cs * zk - sn * zk1;
+        Z[(size_t)i * n + k + 1] = sn * zk + cs * zk1;
+      }
+    }
+  }
+}
+
+// c = T^(1/2) e_1 for T = tridiag(beta, alpha, beta) of size m; negative
+// Ritz values are clamped to zero and counted.
+static int sqrt_e1(const std::vector<double>& alpha, const std::vector<double>& beta, int m,
+                   std::vector<double>& c) {
+  std::vector<double> d(alpha.begin(), alpha.begin() + m), e(beta.begin(), beta.begin() + (m - 1));
+  std::vector<double> Z;
+  tridiag_eig(m, d, e, Z);
+  int neg = 0;
+  c.assign(m, 0.0);
+  for (int k = 0; k < m; k++) {
+    double lam = d[k];
+    if (lam < 0) {
+      neg++;
+      lam = 0;
+    }
+    double w = sqrt(lam) * Z[(size_t)0 * m + k];
+    for (int i = 0; i < m; i++) c[i] += Z[(size_t)i * m + k] * w;
+  }
+  return neg;
+}
+
+namespace bd {
+
+int alloc_lanczos(bd_ctx* c) {
+  if (c->LV) return BD_OK;
+  c->lmax = c->p.lanczos_max > 0 ? c->p.lanczos_max : 80;
+  c->ltol = c->p.lanczos_tol > 0 ? c->p.lanczos_tol : 1e-6;
+  size_t n = 3 * (size_t)c->NT * 32;
+  CU(cudaMalloc(&c->LV, 8 * n * (c->lmax + 1)));
+  CU(cudaMalloc(&c->Lw, 8 * n));
+  CU(cudaMalloc(&c->Lpart, 8 * (size_t)(c->lmax + 1) * kDotBlocks));
+  CU(cudaMalloc(&c->Lh, 8 * (size_t)(c->lmax + 1)));
+  CU(cudaMalloc(&c->Lsc, 8 * 8));
+  CU(cudaMalloc(&c->Lc, 8 * (size_t)(c->lmax + 1)));
+  CU(cudaMalloc(&c->MF, 8 * n));
+  CU(cudaMalloc(&c->Yz, 8 * n));
+  c->bytes += 8 * n * (c->lmax + 4) + 8 * (size_t)(c->lmax + 1) * (kDotBlocks + 2) + 64;
+  return BD_OK;
+}
+
+// sqrt(M) z for the bead-interleaved z on the device (c->R): result in c->Yz.
+// With with_force the first product also forms M F into c->MF.
+int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
+  int s;
+  if (!c->hi_built) return BD_ERR_STATE;
+  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  int N = c->N, NTp = c->NT * 32, n = 3 * NTp, blk = kDotBlocks;
+  size_t vs = (size_t)n;
+  cudaStream_t st = c->stream;
+  // |z| and v_0
+  c->launches += 3;
+  k_sumsq<<<blk, 256, 0, st>>>(z, 3 * N, c->Lpart);
+  k_norm_fin<<<1, 32, 0, st>>>(c->Lpart, blk, c->Lsc);
+  k_interleaved_to_soa<<<(NTp + 255) / 256, 256, 0, st>>>(z, c->Lsc, c->LV, N, NTp);
+  double zn = 0;
+  CU(cudaMemcpyAsync(&zn, c->Lsc, 8, cudaMemcpyDeviceToHost, st));
+  std::vector<double> alpha, beta, cc, cprev;
+  int m = 0, neg = 0;
+  bool conv = false;
+  for (int j = 0; j < c->lmax; j++) {
+    double* vj = c->LV + (size_t)j * vs;
+    VecIn vin_j = {{vj, vj + NTp, vj + 2 * NTp}, 1};
+    if (j == 0 && with_force) {
+      VecIn vf = {{c->fx, c->fy, c->fz}, 1};
+      if ((s = sym_matvec(c, 2, vf, vin_j, c->MF, c->Lw, true)) != BD_OK) return s;
+    } else {
+      if ((s = sym_matvec(c, 1, vin_j, vin_j, c->Lw, c->Lw, true)) != BD_OK) return s;
+    }
+    int nv = j + 1;
+    // two passes of classical Gram-Schmidt against V_0..V_j
+    for (int pass = 0; pass < 2; pass++) {
+      c->launches += 3;
+      k_multidot<<<dim3(blk, nv), 256, 0, st>>>(c->LV, vs, c->Lw, n, c->Lpart);
+      k_reduce_parts<<<1, 128, 0, st>>>(c->Lpart, blk, nv, c->Lh + 0, 0);
+      // keep alpha_j = h_j of both passes in Lc[j] (scratch) via accumulate
+      k_sub_combo<<<blk * 2, 256, 0, st>>>(c->LV, vs, c->Lh, nv, c->Lw, n);
+      if (pass == 0)
+        CU(cudaMemcpyAsync(c->Lc + j, c->Lh + j, 8, cudaMemcpyDeviceToDevice, st));
+      else {
+        c->launches++;
+        k_reduce_parts<<<1, 1, 0, st>>>(c->Lh + j, 1, 1, c->Lc + j, 1);
+      }
+    }
+    c->launches += 2;
+    k_multidot<<<dim3(blk, 1), 256, 0, st>>>(c->Lw, vs, c->Lw, n, c->Lpart);
+    k_norm_fin<<<1, 32, 0, st>>>(c->Lpart, blk, c->Lsc);
+    double ab[2];
+    CU(cudaMemcpyAsync(&ab[0], c->Lc + j, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(&ab[1], c->Lsc, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    alpha.push_back(ab[0]);
+    beta.push_back(ab[1]);
+    m = j + 1;
+    neg = sqrt_e1(alpha, beta, m, cc);
+    if (m >= 2) {
+      double dn = 0, cn = 0;
+      for (int i = 0; i < m; i++) {
+        double prev = i < m - 1 ? cprev[i] : 0.0;
+        dn += (cc[i] - prev) * (cc[i] - prev);
+        cn += cc[i] * cc[i];
+      }
+      if (sqrt(dn) <= c->ltol * sqrt(cn)) {
+        conv = true;
+        break;
+      }
+    }
+    cprev = cc;
+    if (ab[1] <= 1e-300) {  // invariant subspace: exact
+      conv = true;
+      break;
+    }
+    if (j + 1 < c->lmax) {
+      c->launches++;
+      k_scale_into<<<blk * 2, 256, 0, st>>>(c->Lw, c->Lsc, c->LV + (size_t)(j + 1) * vs, n);
+    }
+  }
+  CU(cudaMemcpyAsync(c->Lc, cc.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, st));
+  c->launches++;
+  k_combo<<<blk * 2, 256, 0, st>>>(c->LV, vs, c->Lc, m, zn, c->Yz, n);
+  c->lan_calls++;
+  c->lan_iters += m;
+  c->lan_last = m;
+  if (!conv) c->lan_maxed++;
+  c->lan_negative += neg;
+  if (iters) *iters = m;
+  CU(cudaStreamSynchronize(st));  // cc is a host vector read by the copy above
+  return launch_ok(c);
+}
+
+}  // namespace bd
+
+extern "C" {
+
+int bd_mobility_apply(bd_ctx* c, const double* v, double* out) {
+  if (!c || !v || !out) return BD_ERR_ARG;
+  if (!c->hi_built) return BD_ERR_STATE;
+  int s;
+  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  int N = c->N, NTp = c->NT * 32;
+  std::vector<double> soa(3 * (size_t)NTp, 0.0), res(3 * (size_t)NTp);
+  for (int i = 0; i < N; i++)
+    for (int a = 0; a < 3; a++) soa[(size_t)a * NTp + i] = v[3 * i + a];
+  CU(cudaMemcpyAsync(c->Lw, soa.data(), 8 * soa.size(), cudaMemcpyHostToDevice, c->stream));
+  VecIn vi = {{c->Lw, c->Lw + NTp, c->Lw + 2 * NTp}, 1};
+  if ((s = sym_matvec(c, 1, vi, vi, c->Yz, c->Yz, true)) != BD_OK) return s;
+  CU(cudaMemcpyAsync(res.data(), c->Yz, 8 * res.size(), cudaMemcpyDeviceToHost, c->stream));
+  if ((s = check(c)) != BD_OK) return s;
+  for (int i = 0; i < N; i++)
+    for (int a = 0; a < 3; a++) out[3 * i + a] = res[(size_t)a * NTp + i];
+  return BD_OK;
+}
+
+int bd_lanczos_sqrt(bd_ctx* c, const double* z, double* out, int* iters) {
+  if (!c || !z || !out) return BD_ERR_ARG;
+  int s;
+  CU(cudaMemcpyAsync(c->R, z, 24 * (size_t)c->N, cudaMemcpyHostToDevice, c->stream));
+  if ((s = lanczos_sqrt(c, c->R, false, iters)) != BD_OK) return s;
+  int N = c->N, NTp = c->NT * 32;
+  std::vector<double> res(3 * (size_t)NTp);
+  CU(cudaMemcpyAsync(res.data(), c->Yz, 8 * res.size(), cudaMemcpyDeviceToHost, c->stream));
+  if ((s = check(c)) != BD_OK) return s;
+  for (int i = 0; i < N; i++)
+    for (int a = 0; a < 3; a++) out[3 * i + a] = res[(size_t)a * NTp + i];
+  return BD_OK;
+}
+
+int bd_lanczos_stats(bd_ctx* c, long* o) {
+  if (!c || !o) return BD_ERR_ARG;
+  o[0] = (long)c->lan_calls;
+  o[1] = (long)c->lan_iters;
+  o[2] = (long)c->lan_maxed;
+  o[3] = (long)c->lan_negative;
+  return BD_OK;
+}
+
+int bd_step_lanczos(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
+  if (!c || nsteps < 0) return BD_ERR_ARG;
+  int s;
+  bool ext = c->p.flow == BD_FLOW_EXT;
+  prof_begin(c, BD_PROF_STEP);
+  for (int n = 0; n < nsteps; n++) {
+    unsigned long t = t0 + (unsigned long)n;
+    c->t = t;
+    if ((s = bd_reset_force(c))) return s;
+    c->strain = (double)t * c->p.dt * c->p.edot;
+    host_lattice(c, t, &c->lat);
+    if (ext && (s = bd_transform_coords(c))) return s;
+    if ((s = bd_apply_pbc(c))) return s;
+    if ((s = build_neighbors(c, false))) return s;
+    prof_begin(c, BD_PROF_FORCES);
+    if ((s = bd_bond_force(c))) return s;
+    if ((s = bd_ev_force(c))) return s;
+    if ((s = bd_coulomb_force(c))) return s;
+    prof_end(c, BD_PROF_FORCES);
+    if ((s = bd_get_noise(c))) return s;
+    if (t % (unsigned long)c->srpy == 0 || t == c->tstart || !c->hi_built)
+      if ((s = calc_hi(c))) return s;
+    if (ext) rotate_coords(c, 1);
+    if ((s = lanczos_sqrt(c, c->R, true, nullptr))) return s;
+    c->launches++;
+    k_krylov_update<<<(c->N + 255) / 256, 256, 0, c->stream>>>(
+        c->p.flow, c->rx, c->ry, c->rz, c->dxv, c->dyv, c->dzv, c->MF, c->Yz, c->NT * 32, c->N,
+        c->p.dt, c->p.edot, sqrt(2.0 * c->p.dt));
+    if (with_hop && c->nch > 0 && t % (unsigned long)c->p.MStep == 0) {
+      if (ext && (s = bd_transform_coords(c))) return s;
+      if ((s = charge_hop(c))) return s;
+      if (ext && (s = bd_inverse_coords(c))) return s;
+    }
+  }
+  prof_end(c, BD_PROF_STEP);
+  return check(c);
+}
+
+}  // extern "C"

@@ -222,6 +222,85 @@ __device__ __forceinline__ void near_pair(const Lat& l, const Ewald& ew,
   }
 }
 
+// Ewald-summed RPY tensor for every pair (BD_MOB_EWALD): one CTA per packed
+// tile, one lane per pair; the lane sums the real-space images and the k-space
+// cosines serially (no cross-lane reduction), with the k-vector table staged
+// in shared memory.  Positions held in the rotated frame are rotated back to
+// the lab frame as calcHI does (extensional/src/main14.c:1720-1726).
+template <bool kSmem>
+__global__ void __launch_bounds__(256) k_hi_ewald_tiles(Lat l, Ewald ew,
+                                                        const double* __restrict__ rx,
+                                                        const double* __restrict__ ry,
+                                                        const double* __restrict__ rz, int N,
+                                                        int NT, const int* __restrict__ tileI,
+                                                        const double* __restrict__ kvec_g,
+                                                        double* Mt) {
+  extern __shared__ double ksh[];
+  long long tile = blockIdx.x;
+  int I = tileI[tile];
+  int J = I + (int)(tile - tile_off(I, NT));
+  const double* kvec = kvec_g;
+  if (kSmem) {
+    for (int e = threadIdx.x; e < 9 * ew.nk; e += blockDim.x) ksh[e] = kvec_g[e];
+    __syncthreads();
+    kvec = ksh;
+  }
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* tb = Mt + tile * 6144;
+  int j = J * 32 + lane;
+  double rxj = 0, ryj = 0, rzj = 0;
+  if (j < N) {
+    rxj = l.flow ? rx[j] * l.cth - ry[j] * l.sth : rx[j];
+    ryj = l.flow ? rx[j] * l.sth + ry[j] * l.cth : ry[j];
+    rzj = rz[j];
+  }
+  int side = 2 * ew.nmax + 1, nimg = side * side * side;
+  for (int q = 0; q < 4; q++) {
+    int il = w + 8 * q, i = I * 32 + il;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (i < j && j < N) {
+      double rxi = l.flow ? rx[i] * l.cth - ry[i] * l.sth : rx[i];
+      double ryi = l.flow ? rx[i] * l.sth + ry[i] * l.cth : ry[i];
+      double dxo = rxj - rxi, dyo = ryj - ryi, dzo = rzj - rz[i];
+      for (int m = 0; m < nimg; m++) {
+        int nz = m % side - ew.nmax, ny = (m / side) % side - ew.nmax;
+        int nx = m / (side * side) - ew.nmax;
+        double dx = dxo + nx * l.L1x + ny * l.L2x;
+        double dy = dyo + nx * l.L1y + ny * l.L2y;
+        double dz = dzo + nz * l.L;
+        double rr = dx * dx + dy * dy + dz * dz;
+        if (sqrt(rr) < ew.rce) {
+          double t1, t2;
+          rpy_real(ew, rr, t1, t2);
+          acc[0] += t1 + t2 * dx * dx / rr;
+          acc[1] += t2 * dx * dy / rr;
+          acc[2] += t2 * dx * dz / rr;
+          acc[3] += t1 + t2 * dy * dy / rr;
+          acc[4] += t2 * dy * dz / rr;
+          acc[5] += t1 + t2 * dz * dz / rr;
+        }
+      }
+      for (int c = 0; c < ew.nk; c++) {
+        const double* kv = kvec + 9 * c;
+        double ck = cos(kv[0] * dxo + kv[1] * dyo + kv[2] * dzo);
+        acc[0] += kv[3] * ck;
+        acc[1] += kv[4] * ck;
+        acc[2] += kv[5] * ck;
+        acc[3] += kv[6] * ck;
+        acc[4] += kv[7] * ck;
+        acc[5] += kv[8] * ck;
+      }
+    }
+    for (int a = 0; a < 6; a++) tb[a * 1024 + il * 32 + lane] = acc[a];
+  }
+}
+
+__global__ void k_to_fp32(const double* __restrict__ a, float* b, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t st = (size_t)gridDim.x * blockDim.x;
+  for (; i < n; i += st) b[i] = (float)a[i];
+}
+
 // gridHI (shear/src/gridHI.c:145-240): one warp per bin of one lattice frame;
 // the bin centre is the displacement, except the origin bin at (0.6,0.6,0.6).
 __global__ void __launch_bounds__(256) k_grid_bins(Lat l, Ewald ew,
@@ -252,29 +331,27 @@ __global__ void __launch_bounds__(256) k_grid_bins(Lat l, Ewald ew,
   }
 }
 
-// Input vector with component pointers and stride: x_c(i) = p[c][i*stride].
-struct VecIn {
-  const double* p[3];
-  int stride;
-};
-
 __device__ __forceinline__ double vin(const VecIn& v, int c, int i) {
   return v.p[c][(size_t)i * v.stride];
 }
 
-// Partial products of one packed tile with two right-hand sides.
-template <typename T>
-__global__ void __launch_bounds__(256) k_sym_matvec2(const T* __restrict__ Mt,
-                                                     const int* __restrict__ tileI, int NT, int N,
-                                                     VecIn v0, VecIn v1, double* rowpart,
-                                                     double* colpart) {
+// Partial products of one packed tile with R right-hand sides (R = 1, 2).
+// T is the tile storage type (double, or float with FP64 accumulation).  The
+// tile's block (il, jl) multiplies x_J into row il and, by block symmetry,
+// x_I into column jl; per-tile partial sums go to scratch (96 R doubles for
+// rows, 96 R for columns).
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_sym_matvec(const T* __restrict__ Mt,
+                                                    const int* __restrict__ tileI, int NT, int N,
+                                                    VecIn v0, VecIn v1, double* rowpart,
+                                                    double* colpart) {
   long long tile = blockIdx.x;
   int I = tileI[tile];
   int J = I + (int)(tile - tile_off(I, NT));
-  __shared__ double xI[2][3][32], xJ[2][3][32], racc[2][3][32];
-  __shared__ double cacc[8][6][32];
+  __shared__ double xI[R][3][32], xJ[R][3][32], racc[R][3][32];
+  __shared__ double cacc[8][3 * R][32];
   int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  if (tid < 192) {
+  if (tid < 96 * R) {
     int r = tid / 96, c = (tid / 32) % 3, k = tid & 31;
     int i = I * 32 + k, j = J * 32 + k;
     const VecIn& v = r ? v1 : v0;
@@ -290,7 +367,9 @@ __global__ void __launch_bounds__(256) k_sym_matvec2(const T* __restrict__ Mt,
     for (int a = 0; a < 6; a++) m[q][a] = (double)tb[a * 1024 + il * 32 + lane];
   }
   __syncthreads();
-  double cs[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  double cs[R][3];
+#pragma unroll
+  for (int r = 0; r < R; r++) cs[r][0] = cs[r][1] = cs[r][2] = 0.0;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     int il = w + 8 * q;
@@ -298,7 +377,7 @@ __global__ void __launch_bounds__(256) k_sym_matvec2(const T* __restrict__ Mt,
     double m0 = valid ? m[q][0] : 0.0, m1 = valid ? m[q][1] : 0.0, m2 = valid ? m[q][2] : 0.0;
     double m3 = valid ? m[q][3] : 0.0, m4 = valid ? m[q][4] : 0.0, m5 = valid ? m[q][5] : 0.0;
 #pragma unroll
-    for (int r = 0; r < 2; r++) {
+    for (int r = 0; r < R; r++) {
       double x0 = xJ[r][0][lane], x1 = xJ[r][1][lane], x2 = xJ[r][2][lane];
       double ra = m0 * x0 + m1 * x1 + m2 * x2;
       double rb = m1 * x0 + m3 * x1 + m4 * x2;
@@ -321,39 +400,45 @@ __global__ void __launch_bounds__(256) k_sym_matvec2(const T* __restrict__ Mt,
     }
   }
 #pragma unroll
-  for (int r = 0; r < 2; r++)
+  for (int r = 0; r < R; r++)
 #pragma unroll
     for (int a = 0; a < 3; a++) cacc[w][r * 3 + a][lane] = cs[r][a];
   __syncthreads();
-  if (tid < 192) {
+  if (tid < 96 * R) {
     int ra = tid / 32, k = tid & 31;
     double s = 0;
 #pragma unroll
     for (int ww = 0; ww < 8; ww++) s += cacc[ww][ra][k];
-    colpart[tile * 192 + tid] = s;
-    rowpart[tile * 192 + tid] = racc[ra / 3][ra % 3][k];
+    colpart[tile * (96 * R) + tid] = s;
+    rowpart[tile * (96 * R) + tid] = racc[ra / 3][ra % 3][k];
   }
 }
 
 // First reduction level: block (K, s) sums its share of the row partials of
-// tiles (K, J >= K) and the column partials of tiles (I <= K, K).
+// tiles (K, J >= K) and the column partials of tiles (I <= K, K);
+// blockDim = 96 R.
 __global__ void k_matvec_reduce1(const double* __restrict__ rowpart,
                                  const double* __restrict__ colpart, int NT, double* part) {
-  int K = blockIdx.x, s = blockIdx.y, e = threadIdx.x;  // e < 192
+  int K = blockIdx.x, s = blockIdx.y, e = threadIdx.x, E = blockDim.x;
   double acc = 0;
-  for (int J = K + s; J < NT; J += kRedSplit) acc += rowpart[(tile_off(K, NT) + (J - K)) * 192 + e];
-  for (int I = s; I <= K; I += kRedSplit) acc += colpart[(tile_off(I, NT) + (K - I)) * 192 + e];
-  part[((size_t)K * kRedSplit + s) * 192 + e] = acc;
+  for (int J = K + s; J < NT; J += kRedSplit) acc += rowpart[(tile_off(K, NT) + (J - K)) * E + e];
+  for (int I = s; I <= K; I += kRedSplit) acc += colpart[(tile_off(I, NT) + (K - I)) * E + e];
+  part[((size_t)K * kRedSplit + s) * E + e] = acc;
 }
 
-// Second level: Y[r][a][K*32+k] = sum over splits.
-__global__ void k_matvec_reduce2(const double* __restrict__ part, int NT, double* Y0, double* Y1) {
-  int K = blockIdx.x, e = threadIdx.x;
+// Second level: Y_r[a*NT*32 + K*32 + k] = sum over splits, plus the diagonal
+// block diag(D0,D1,D2) applied to the input when addiag is set.
+__global__ void k_matvec_reduce2(const double* __restrict__ part, int NT, int N, double* Y0,
+                                 double* Y1, VecIn v0, VecIn v1, int addiag, double D0,
+                                 double D1, double D2) {
+  int K = blockIdx.x, e = threadIdx.x, E = blockDim.x;
   double acc = 0;
-  for (int s = 0; s < kRedSplit; s++) acc += part[((size_t)K * kRedSplit + s) * 192 + e];
+  for (int s = 0; s < kRedSplit; s++) acc += part[((size_t)K * kRedSplit + s) * E + e];
   int r = e / 96, a = (e / 32) % 3, k = e & 31;
+  int i = K * 32 + k;
+  if (addiag && i < N) acc += (a == 0 ? D0 : a == 1 ? D1 : D2) * vin(r ? v1 : v0, a, i);
   double* Y = r ? Y1 : Y0;
-  Y[(size_t)a * NT * 32 + K * 32 + k] = acc;
+  Y[(size_t)a * NT * 32 + i] = acc;
 }
 
 // TEA displacement and position update (updateHI, shear/src/main26.c:787-855;
@@ -414,6 +499,7 @@ static int ensure_tiles(bd_ctx* c) {
   if (c->Mt) return BD_OK;
   size_t nt = c->ntiles;
   if (cudaMalloc(&c->Mt, 8 * nt * 6144) != cudaSuccess) return BD_ERR_OOM;
+  CU(cudaMemsetAsync(c->Mt, 0, 8 * nt * 6144, c->stream));
   std::vector<int> ti(nt);
   size_t k = 0;
   for (int I = 0; I < c->NT; I++)
@@ -421,7 +507,7 @@ static int ensure_tiles(bd_ctx* c) {
   CU(cudaMalloc(&c->tileI, 4 * nt));
   CU(cudaMemcpy(c->tileI, ti.data(), 4 * nt, cudaMemcpyHostToDevice));
   long long N = c->N;
-  c->near_cap = std::min<long long>(N * (N - 1) / 2 + 1, 512 * N);
+  c->near_cap = c->p.mobility == BD_MOB_EWALD ? 1 : std::min<long long>(N * (N - 1) / 2 + 1, 512 * N);
   CU(cudaMalloc(&c->near_pairs, 8 * c->near_cap));
   CU(cudaMalloc(&c->near_count, 16));
   CU(cudaMalloc(&c->rowpart, 8 * nt * 192));
@@ -438,7 +524,7 @@ static int ensure_tiles(bd_ctx* c) {
 // reciprocal lattice, extensional/src/main14.c:1582-1588), generated with
 // the reference's loop structure and arithmetic.
 static void hi_setup(bd_ctx* c, const Lat& l, Ewald* ew, std::vector<double>* kv, double Dtr[3],
-                     double M_HI = 4.0, int tp = 0) {
+                     double M_HI = 4.0, int tp = 0, bool exact_self = false) {
   double L = l.L, boxvol = c->boxvol;
   if (tp == 0) tp = c->tp;
   int treal = l.treal, nmax;
@@ -551,12 +637,13 @@ static void hi_setup(bd_ctx* c, const Lat& l, Ewald* ew, std::vector<double>* kv
     Dtr[1] += (*kv)[9 * k + 6];
     Dtr[2] += (*kv)[9 * k + 8];
   }
-  // self images with all three indices non-zero, yy projection added to zz
-  // (shear/src/main26.c:1667-1686)
+  // self images: the reference requires all three indices non-zero and adds
+  // the yy projection to the zz entry (shear/src/main26.c:1667-1686); with
+  // exact_self every image but the origin counts and zz uses dz
   for (int nx = -nmax; nx < nmax + 1; nx++)
     for (int ny = -nmax; ny < nmax + 1; ny++)
       for (int nz = -nmax; nz < nmax + 1; nz++)
-        if (nx != 0 && ny != 0 && nz != 0) {
+        if (exact_self ? (nx != 0 || ny != 0 || nz != 0) : (nx != 0 && ny != 0 && nz != 0)) {
           double dx = nx * L1[0] + ny * L2[0], dy = nx * L1[1] + ny * L2[1], dz = nz * L;
           double rr = dx * dx + dy * dy + dz * dz, r = sqrt(rr);
           double C1 = 0.75 / r + 0.5 / (r * rr);
@@ -567,7 +654,7 @@ static void hi_setup(bd_ctx* c, const Lat& l, Ewald* ew, std::vector<double>* kv
           double t2 = C3 * erfc(alpha * r) + C4 * exp(-alpha2 * rr) / rtpi;
           Dtr[0] += t1 + t2 * dx * dx / rr;
           Dtr[1] += t1 + t2 * dy * dy / rr;
-          Dtr[2] += t1 + t2 * dy * dy / rr;
+          Dtr[2] += t1 + t2 * (exact_self ? dz * dz : dy * dy) / rr;
         }
   ew->alpha = alpha;
   ew->alpha2 = alpha2;
@@ -596,8 +683,10 @@ int calc_hi(bd_ctx* c) {
   Lat l = step_lat(c);
   Ewald ew;
   std::vector<double> kv;
-  hi_setup(c, l, &ew, &kv, c->Dtr);
+  bool ewald_all = c->p.mobility == BD_MOB_EWALD;
+  hi_setup(c, l, &ew, &kv, c->Dtr, 4.0, 0, ewald_all);
   if ((int)kv.size() / 9 > c->kvec_cap) {
+    CU(cudaStreamSynchronize(c->stream));
     if (c->kvec) cudaFree(c->kvec);
     c->kvec_cap = (int)kv.size() / 9 + 64;
     CU(cudaMalloc(&c->kvec, 8 * 9 * (size_t)c->kvec_cap));
@@ -605,36 +694,77 @@ int calc_hi(bd_ctx* c) {
   c->nk = ew.nk;
   if (!kv.empty())
     CU(cudaMemcpyAsync(c->kvec, kv.data(), 8 * kv.size(), cudaMemcpyHostToDevice, c->stream));
-  CU(cudaMemsetAsync(c->near_count, 0, 4, c->stream));
   prof_begin(c, BD_PROF_HI_BUILD);
-  c->launches++;
-  k_hi_far<<<(unsigned)c->ntiles, 256, 0, c->stream>>>(
-      l, ew, c->rx, c->ry, c->rz, c->N, c->NT, c->tileI, c->grid, c->nbx, c->nby, c->nbz, c->nhx,
-      c->nhy, c->nhz, c->bsx, c->bsy, c->bsz, c->nbins, c->Mt, (int2*)c->near_pairs,
-      c->near_count, (long long)c->near_cap, c->err);
-  c->launches++;
-  k_hi_near<<<148 * 8, 256, 0, c->stream>>>(l, ew, c->rx, c->ry, c->rz, c->NT,
-                                                     (const int2*)c->near_pairs, c->near_count,
-                                                     (long long)c->near_cap, c->kvec, c->Mt);
+  if (ewald_all) {
+    size_t smem = 8 * 9 * (size_t)ew.nk;
+    c->launches++;
+    if (smem <= 96 * 1024) {
+      cudaFuncSetAttribute(k_hi_ewald_tiles<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           96 * 1024);
+      k_hi_ewald_tiles<true><<<(unsigned)c->ntiles, 256, smem, c->stream>>>(
+          l, ew, c->rx, c->ry, c->rz, c->N, c->NT, c->tileI, c->kvec, c->Mt);
+    } else {
+      k_hi_ewald_tiles<false><<<(unsigned)c->ntiles, 256, 0, c->stream>>>(
+          l, ew, c->rx, c->ry, c->rz, c->N, c->NT, c->tileI, c->kvec, c->Mt);
+    }
+  } else {
+    CU(cudaMemsetAsync(c->near_count, 0, 4, c->stream));
+    c->launches++;
+    k_hi_far<<<(unsigned)c->ntiles, 256, 0, c->stream>>>(
+        l, ew, c->rx, c->ry, c->rz, c->N, c->NT, c->tileI, c->grid, c->nbx, c->nby, c->nbz,
+        c->nhx, c->nhy, c->nhz, c->bsx, c->bsy, c->bsz, c->nbins, c->Mt, (int2*)c->near_pairs,
+        c->near_count, (long long)c->near_cap, c->err);
+    c->launches++;
+    k_hi_near<<<148 * 8, 256, 0, c->stream>>>(l, ew, c->rx, c->ry, c->rz, c->NT,
+                                              (const int2*)c->near_pairs, c->near_count,
+                                              (long long)c->near_cap, c->kvec, c->Mt);
+  }
+  if (c->p.precision == BD_PREC_FP32) {
+    if (!c->Mt32) {
+      CU(cudaStreamSynchronize(c->stream));
+      if (cudaMalloc(&c->Mt32, 4 * c->ntiles * 6144) != cudaSuccess) return BD_ERR_OOM;
+      c->bytes += 4 * c->ntiles * 6144;
+    }
+    c->launches++;
+    k_to_fp32<<<148 * 16, 256, 0, c->stream>>>(c->Mt, c->Mt32, c->ntiles * 6144);
+  }
   prof_end(c, BD_PROF_HI_BUILD);
   c->hi_built = true;
   return launch_ok(c);
 }
 
-// y0 = M_off v0, y1 = M_off v1 over the packed tiles (off-diagonal blocks).
-static int sym_matvec2(bd_ctx* c, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1) {
+// Y_r = M v_r for R = 1 or 2 right-hand sides over the packed tiles (FP64 or
+// FP32 storage); with addiag the uniform diagonal blocks are included,
+// otherwise only the off-diagonal blocks.
+int sym_matvec(bd_ctx* c, int R, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1,
+               bool addiag) {
+  unsigned nt = (unsigned)c->ntiles;
   prof_begin(c, BD_PROF_MATVEC);
   c->launches++;
-  k_sym_matvec2<double><<<(unsigned)c->ntiles, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N,
-                                                                     v0, v1, c->rowpart,
-                                                                     c->colpart);
+  if (c->Mt32) {
+    if (R == 2)
+      k_sym_matvec<float, 2><<<nt, 256, 0, c->stream>>>(c->Mt32, c->tileI, c->NT, c->N, v0, v1,
+                                                        c->rowpart, c->colpart);
+    else
+      k_sym_matvec<float, 1><<<nt, 256, 0, c->stream>>>(c->Mt32, c->tileI, c->NT, c->N, v0, v1,
+                                                        c->rowpart, c->colpart);
+  } else {
+    if (R == 2)
+      k_sym_matvec<double, 2><<<nt, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N, v0, v1,
+                                                         c->rowpart, c->colpart);
+    else
+      k_sym_matvec<double, 1><<<nt, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N, v0, v1,
+                                                         c->rowpart, c->colpart);
+  }
   prof_end(c, BD_PROF_MATVEC);
   double* part = c->colpart + c->ntiles * 192;
   c->launches++;
-  k_matvec_reduce1<<<dim3(c->NT, kRedSplit), 192, 0, c->stream>>>(c->rowpart, c->colpart, c->NT,
-                                                                  part);
+  k_matvec_reduce1<<<dim3(c->NT, kRedSplit), 96 * R, 0, c->stream>>>(c->rowpart, c->colpart,
+                                                                    c->NT, part);
   c->launches++;
-  k_matvec_reduce2<<<c->NT, 192, 0, c->stream>>>(part, c->NT, Y0, Y1);
+  k_matvec_reduce2<<<c->NT, 96 * R, 0, c->stream>>>(part, c->NT, c->N, Y0, Y1, v0, v1,
+                                                    addiag ? 1 : 0, c->Dtr[0], c->Dtr[1],
+                                                    c->Dtr[2]);
   return launch_ok(c);
 }
 
@@ -652,7 +782,7 @@ int update_hi(bd_ctx* c) {
   if (c->p.flow == BD_FLOW_EXT) rotate_coords(c, 1);
   VecIn vf = {{c->fx, c->fy, c->fz}, 1};
   VecIn vr = {{c->R, c->R + 1, c->R + 2}, 3};
-  if ((s = sym_matvec2(c, vf, vr, c->U, c->W)) != BD_OK) return s;
+  if ((s = sym_matvec(c, 2, vf, vr, c->U, c->W, false)) != BD_OK) return s;
   double p = sqrt(2.0 / c->p.dt);
   c->launches++;
   k_tea_update<<<(c->N + 255) / 256, 256, 0, c->stream>>>(
