@@ -86,8 +86,11 @@ def test_krylov_steps_stable(flow):
     Nb, Nc, L = 25, 20, 30.0
     x, y, z = _system(flow, Nb, Nc, L, 41)
     q = B.random_charges(Nb, Nc, 0.5, 43)
+    # FENE k = 30 in both flows (the shear tree's forced k = 200 is for its
+    # Hookean spring; shear_kappas_override keeps the configured k)
     c = B.Context(B.make_params(flow, Nb, Nc, L, 0.01, 5e-4, mobility="ewald", precision="fp32",
-                                noise="philox", MStep=100, Ncharges=len(q)))
+                                noise="philox", MStep=100, Ncharges=len(q),
+                                shear_kappas_override=1))
     c.set_positions(x, y, z)
     c.set_charges(q)
     c.set_time(0, 0)
