@@ -43,7 +43,8 @@ typedef enum {
   BD_ERR_STATE = 8,        /* call out of order (e.g. no mobility built) */
   BD_ERR_TIMEOUT = 9,      /* a bounded device wait gave up */
   BD_ERR_LANCZOS = 10,     /* Krylov square root missed its tolerance */
-  BD_ERR_ASYMMETRIC = 11   /* lookup tensor not symmetric */
+  BD_ERR_ASYMMETRIC = 11,  /* lookup tensor not symmetric */
+  BD_ERR_CAPACITY = 12     /* system larger than a fixed-size buffer allows */
 } bd_status;
 
 typedef enum { BD_FLOW_SHEAR = 0, BD_FLOW_EXT = 1 } bd_flow;
@@ -209,6 +210,21 @@ int bd_lanczos_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
 /* calls, total Krylov iterations, calls that hit lanczos_max, negative Ritz
  * values clamped (a hybrid mobility need not be positive definite) */
 int bd_lanczos_stats(bd_ctx *ctx, long *out4);
+/* No counterpart in the reference.  out = M v like bd_mobility_apply, for
+ * callers that must not allocate device memory where they call it (a loop
+ * running while another framework's pool owns the device, a fixed memory
+ * budget, or code that must avoid the device-wide synchronisation
+ * cudaMalloc/cudaFree can cause).  v and out are device pointers,
+ * bead-interleaved (v[3 i + a]); the call is asynchronous on the context's
+ * stream and allocates nothing: its scratch is a fixed device array of the
+ * library (14.3 MB, held on every GPU that loads the library until exit), so
+ * N may not exceed BD_NOALLOC_MAX_BEADS (else BD_ERR_CAPACITY).  All calls on
+ * a device share that array: calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture.  The context's device must be current. */
+#define BD_NOALLOC_MAX_BEADS 4096
+int bd_mobility_apply_noalloc(bd_ctx *ctx, const double *v, double *out);
+
 /* One Brownian-dynamics step with the Krylov displacement
  * dr = dt M F + sqrt(2 dt) M^(1/2) z + dt u(r): the reference's step order
  * (lattice, PBC, neighbour check, forces, mobility rebuild every srpy steps,

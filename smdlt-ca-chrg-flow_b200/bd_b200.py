@@ -23,7 +23,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
-SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu"]
+SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
+           "bd_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

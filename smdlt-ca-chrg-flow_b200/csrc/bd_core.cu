@@ -534,6 +534,7 @@ const char* bd_status_string(int s) {
     case BD_ERR_TIMEOUT: return "bounded device wait timed out";
     case BD_ERR_LANCZOS: return "Lanczos tolerance not met";
     case BD_ERR_ASYMMETRIC: return "asymmetric lookup tensor";
+    case BD_ERR_CAPACITY: return "system larger than the fixed buffer allows";
   }
   return "unknown status";
 }
