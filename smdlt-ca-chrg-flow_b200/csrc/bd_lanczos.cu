@@ -31,46 +31,6 @@ using namespace bd;
 
 static const int kDotBlocks = 148;  // one CTA per SM for the vector reductions
 
-// partial[k][b] = sum over block b's chunk of V_k . w   (grid: kDotBlocks x nv)
-__global__ void __launch_bounds__(256) k_multidot(const double* __restrict__ V, size_t vstride,
-                                                  const double* __restrict__ w, int n,
-                                                  double* part) {
-  int k = blockIdx.y;
-  const double* v = V + (size_t)k * vstride;
-  double s = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    s += v[i] * w[i];
-  __shared__ double sh[8];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sh[q];
-    part[(size_t)k * gridDim.x + blockIdx.x] = t;
-  }
-}
-
-// out[k] (+)= sum_b part[k][b]; with acc the result is added to out.
-__global__ void k_reduce_parts(const double* __restrict__ part, int nblk, int nv, double* out,
-                               int acc) {
-  int k = threadIdx.x;
-  if (k >= nv) return;
-  double s = 0;
-  for (int b = 0; b < nblk; b++) s += part[(size_t)k * nblk + b];
-  out[k] = acc ? out[k] + s : s;
-}
-
-// w -= sum_{k < nv} h[k] V_k
-__global__ void k_sub_combo(const double* __restrict__ V, size_t vstride,
-                            const double* __restrict__ h, int nv, double* w, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double s = 0;
-    for (int k = 0; k < nv; k++) s += h[k] * V[(size_t)k * vstride + i];
-    w[i] -= s;
-  }
-}
-
 // sc[0] = sqrt(sum of part) = |w|, sc[1] = 1/|w|
 __global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc) {
   if (threadIdx.x) return;
@@ -78,13 +38,6 @@ __global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc
   for (int b = 0; b < nblk; b++) s += part[b];
   sc[0] = sqrt(s);
   sc[1] = sc[0] > 0 ? 1.0 / sc[0] : 0.0;
-}
-
-__global__ void k_scale_into(const double* __restrict__ w, const double* __restrict__ sc,
-                             double* v, int n) {
-  double f = sc[1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    v[i] = w[i] * f;
 }
 
 // v (SoA, padded) = z (bead-interleaved) / |z|; padding entries are zero
@@ -104,6 +57,118 @@ __global__ void k_combo(const double* __restrict__ V, size_t vstride,
     for (int k = 0; k < nv; k++) s += c[k] * V[(size_t)k * vstride + i];
     y[i] = scale * s;
   }
+}
+
+// Fused classical Gram-Schmidt (two passes) for Lanczos step j, split over
+// kDotBlocks CTAs that each own one contiguous chunk of the 3 NTp entries.
+// A dot product is the sum over chunks of chunk-local dots, so a CTA can
+// update its own chunk as soon as it has the full sums; every CTA re-adds the
+// per-chunk partials in the same order, which keeps results deterministic.
+//   stage 0: part1[k][b] = V_k . w over chunk b                 (k <= j)
+//   stage 1: h = sum_b part1; w_b -= V_b h; part2[k][b] = V_k . w_b
+//   stage 2: h2 = sum_b part2; w_b -= V_b h2; part3[b] = |w_b|^2;
+//            CTA 0 stores alpha_j = h_j + h2_j
+//   stage 3: beta_j = sqrt(sum_b part3); v_{j+1,b} = w_b / beta_j
+__device__ __forceinline__ void chunk_range(int n, int& lo, int& hi) {
+  int per = (n + gridDim.x - 1) / gridDim.x;
+  lo = blockIdx.x * per;
+  hi = min(n, lo + per);
+}
+
+// one warp per vector k (strided): lanes over the chunk, shuffle reduction
+__device__ __forceinline__ void chunk_dots(const double* __restrict__ V, size_t vs, int nv,
+                                           const double* __restrict__ w, int lo, int hi,
+                                           double* part) {
+  int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = wp; k < nv; k += nw) {
+    const double* v = V + (size_t)k * vs;
+    double s = 0;
+    for (int i = lo + lane; i < hi; i += 32) s += v[i] * w[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) part[(size_t)k * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// h[k] = sum_b part[k][b] into shared memory (every CTA, same order)
+__device__ __forceinline__ void sum_parts(const double* __restrict__ part, int nv, double* h) {
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+    double s = 0;
+    for (int b = 0; b < (int)gridDim.x; b++) s += part[(size_t)k * gridDim.x + b];
+    h[k] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_orth0(const double* __restrict__ V, size_t vs, int nv,
+                                               const double* __restrict__ w, int n,
+                                               double* part1) {
+  int lo, hi;
+  chunk_range(n, lo, hi);
+  chunk_dots(V, vs, nv, w, lo, hi, part1);
+}
+
+__global__ void __launch_bounds__(256) k_orth1(const double* __restrict__ V, size_t vs, int nv,
+                                               double* w, int n, const double* __restrict__ part1,
+                                               double* part2, double* hsave) {
+  __shared__ double h[128];
+  int lo, hi;
+  chunk_range(n, lo, hi);
+  sum_parts(part1, nv, h);
+  if (blockIdx.x == 0)
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) hsave[k] = h[k];
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    double s = 0;
+    for (int k = 0; k < nv; k++) s += h[k] * V[(size_t)k * vs + i];
+    w[i] -= s;
+  }
+  __syncthreads();
+  chunk_dots(V, vs, nv, w, lo, hi, part2);
+}
+
+__global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, size_t vs, int nv,
+                                               double* w, int n, const double* __restrict__ part2,
+                                               double* part3, const double* __restrict__ hsave,
+                                               double* alpha, int j) {
+  __shared__ double h[128];
+  __shared__ double red[8];
+  int lo, hi;
+  chunk_range(n, lo, hi);
+  sum_parts(part2, nv, h);
+  double s2 = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    double s = 0;
+    for (int k = 0; k < nv; k++) s += h[k] * V[(size_t)k * vs + i];
+    double x = w[i] - s;
+    w[i] = x;
+    s2 += x * x;
+  }
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
+    part3[blockIdx.x] = t;
+    if (blockIdx.x == 0) alpha[j] = hsave[j] + h[j];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_orth3(const double* __restrict__ w, int n,
+                                               const double* __restrict__ part3, double* beta,
+                                               int j, double* vnext, int write_next) {
+  __shared__ double b;
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < (int)gridDim.x; q++) s += part3[q];
+    b = sqrt(s);
+    if (blockIdx.x == 0) beta[j] = b;
+  }
+  __syncthreads();
+  if (!write_next) return;
+  double f = b > 0 ? 1.0 / b : 0.0;
+  int lo, hi;
+  chunk_range(n, lo, hi);
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) vnext[i] = w[i] * f;
 }
 
 // |z|^2 partials over the bead-interleaved noise
@@ -230,13 +295,14 @@ int alloc_lanczos(bd_ctx* c) {
   size_t n = 3 * (size_t)c->NT * 32;
   CU(cudaMalloc(&c->LV, 8 * n * (c->lmax + 1)));
   CU(cudaMalloc(&c->Lw, 8 * n));
-  CU(cudaMalloc(&c->Lpart, 8 * (size_t)(c->lmax + 1) * kDotBlocks));
+  CU(cudaMalloc(&c->Lpart, 8 * (size_t)3 * (c->lmax + 1) * kDotBlocks));
   CU(cudaMalloc(&c->Lh, 8 * (size_t)(c->lmax + 1)));
-  CU(cudaMalloc(&c->Lsc, 8 * 8));
+  CU(cudaMalloc(&c->Lsc, 8 * (size_t)(c->lmax + 16)));
   CU(cudaMalloc(&c->Lc, 8 * (size_t)(c->lmax + 1)));
   CU(cudaMalloc(&c->MF, 8 * n));
   CU(cudaMalloc(&c->Yz, 8 * n));
-  c->bytes += 8 * n * (c->lmax + 4) + 8 * (size_t)(c->lmax + 1) * (kDotBlocks + 2) + 64;
+  c->bytes += 8 * n * (c->lmax + 4) + 8 * (size_t)(c->lmax + 1) * (3 * kDotBlocks + 2) +
+              8 * (size_t)(c->lmax + 16);
   return BD_OK;
 }
 
@@ -259,6 +325,12 @@ int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
   std::vector<double> alpha, beta, cc, cprev;
   int m = 0, neg = 0;
   bool conv = false;
+  // alpha_j, beta_j stay on the device (Lh[0..lmax), Lh[lmax+1..]); the host
+  // reads them only at checkpoints: from two before the previous call's
+  // Krylov dimension on, every second iteration
+  double* d_alpha = c->Lh;
+  double* d_beta = c->Lsc + 8;
+  int next_check = std::max(4, c->lan_last - 2);
   for (int j = 0; j < c->lmax; j++) {
     double* vj = c->LV + (size_t)j * vs;
     VecIn vin_j = {{vj, vj + NTp, vj + 2 * NTp}, 1};
@@ -269,52 +341,36 @@ int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
       if ((s = sym_matvec(c, 1, vin_j, vin_j, c->Lw, c->Lw, true)) != BD_OK) return s;
     }
     int nv = j + 1;
-    // two passes of classical Gram-Schmidt against V_0..V_j
-    for (int pass = 0; pass < 2; pass++) {
-      c->launches += 3;
-      k_multidot<<<dim3(blk, nv), 256, 0, st>>>(c->LV, vs, c->Lw, n, c->Lpart);
-      k_reduce_parts<<<1, 128, 0, st>>>(c->Lpart, blk, nv, c->Lh + 0, 0);
-      // keep alpha_j = h_j of both passes in Lc[j] (scratch) via accumulate
-      k_sub_combo<<<blk * 2, 256, 0, st>>>(c->LV, vs, c->Lh, nv, c->Lw, n);
-      if (pass == 0)
-        CU(cudaMemcpyAsync(c->Lc + j, c->Lh + j, 8, cudaMemcpyDeviceToDevice, st));
-      else {
-        c->launches++;
-        k_reduce_parts<<<1, 1, 0, st>>>(c->Lh + j, 1, 1, c->Lc + j, 1);
-      }
-    }
-    c->launches += 2;
-    k_multidot<<<dim3(blk, 1), 256, 0, st>>>(c->Lw, vs, c->Lw, n, c->Lpart);
-    k_norm_fin<<<1, 32, 0, st>>>(c->Lpart, blk, c->Lsc);
-    double ab[2];
-    CU(cudaMemcpyAsync(&ab[0], c->Lc + j, 8, cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(&ab[1], c->Lsc, 8, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
-    alpha.push_back(ab[0]);
-    beta.push_back(ab[1]);
+    double* part1 = c->Lpart;
+    double* part2 = c->Lpart + (size_t)(c->lmax + 1) * blk;
+    double* part3 = c->Lpart + (size_t)2 * (c->lmax + 1) * blk;
+    double* hsave = c->Lc;
+    c->launches += 4;
+    k_orth0<<<blk, 256, 0, st>>>(c->LV, vs, nv, c->Lw, n, part1);
+    k_orth1<<<blk, 256, 0, st>>>(c->LV, vs, nv, c->Lw, n, part1, part2, hsave);
+    k_orth2<<<blk, 256, 0, st>>>(c->LV, vs, nv, c->Lw, n, part2, part3, hsave, d_alpha, j);
+    k_orth3<<<blk, 256, 0, st>>>(c->Lw, n, part3, d_beta, j, c->LV + (size_t)(j + 1) * vs,
+                                 j + 1 <= c->lmax ? 1 : 0);
     m = j + 1;
+    if (m < next_check && m < c->lmax) continue;
+    alpha.resize(m);
+    beta.resize(m);
+    CU(cudaMemcpyAsync(alpha.data(), d_alpha, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(beta.data(), d_beta, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
     neg = sqrt_e1(alpha, beta, m, cc);
-    if (m >= 2) {
-      double dn = 0, cn = 0;
-      for (int i = 0; i < m; i++) {
-        double prev = i < m - 1 ? cprev[i] : 0.0;
-        dn += (cc[i] - prev) * (cc[i] - prev);
-        cn += cc[i] * cc[i];
-      }
-      if (sqrt(dn) <= c->ltol * sqrt(cn)) {
-        conv = true;
-        break;
-      }
+    sqrt_e1(alpha, beta, m - 1, cprev);
+    double dn = 0, cn = 0;
+    for (int i = 0; i < m; i++) {
+      double prev = i < m - 1 ? cprev[i] : 0.0;
+      dn += (cc[i] - prev) * (cc[i] - prev);
+      cn += cc[i] * cc[i];
     }
-    cprev = cc;
-    if (ab[1] <= 1e-300) {  // invariant subspace: exact
+    if (sqrt(dn) <= c->ltol * sqrt(cn) || beta[m - 1] <= 1e-300) {
       conv = true;
       break;
     }
-    if (j + 1 < c->lmax) {
-      c->launches++;
-      k_scale_into<<<blk * 2, 256, 0, st>>>(c->Lw, c->Lsc, c->LV + (size_t)(j + 1) * vs, n);
-    }
+    next_check = m + 2;
   }
   CU(cudaMemcpyAsync(c->Lc, cc.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, st));
   c->launches++;
