@@ -335,83 +335,149 @@ __device__ __forceinline__ double vin(const VecIn& v, int c, int i) {
   return v.p[c][(size_t)i * v.stride];
 }
 
-// Partial products of one packed tile with R right-hand sides (R = 1, 2).
-// T is the tile storage type (double, or float with FP64 accumulation).  The
-// tile's block (il, jl) multiplies x_J into row il and, by block symmetry,
-// x_I into column jl; per-tile partial sums go to scratch (96 R doubles for
-// rows, 96 R for columns).
+// Loads four consecutive tile entries (one row, four columns) as 16-byte
+// vectors: one float4, or two double2.
+__device__ __forceinline__ void load4(const float* p, double o[4]) {
+  float4 v = *reinterpret_cast<const float4*>(p);
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double* p, double o[4]) {
+  double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  o[0] = a.x;
+  o[1] = a.y;
+  o[2] = b.x;
+  o[3] = b.y;
+}
+
+// Partial products of packed tiles with R right-hand sides (R = 1, 2).  T is
+// the tile storage type (double, or float with FP64 accumulation).  A group of
+// 64 threads owns one tile; thread (rg, cg) owns the 4x4 sub-block of 3x3
+// blocks at rows 4rg.. and columns 4cg.., read with 16-byte loads.  Each
+// block multiplies x_J into its row and, by block symmetry, x_I into its
+// column; row sums are finished across the 8 threads of a row group by
+// shuffles, column sums across the 8 row groups by shuffles and one shared
+// exchange between the group's two warps.  Four tiles per 256-thread CTA.
+// Per-tile partials go to scratch: 96 R doubles for rows, 96 R for columns.
 template <typename T, int R>
 __global__ void __launch_bounds__(256) k_sym_matvec(const T* __restrict__ Mt,
                                                     const int* __restrict__ tileI, int NT, int N,
-                                                    VecIn v0, VecIn v1, double* rowpart,
-                                                    double* colpart) {
-  long long tile = blockIdx.x;
-  int I = tileI[tile];
-  int J = I + (int)(tile - tile_off(I, NT));
-  __shared__ double xI[R][3][32], xJ[R][3][32], racc[R][3][32];
-  __shared__ double cacc[8][3 * R][32];
-  int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  if (tid < 96 * R) {
-    int r = tid / 96, c = (tid / 32) % 3, k = tid & 31;
-    int i = I * 32 + k, j = J * 32 + k;
-    const VecIn& v = r ? v1 : v0;
-    xI[r][c][k] = i < N ? vin(v, c, i) : 0.0;
-    xJ[r][c][k] = j < N ? vin(v, c, j) : 0.0;
+                                                    long long ntiles, VecIn v0, VecIn v1,
+                                                    double* rowpart, double* colpart) {
+  const int g = threadIdx.x >> 6, t = threadIdx.x & 63;
+  const int rg = t >> 3, cg = t & 7, lane = threadIdx.x & 31;
+  long long tile = (long long)blockIdx.x * 4 + g;
+  bool active = tile < ntiles;
+  int I = 0, J = 0;
+  if (active) {
+    I = tileI[tile];
+    J = I + (int)(tile - tile_off(I, NT));
   }
-  const T* tb = Mt + tile * 6144;
-  double m[4][6];
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    int il = w + 8 * q;
-#pragma unroll
-    for (int a = 0; a < 6; a++) m[q][a] = (double)tb[a * 1024 + il * 32 + lane];
+  __shared__ double xs[4][R][2][3][32];
+  __shared__ double cx[4][R][3][4][8];  // column partials of the upper warp, per (rhs, comp, col, cg)
+  for (int e = t; e < 2 * R * 96; e += 64) {
+    int r = e / 192, rem = e % 192, side = rem / 96, c = (rem / 32) % 3, k = rem & 31;
+    int idx = (side ? J : I) * 32 + k;
+    xs[g][r][side][c][k] = (active && idx < N) ? vin(r ? v1 : v0, c, idx) : 0.0;
   }
   __syncthreads();
-  double cs[R][3];
-#pragma unroll
-  for (int r = 0; r < R; r++) cs[r][0] = cs[r][1] = cs[r][2] = 0.0;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    int il = w + 8 * q;
-    bool valid = (I != J) || (il < lane);
-    double m0 = valid ? m[q][0] : 0.0, m1 = valid ? m[q][1] : 0.0, m2 = valid ? m[q][2] : 0.0;
-    double m3 = valid ? m[q][3] : 0.0, m4 = valid ? m[q][4] : 0.0, m5 = valid ? m[q][5] : 0.0;
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      double x0 = xJ[r][0][lane], x1 = xJ[r][1][lane], x2 = xJ[r][2][lane];
-      double ra = m0 * x0 + m1 * x1 + m2 * x2;
-      double rb = m1 * x0 + m3 * x1 + m4 * x2;
-      double rc = m2 * x0 + m4 * x1 + m5 * x2;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        ra += __shfl_xor_sync(0xffffffffu, ra, o);
-        rb += __shfl_xor_sync(0xffffffffu, rb, o);
-        rc += __shfl_xor_sync(0xffffffffu, rc, o);
-      }
-      if (lane == 0) {
-        racc[r][0][il] = ra;
-        racc[r][1][il] = rb;
-        racc[r][2][il] = rc;
-      }
-      double y0 = xI[r][0][il], y1 = xI[r][1][il], y2 = xI[r][2][il];
-      cs[r][0] += m0 * y0 + m1 * y1 + m2 * y2;
-      cs[r][1] += m1 * y0 + m3 * y1 + m4 * y2;
-      cs[r][2] += m2 * y0 + m4 * y1 + m5 * y2;
-    }
-  }
+  double rs[R][4][3], cs[R][4][3];
 #pragma unroll
   for (int r = 0; r < R; r++)
 #pragma unroll
-    for (int a = 0; a < 3; a++) cacc[w][r * 3 + a][lane] = cs[r][a];
-  __syncthreads();
-  if (tid < 96 * R) {
-    int ra = tid / 32, k = tid & 31;
-    double s = 0;
+    for (int k = 0; k < 4; k++) rs[r][k][0] = rs[r][k][1] = rs[r][k][2] = cs[r][k][0] = cs[r][k][1] = cs[r][k][2] = 0.0;
+  double xj[R][3][4];
 #pragma unroll
-    for (int ww = 0; ww < 8; ww++) s += cacc[ww][ra][k];
-    colpart[tile * (96 * R) + tid] = s;
-    rowpart[tile * (96 * R) + tid] = racc[ra / 3][ra % 3][k];
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) xj[r][a][k] = xs[g][r][1][a][4 * cg + k];
+  const T* tb = Mt + (active ? tile : 0) * 6144;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    int il = 4 * rg + rr;
+    double m[6][4];
+#pragma unroll
+    for (int c = 0; c < 6; c++) load4(tb + c * 1024 + il * 32 + 4 * cg, m[c]);
+    double xi[R][3];
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int a = 0; a < 3; a++) xi[r][a] = xs[g][r][0][a][il];
+#pragma unroll
+    for (int cc = 0; cc < 4; cc++) {
+      int jl = 4 * cg + cc;
+      bool valid = active && ((I != J) || (il < jl));
+      double m0 = valid ? m[0][cc] : 0.0, m1 = valid ? m[1][cc] : 0.0, m2 = valid ? m[2][cc] : 0.0;
+      double m3 = valid ? m[3][cc] : 0.0, m4 = valid ? m[4][cc] : 0.0, m5 = valid ? m[5][cc] : 0.0;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        double x0 = xj[r][0][cc], x1 = xj[r][1][cc], x2 = xj[r][2][cc];
+        rs[r][rr][0] += m0 * x0 + m1 * x1 + m2 * x2;
+        rs[r][rr][1] += m1 * x0 + m3 * x1 + m4 * x2;
+        rs[r][rr][2] += m2 * x0 + m4 * x1 + m5 * x2;
+        double y0 = xi[r][0], y1 = xi[r][1], y2 = xi[r][2];
+        cs[r][cc][0] += m0 * y0 + m1 * y1 + m2 * y2;
+        cs[r][cc][1] += m1 * y0 + m3 * y1 + m4 * y2;
+        cs[r][cc][2] += m2 * y0 + m4 * y1 + m5 * y2;
+      }
+    }
   }
+  // rows: sum over the 8 column groups (lane bits 0..2)
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        double v = rs[r][k][a];
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        rs[r][k][a] = v;
+      }
+  // columns: sum over the 4 row groups of this warp (lane bits 3..4)
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        double v = cs[r][k][a];
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        cs[r][k][a] = v;
+      }
+  bool upper = t >= 32;  // second warp of the group: row groups 4..7
+  if (upper && lane < 8)
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) cx[g][r][a][k][cg] = cs[r][k][a];
+  __syncthreads();
+  if (!active) return;
+  double* rp = rowpart + tile * (96 * R);
+  double* cp = colpart + tile * (96 * R);
+  if (cg == 0)
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) rp[r * 96 + a * 32 + 4 * rg + k] = rs[r][k][a];
+  if (!upper && lane < 8)
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          cp[r * 96 + a * 32 + 4 * cg + k] = cs[r][k][a] + cx[g][r][a][k][cg];
 }
 
 // First reduction level: block (K, s) sums its share of the row partials of
@@ -738,23 +804,24 @@ int calc_hi(bd_ctx* c) {
 // otherwise only the off-diagonal blocks.
 int sym_matvec(bd_ctx* c, int R, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1,
                bool addiag) {
-  unsigned nt = (unsigned)c->ntiles;
+  long long ntl = (long long)c->ntiles;
+  unsigned nb = (unsigned)((ntl + 3) / 4);
   prof_begin(c, BD_PROF_MATVEC);
   c->launches++;
   if (c->Mt32) {
     if (R == 2)
-      k_sym_matvec<float, 2><<<nt, 256, 0, c->stream>>>(c->Mt32, c->tileI, c->NT, c->N, v0, v1,
-                                                        c->rowpart, c->colpart);
+      k_sym_matvec<float, 2><<<nb, 256, 0, c->stream>>>(c->Mt32, c->tileI, c->NT, c->N, ntl, v0,
+                                                        v1, c->rowpart, c->colpart);
     else
-      k_sym_matvec<float, 1><<<nt, 256, 0, c->stream>>>(c->Mt32, c->tileI, c->NT, c->N, v0, v1,
-                                                        c->rowpart, c->colpart);
+      k_sym_matvec<float, 1><<<nb, 256, 0, c->stream>>>(c->Mt32, c->tileI, c->NT, c->N, ntl, v0,
+                                                        v1, c->rowpart, c->colpart);
   } else {
     if (R == 2)
-      k_sym_matvec<double, 2><<<nt, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N, v0, v1,
-                                                         c->rowpart, c->colpart);
+      k_sym_matvec<double, 2><<<nb, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N, ntl, v0,
+                                                         v1, c->rowpart, c->colpart);
     else
-      k_sym_matvec<double, 1><<<nt, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N, v0, v1,
-                                                         c->rowpart, c->colpart);
+      k_sym_matvec<double, 1><<<nb, 256, 0, c->stream>>>(c->Mt, c->tileI, c->NT, c->N, ntl, v0,
+                                                         v1, c->rowpart, c->colpart);
   }
   prof_end(c, BD_PROF_MATVEC);
   double* part = c->colpart + c->ntiles * 192;
