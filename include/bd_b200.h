@@ -53,9 +53,12 @@ typedef enum { BD_FLOW_SHEAR = 0, BD_FLOW_EXT = 1 } bd_flow;
  * Philox4x32-10 Gaussians (parallel; the production source). */
 typedef enum { BD_NOISE_RAN1 = 0, BD_NOISE_PHILOX = 1 } bd_noise;
 /* Pair mobility: the reference's hybrid (Ewald sum below a minimum-image
- * distance of 12, lookup table beyond, shear/src/main26.c:1714-1794) or the
- * Ewald sum for every pair. */
-typedef enum { BD_MOB_HYBRID = 0, BD_MOB_EWALD = 1 } bd_mobility_kind;
+ * distance of 12, lookup table beyond, shear/src/main26.c:1714-1794), the
+ * Ewald sum for every pair as a dense packed matrix, or the same Ewald sum
+ * applied matrix-free by smooth particle-mesh Ewald (no reference
+ * counterpart; O(N + K^3 log K) per product, for systems whose dense
+ * matrix does not fit). */
+typedef enum { BD_MOB_HYBRID = 0, BD_MOB_EWALD = 1, BD_MOB_PME = 2 } bd_mobility_kind;
 /* Storage of the packed mobility tiles used by the products: FP64, or FP32
  * with FP64 accumulation. */
 typedef enum { BD_PREC_FP64 = 0, BD_PREC_FP32 = 1 } bd_precision;
@@ -94,6 +97,16 @@ typedef struct {
   int precision;             /* bd_precision */
   double lanczos_tol;        /* relative change of sqrt(M) z between iterations; 0 -> 1e-6 */
   int lanczos_max;           /* Krylov dimension cap; 0 -> 80 */
+  /* BD_MOB_PME discretisation (no reference counterpart): grid points per
+   * reduced lattice direction (0 -> smallest 2^a 3^b 5^c 7^d >= 1.9 L),
+   * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> 10, at
+   * most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
+   * real-space pairs per bead (0 -> 512). */
+  int pme_grid;
+  int pme_order;
+  double pme_rc;
+  double pme_alpha;
+  int pme_max_pairs;
 } bd_params;
 
 typedef struct bd_ctx bd_ctx;

@@ -24,7 +24,8 @@ ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
-           "bd_noalloc.cu"]
+           "bd_noalloc.cu", "bd_pme.cu"]
+CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -39,7 +40,8 @@ def build(verbose: bool = False) -> str:
     """Compile libbd_b200.so for sm_100a with nvcc (in-tree)."""
     srcs = [os.path.join(PKG, "csrc", s) for s in SOURCES]
     cmd = ["nvcc", "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
-           f"-I{INCLUDE}", "-o", LIB, *srcs]
+           f"-I{INCLUDE}", "-o", LIB, *srcs, f"-L{CUDA_LIB}", "-lcufft",
+           "-Xlinker", f"-rpath,{CUDA_LIB}"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
@@ -65,7 +67,8 @@ class Params(C.Structure):
         ("strain_ss", C.c_double), ("max_neighbors", C.c_int), ("seed", C.c_long),
         ("noise", C.c_int), ("philox_seed", C.c_ulonglong),
         ("mobility", C.c_int), ("precision", C.c_int), ("lanczos_tol", C.c_double),
-        ("lanczos_max", C.c_int),
+        ("lanczos_max", C.c_int), ("pme_grid", C.c_int), ("pme_order", C.c_int),
+        ("pme_rc", C.c_double), ("pme_alpha", C.c_double), ("pme_max_pairs", C.c_int),
     ]
 
 
@@ -148,12 +151,27 @@ def _chk(status: int, where: str) -> None:
         raise BDError(status, where)
 
 
+def pme_default_grid(L):
+    """bd_create's default particle-mesh grid: the smallest 2^a 3^b 5^c 7^d
+    at or above 1.9 L."""
+    K = int(np.ceil(1.9 * L))
+    while True:
+        r = K
+        for f in (2, 3, 5, 7):
+            while r % f == 0:
+                r //= f
+        if r == 1:
+            return K
+        K += 1
+
+
 def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3.0, kappab=0.0,
                 epsilon=1.0, lambda_b=2.0, lambda_d=5.0, Ncharges=0, barrier=3.0, barrier2=3.0,
                 MStep=100, nt_avg=8, bin_size=2.0, srpy=100, sbins=20, strain_ss=10.0,
                 max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0,
                 noise="ran1", philox_seed=20261203, mobility="hybrid", precision="fp64",
-                lanczos_tol=1e-6, lanczos_max=80) -> Params:
+                lanczos_tol=1e-6, lanczos_max=80, pme_grid=0, pme_order=0, pme_rc=0.0,
+                pme_alpha=0.0, pme_max_pairs=0) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
     p.box_volume = box_volume
@@ -167,9 +185,11 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
     p.seed = (830062920 if flow == FLOW_SHEAR else 981272199) if seed is None else seed
     p.noise = NOISE_PHILOX if noise == "philox" else NOISE_RAN1
     p.philox_seed = philox_seed
-    p.mobility = 1 if mobility == "ewald" else 0
+    p.mobility = {"hybrid": 0, "ewald": 1, "pme": 2}[mobility]
     p.precision = 1 if precision == "fp32" else 0
     p.lanczos_tol, p.lanczos_max = lanczos_tol, lanczos_max
+    p.pme_grid, p.pme_order, p.pme_rc = pme_grid, pme_order, pme_rc
+    p.pme_alpha, p.pme_max_pairs = pme_alpha, pme_max_pairs
     return p
 
 

@@ -583,10 +583,32 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   c->strain_ss = p->strain_ss > 0 ? p->strain_ss : 10.0;
   c->strain_interval = c->strain_ss / c->sbins;
   c->maxnb = p->max_neighbors > 0 ? p->max_neighbors : 256;
-  if (p->lanczos_max > 120 || p->mobility < 0 || p->mobility > 1 || p->precision < 0 ||
+  if (p->lanczos_max > 120 || p->mobility < 0 || p->mobility > 2 || p->precision < 0 ||
       p->precision > 1) {
     bd_destroy(c);
     return BD_ERR_ARG;
+  }
+  // smooth-PME discretisation
+  {
+    int K = p->pme_grid;
+    if (K <= 0) {
+      K = (int)ceil(1.9 * p->L);
+      for (;; K++) {
+        int r = K;
+        for (int f : {2, 3, 5, 7})
+          while (r % f == 0) r /= f;
+        if (r == 1) break;
+      }
+    }
+    c->pmeK = K;
+    c->pme_p = p->pme_order > 0 ? p->pme_order : 8;
+    c->pme_rc = p->pme_rc > 0 ? p->pme_rc : 10.0;
+    c->pme_alpha = p->pme_alpha > 0 ? p->pme_alpha : 4.0 / c->pme_rc;
+    if (K < 8 || K > 1024 || c->pme_p < 4 || c->pme_p > 8 || (c->pme_p & 1) ||
+        c->pme_p > K || c->pme_rc > 0.43 * p->L) {
+      bd_destroy(c);
+      return BD_ERR_ARG;
+    }
   }
   // lookup-grid geometry (initLattice, shear/src/Initialization.c:244-295,
   // extensional/src/Initialization.c:252-285)
@@ -685,6 +707,7 @@ int bd_destroy(bd_ctx* c) {
                   c->Ctab, c->Mt32, c->LV, c->Lw, c->Lpart, c->Lh, c->Lsc, c->Lc, c->MF, c->Yz};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  pme_free(c);
   prof_clear(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

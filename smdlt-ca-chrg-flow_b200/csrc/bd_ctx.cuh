@@ -89,6 +89,24 @@ struct bd_ctx {
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
   int lan_last;
 
+  // smooth-PME mobility (BD_MOB_PME)
+  int pmeK, pme_p;
+  double pme_rc, pme_alpha, pme_self;
+  bool pme_ready;
+  bool pme_f32;      // grids, spectra, influence and pair tensors in FP32
+  void *pme_grid;    // 3 x K^3 real grids
+  void *pme_spec;    // 3 x K*K*(K/2+1) complex spectra
+  void *pme_infl;    // 6 x half spectrum influence tensor
+  double *pme_bsq;   // |b_d(m)|^2, 3 x K
+  double *pme_soff;  // self-block off-diagonal (xy, xz, yz), then per-block partials
+  int pme_nblk;      // blocks of the influence kernel
+  int *pme_base;     // per bead base grid index, 3 x N
+  double *pme_w;     // per bead spline weights, 3 x N x 8
+  int pme_plan_f, pme_plan_b;
+  int rl_cap, rl_ncell_cap;  // real-space pair rows
+  int *rl_cnt, *rl_rows, *rl_cell_of, *rl_beads, *rl_cell_count, *rl_cell_start, *rl_cursor;
+  void *rl_T;        // pair tensors, 6 per pair (FP64 or FP32)
+
   size_t bytes;
 
   // profiling: CUDA events around selected kernels on the context's stream
@@ -128,6 +146,11 @@ int sym_matvec(bd_ctx* c, int R, const VecIn& v0, const VecIn& v1, double* Y0, d
 
 // charge hopping
 int charge_hop(bd_ctx* c);
+
+// smooth-PME mobility
+int pme_prepare(bd_ctx* c, const Lat& l);
+int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride);
+void pme_free(bd_ctx* c);
 
 // Krylov square root
 int alloc_lanczos(bd_ctx* c);

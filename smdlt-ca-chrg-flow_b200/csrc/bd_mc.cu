@@ -75,10 +75,13 @@ __global__ void __launch_bounds__(1024) k_charge_hop(
     Lat l, const double* __restrict__ rx, const double* __restrict__ ry,
     const double* __restrict__ rz, int N, int Nb, int nch, int* track, int* old,
     const double* __restrict__ qk_in, const double* __restrict__ rowsum, Ran1* rng,
-    double lambda_b, double kappa_d, double barrier, double barrier2, int* log) {
+    double lambda_b, double kappa_d, double barrier, double barrier2, int* log, int* gidx,
+    double* gq) {
+  // charge sites and values in shared memory, or in global scratch (gidx,
+  // gq non-null) when they do not fit
   extern __shared__ unsigned char smem[];
-  int* sidx = (int*)smem;
-  double* sq = (double*)(smem + (((size_t)nch * 4 + 15) & ~(size_t)15));
+  int* sidx = gidx ? gidx : (int*)smem;
+  double* sq = gq ? gq : (double*)(smem + (((size_t)nch * 4 + 15) & ~(size_t)15));
   __shared__ double red[33];
   __shared__ int s_first, s_c2, s_test, s_block, s_acc;
   __shared__ double s_mm;
@@ -235,11 +238,19 @@ int charge_hop(bd_ctx* c) {
   if (c->t % (unsigned long)c->p.MStep != 0) return BD_OK;
   int nch = c->nch, N = c->N;
   size_t smem = (((size_t)nch * 4 + 15) & ~(size_t)15) + 8 * (size_t)nch;
-  if (smem > 200 * 1024) return BD_ERR_ARG;  // sequential sweep holds the charges in shared memory
-  // scratch in dE: [0, 4 nch) doubles: gathered (x,y,z,q); then row sums; then qk
+  // scratch in dE (64 N doubles): [0, 4 nch) gathered (x,y,z,q); then row
+  // sums; then qk; then, for sweeps whose charges do not fit in shared
+  // memory, the working copies of the charge values and sites
   double4* cq = (double4*)c->dE;
   double* rowsum = c->dE + 4 * (size_t)nch;
   double* qk = rowsum + nch;
+  double* gq = nullptr;
+  int* gidx = nullptr;
+  if (smem > 200 * 1024) {
+    gq = qk + nch;
+    gidx = (int*)(gq + nch);
+    smem = 0;
+  }
   Lat l = c->lat;
   int treal = (int)(c->t % (unsigned long)c->tp);
   l.treal = treal;
@@ -258,7 +269,7 @@ int charge_hop(bd_ctx* c) {
   k_charge_hop<<<1, kHopThreads, smem, c->stream>>>(l, c->rx, c->ry, c->rz, N, c->Nb, nch,
                                                     c->track, c->old, qk, rowsum, c->rng,
                                                     c->p.lambda_b, c->kappa_d, c->p.barrier,
-                                                    c->p.barrier2, c->hoplog);
+                                                    c->p.barrier2, c->hoplog, gidx, gq);
   prof_end(c, BD_PROF_HOP);
   c->launches++;
   k_clear_charges<<<(N + 255) / 256, 256, 0, c->stream>>>(c->cflags, c->q, N);

@@ -745,6 +745,12 @@ static Lat step_lat(bd_ctx* c) {
 
 int calc_hi(bd_ctx* c) {
   int s;
+  if (c->p.mobility == BD_MOB_PME) {
+    prof_begin(c, BD_PROF_HI_BUILD);
+    s = pme_prepare(c, step_lat(c));
+    prof_end(c, BD_PROF_HI_BUILD);
+    return s;
+  }
   if ((s = ensure_tiles(c)) != BD_OK) return s;
   Lat l = step_lat(c);
   Ewald ew;
@@ -804,6 +810,14 @@ int calc_hi(bd_ctx* c) {
 // otherwise only the off-diagonal blocks.
 int sym_matvec(bd_ctx* c, int R, const VecIn& v0, const VecIn& v1, double* Y0, double* Y1,
                bool addiag) {
+  if (c->p.mobility == BD_MOB_PME) {
+    // the particle-mesh product always includes the diagonal blocks
+    if (!addiag) return BD_ERR_STATE;
+    int s, NTp = c->NT * 32;
+    if ((s = pme_apply(c, v0, Y0, Y0 + NTp, Y0 + 2 * NTp, 1)) != BD_OK) return s;
+    if (R == 2 && (s = pme_apply(c, v1, Y1, Y1 + NTp, Y1 + 2 * NTp, 1)) != BD_OK) return s;
+    return BD_OK;
+  }
   long long ntl = (long long)c->ntiles;
   unsigned nb = (unsigned)((ntl + 3) / 4);
   prof_begin(c, BD_PROF_MATVEC);
@@ -845,7 +859,7 @@ int update_hi(bd_ctx* c) {
     c->sbin = sb;
     c->bt = c->btab[sb];
   }
-  if (!c->hi_built) return BD_ERR_STATE;
+  if (!c->hi_built || c->p.mobility == BD_MOB_PME) return BD_ERR_STATE;
   if (c->p.flow == BD_FLOW_EXT) rotate_coords(c, 1);
   VecIn vf = {{c->fx, c->fy, c->fz}, 1};
   VecIn vr = {{c->R, c->R + 1, c->R + 2}, 3};
@@ -860,7 +874,7 @@ int update_hi(bd_ctx* c) {
 }
 
 int download_mobility(bd_ctx* c, double* M9) {
-  if (!c->hi_built) return BD_ERR_STATE;
+  if (!c->hi_built || !c->Mt) return BD_ERR_STATE;  // the PME mobility has no stored matrix
   int N = c->N, NT = c->NT;
   std::vector<double> h(c->ntiles * 6144);
   CU(cudaMemcpyAsync(h.data(), c->Mt, 8 * h.size(), cudaMemcpyDeviceToHost, c->stream));

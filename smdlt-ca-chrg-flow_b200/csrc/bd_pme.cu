@@ -1,0 +1,703 @@
+// Matrix-free Rotne-Prager-Yamakawa mobility by smooth particle-mesh Ewald.
+//
+// No counterpart in the reference, whose mobility is a dense 3N x 3N matrix
+// (calcHI, shear/src/main26.c:1530-1806).  It uses the same Beenakker Ewald
+// split as calcHI, M = M_real + M_self + M_recip:
+//  * M_real: for pairs closer than rc (lattice minimum image, rc below half
+//    the narrowest cell width) the real-space Beenakker kernel with the
+//    overlap form for r <= 2 (the C1..C4 terms of shear/src/main26.c:
+//    1727-1741); the 3x3 pair tensors are built once per step into a row
+//    list and applied as a sparse block product;
+//  * M_self: 1 - 6 alpha/sqrt(pi) + 40 alpha^3/(3 sqrt(pi)) on the diagonal;
+//  * M_recip = sum over k != 0 of (phi(k)/V)(I - k k^T/k^2) cos(k.r_ij),
+//    phi(k) = (1 - k^2/3)(1 + k^2/4a^2 + k^4/8a^4)(6 pi/k^2) exp(-k^2/4a^2)
+//    (the coefficient of shear/src/main26.c:1622), evaluated by smooth PME
+//    (Essmann et al., J. Chem. Phys. 103, 8577 (1995)) on the deforming
+//    cell: fractional coordinates s = H^-1 r, cardinal B-splines of even
+//    order p on a K^3 grid, three-component R2C FFT, multiplication by
+//    (phi/V)(I - k k^T/k^2) |b1 b2 b3|^2 with k = 2 pi H^-T m, C2R FFT and
+//    interpolation with the same weights.
+// The periodic lattice is described by its Gauss-reduced basis (shortest
+// vectors of the lattice spanned by L1, L2 and L e_z): the lattice sums do
+// not depend on the basis, and the reduced one keeps the grid spacing and the
+// minimum-image cell widths bounded over the whole deformation period
+// (|a| <= 1.16 L, widths >= 0.86 L for planar extension).
+// Two conventions of calcHI are kept so that the sum reproduces its tensor:
+//  * for overlapping beads (r < 2) its real-space form depends on the split
+//    parameter; those pairs get that dependence at calcHI's own parameter
+//    M_HI / rce (shear/src/main26.c:1536-1552) rather than at the PME one;
+//  * calcHI stores only the diagonal entries of the self blocks
+//    (shear/src/main26.c:1663-1700); the off-diagonal entries of the k-space
+//    self sum, which a sheared or stretched cell makes non-zero, are removed.
+// cuFFT is used for the transforms only.  Spreading uses FP64 atomics; the
+// spline weights and pair tensors are computed once per step because the
+// positions do not change during a Krylov solve.
+#include <cufft.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bd_ctx.cuh"
+
+using namespace bd;
+
+#define CU(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
+  } while (0)
+#define CF(call)                                  \
+  do {                                            \
+    if ((call) != CUFFT_SUCCESS) return BD_ERR_CUDA; \
+  } while (0)
+
+struct Cell {
+  double H[9];     // lattice vectors as columns (lab frame), row-major 3x3
+  double Hi[9];    // inverse
+  double V;        // volume
+};
+
+static const int kMaxOrder = 8;
+
+__device__ __forceinline__ void frac_of(const Cell& c, double x, double y, double z, double s[3]) {
+  s[0] = c.Hi[0] * x + c.Hi[1] * y + c.Hi[2] * z;
+  s[1] = c.Hi[3] * x + c.Hi[4] * y + c.Hi[5] * z;
+  s[2] = c.Hi[6] * x + c.Hi[7] * y + c.Hi[8] * z;
+}
+
+// Cardinal B-spline weights: w[k] = M_p(f + k), k = 0..p-1, for the grid point
+// floor(u) - k, from M_n(x) = (x M_{n-1}(x) + (n - x) M_{n-1}(x - 1))/(n - 1).
+__device__ __forceinline__ void bspline(double f, int p, double* w) {
+  double a[kMaxOrder], b[kMaxOrder];
+  a[0] = f;
+  a[1] = 1.0 - f;
+  for (int n = 3; n <= p; n++) {
+    for (int k = 0; k < n; k++) {
+      double hi = k < n - 1 ? a[k] : 0.0, lo = k >= 1 ? a[k - 1] : 0.0;
+      b[k] = ((f + k) * hi + (n - f - k) * lo) / (n - 1);
+    }
+    for (int k = 0; k < n; k++) a[k] = b[k];
+  }
+  for (int k = 0; k < p; k++) w[k] = a[k];
+}
+
+// Per bead: base grid index floor(u) and the p weights in each lattice
+// direction (u = K s, s wrapped into [0,1)).  Positions held in the rotated
+// frame are taken to the lab frame with (cr, sr) = (cos, sin) of the lattice
+// angle, x = x' cr - y' sr, y = x' sr + y' cr (inverseCoords,
+// extensional/src/main14.c:1525-1535); lab-frame positions pass (1, 0).
+__global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
+                              const double* __restrict__ ry, const double* __restrict__ rz,
+                              double cr, double sr, int N, int K, int p, int* base, double* w,
+                              int* err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double x = rx[i] * cr - ry[i] * sr, y = rx[i] * sr + ry[i] * cr, z = rz[i];
+  double s[3];
+  frac_of(cell, x, y, z, s);
+  for (int d = 0; d < 3; d++) {
+    double sd = s[d] - floor(s[d]);
+    double u = sd * K;
+    if (!(u >= 0.0 && u <= (double)K)) {  // non-finite position: keep indices in range
+      u = 0.0;
+      atomicOr(err, ERRB_NONFINITE);
+    }
+    int fl = (int)floor(u);
+    double f = u - fl;
+    if (fl >= K) fl -= K;
+    base[3 * i + d] = fl;
+    bspline(f, p, w + ((size_t)3 * i + d) * kMaxOrder);
+  }
+}
+
+// Q[c][g] += v_c(i) W_i(g): one warp per bead, the P^3 stencil points
+// spread over the lanes with the fastest index along the contiguous grid
+// direction, so each atomic instruction of a warp covers runs of P adjacent
+// grid values.  FP64 atomics into the grid.
+template <int P, typename R>
+__global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base,
+                                                    const double* __restrict__ w, int N, int K,
+                                                    VecIn v, R* grid) {
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= N) return;
+  double f0 = v.p[0][(size_t)i * v.stride];
+  double f1 = v.p[1][(size_t)i * v.stride];
+  double f2 = v.p[2][(size_t)i * v.stride];
+  const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
+  const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
+  const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
+  int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
+  size_t K3 = (size_t)K * K * K;
+  for (int q = lane; q < P * P * P; q += 32) {
+    int c = q % P, b = (q / P) % P, a = q / (P * P);
+    int g0 = b0 - a, g1 = b1 - b, g2 = b2 - c;
+    g0 += g0 < 0 ? K : 0;
+    g1 += g1 < 0 ? K : 0;
+    g2 += g2 < 0 ? K : 0;
+    double wt = w0[a] * w1[b] * w2[c];
+    size_t g = ((size_t)g0 * K + g1) * K + g2;
+    atomicAdd(grid + g, (R)(wt * f0));
+    atomicAdd(grid + K3 + g, (R)(wt * f1));
+    atomicAdd(grid + 2 * K3 + g, (R)(wt * f2));
+  }
+}
+
+// Influence tensor on the half spectrum: (phi(k)/V)(I - k k^T/k^2) |b|^2,
+// six components per point, zero at m = 0.
+// Also the off-diagonal entries of sum_{k != 0} (phi/V)(I - k k^T/k^2) over
+// the full spectrum (half spectrum with Hermitian multiplicity), one partial
+// sum per block in soff_part[3 * block + (xy, xz, yz)].
+template <typename R>
+__global__ void __launch_bounds__(256) k_pme_influence(Cell cell, int K, double alpha,
+                                                       const double* __restrict__ bsq, R* infl,
+                                                       double* soff_part) {
+  int Kh = K / 2 + 1;
+  size_t n = (size_t)K * K * Kh;
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double sxy = 0, sxz = 0, syz = 0;
+  __shared__ double red[3][256];
+  if (e < n) {
+    int m2 = (int)(e % Kh), m1 = (int)((e / Kh) % K), m0 = (int)(e / ((size_t)Kh * K));
+    R* o = infl + 6 * e;
+    if (m0 == 0 && m1 == 0 && m2 == 0) {
+      for (int a = 0; a < 6; a++) o[a] = (R)0;
+    } else {
+      int s0 = m0 < (K + 1) / 2 ? m0 : m0 - K, s1 = m1 < (K + 1) / 2 ? m1 : m1 - K, s2 = m2;
+      // k = 2 pi (s0 b0 + s1 b1 + s2 b2), b_d = row d of H^-1
+      double k[3];
+      for (int a = 0; a < 3; a++)
+        k[a] = 2.0 * M_PI *
+               (s0 * cell.Hi[0 * 3 + a] + s1 * cell.Hi[1 * 3 + a] + s2 * cell.Hi[2 * 3 + a]);
+      double kk = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+      double a2 = alpha * alpha;
+      double phi = (1.0 - kk / 3.0) * (1.0 + kk / (4.0 * a2) + kk * kk / (8.0 * a2 * a2)) * 6.0 *
+                   M_PI / kk * exp(-kk / (4.0 * a2)) / cell.V;
+      double f = phi * bsq[m0] * bsq[K + m1] * bsq[2 * K + m2];
+      o[0] = (R)(f * (1.0 - k[0] * k[0] / kk));
+      o[1] = (R)(f * (-k[0] * k[1] / kk));
+      o[2] = (R)(f * (-k[0] * k[2] / kk));
+      o[3] = (R)(f * (1.0 - k[1] * k[1] / kk));
+      o[4] = (R)(f * (-k[1] * k[2] / kk));
+      o[5] = (R)(f * (1.0 - k[2] * k[2] / kk));
+      double mult = (m2 == 0 || (K % 2 == 0 && m2 == K / 2)) ? 1.0 : 2.0;
+      sxy = -mult * phi * k[0] * k[1] / kk;
+      sxz = -mult * phi * k[0] * k[2] / kk;
+      syz = -mult * phi * k[1] * k[2] / kk;
+    }
+  }
+  red[0][threadIdx.x] = sxy;
+  red[1][threadIdx.x] = sxz;
+  red[2][threadIdx.x] = syz;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int a = 0; a < 3; a++) red[a][threadIdx.x] += red[a][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) soff_part[3 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Fixed-order sum of the per-block self off-diagonal partials.
+__global__ void k_pme_soff_fin(const double* __restrict__ part, int nb, double* soff) {
+  __shared__ double red[3][256];
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    a0 += part[3 * b];
+    a1 += part[3 * b + 1];
+    a2 += part[3 * b + 2];
+  }
+  red[0][threadIdx.x] = a0;
+  red[1][threadIdx.x] = a1;
+  red[2][threadIdx.x] = a2;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int a = 0; a < 3; a++) red[a][threadIdx.x] += red[a][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) soff[threadIdx.x] = red[threadIdx.x][0];
+}
+
+template <typename R, typename Cx>
+__global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size_t n) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const R* t = infl + 6 * e;
+  Cx x = spec[e], y = spec[n + e], z = spec[2 * n + e];
+  Cx u, v, w;
+  u.x = t[0] * x.x + t[1] * y.x + t[2] * z.x;
+  u.y = t[0] * x.y + t[1] * y.y + t[2] * z.y;
+  v.x = t[1] * x.x + t[3] * y.x + t[4] * z.x;
+  v.y = t[1] * x.y + t[3] * y.y + t[4] * z.y;
+  w.x = t[2] * x.x + t[4] * y.x + t[5] * z.x;
+  w.y = t[2] * x.y + t[4] * y.y + t[5] * z.y;
+  spec[e] = u;
+  spec[n + e] = v;
+  spec[2 * n + e] = w;
+}
+
+// out_c(i) = sum_g W_i(g) grid_c(g) + self * v_c(i) - S_off v(i)
+//            + sum_j T_ij v_j (row list)
+// One warp per bead: lanes share the stencil points and the pair row, then a
+// butterfly reduction.
+template <int P, typename R>
+__global__ void __launch_bounds__(256) k_pme_gather(
+    const int* __restrict__ base, const double* __restrict__ w, int N, int K,
+    const R* __restrict__ grid, double self, const double* __restrict__ soff, VecIn v,
+    const int* __restrict__ rcnt, const int* __restrict__ rrows, const R* __restrict__ rT,
+    int rcap, double* o0, double* o1, double* o2, int ostride) {
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= N) return;
+  const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
+  const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
+  const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
+  int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
+  size_t K3 = (size_t)K * K * K;
+  double u0 = 0, u1 = 0, u2 = 0;
+  for (int q = lane; q < P * P * P; q += 32) {
+    int c = q % P, b = (q / P) % P, a = q / (P * P);
+    int g0 = b0 - a, g1 = b1 - b, g2 = b2 - c;
+    g0 += g0 < 0 ? K : 0;
+    g1 += g1 < 0 ? K : 0;
+    g2 += g2 < 0 ? K : 0;
+    double wt = w0[a] * w1[b] * w2[c];
+    size_t g = ((size_t)g0 * K + g1) * K + g2;
+    u0 += wt * (double)grid[g];
+    u1 += wt * (double)grid[K3 + g];
+    u2 += wt * (double)grid[2 * K3 + g];
+  }
+  int n = rcnt[i];
+  const int* row = rrows + (size_t)i * rcap;
+  const R* T = rT + (size_t)i * rcap * 6;
+  for (int k = lane; k < n; k += 32) {
+    int j = row[k];
+    double x0 = v.p[0][(size_t)j * v.stride], x1 = v.p[1][(size_t)j * v.stride];
+    double x2 = v.p[2][(size_t)j * v.stride];
+    const R* t = T + 6 * k;
+    double t0 = t[0], t1 = t[1], t2 = t[2], t3 = t[3], t4 = t[4], t5 = t[5];
+    u0 += t0 * x0 + t1 * x1 + t2 * x2;
+    u1 += t1 * x0 + t3 * x1 + t4 * x2;
+    u2 += t2 * x0 + t4 * x1 + t5 * x2;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    u0 += __shfl_xor_sync(0xffffffffu, u0, o);
+    u1 += __shfl_xor_sync(0xffffffffu, u1, o);
+    u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+  }
+  if (lane == 0) {
+    double vi0 = v.p[0][(size_t)i * v.stride], vi1 = v.p[1][(size_t)i * v.stride];
+    double vi2 = v.p[2][(size_t)i * v.stride];
+    double sxy = soff[0], sxz = soff[1], syz = soff[2];
+    o0[(size_t)i * ostride] = u0 + self * vi0 - sxy * vi1 - sxz * vi2;
+    o1[(size_t)i * ostride] = u1 + self * vi1 - sxy * vi0 - syz * vi2;
+    o2[(size_t)i * ostride] = u2 + self * vi2 - sxz * vi0 - syz * vi1;
+  }
+}
+
+// Real-space Beenakker kernel t1 I + t2 r r^T/r^2 (shear/src/main26.c:
+// 1727-1741) at split parameter alpha; with far the r > 2 form at any r.
+__device__ __forceinline__ void real_kernel(double alpha, double rr, bool far, double& t1,
+                                            double& t2) {
+  double r = sqrt(rr), a = alpha, a2 = a * a, a3 = a2 * a, a5 = a3 * a2, a7 = a5 * a2;
+  double C1, C2, C3, C4;
+  if (far || r > 2.0) {
+    C1 = 0.75 / r + 0.5 / (r * rr);
+    C2 = 4.0 * a7 * rr * rr + 3.0 * a3 * rr - 20.0 * a5 * rr - 4.5 * a + 14.0 * a3 + a / rr;
+    C3 = 0.75 / r - 1.5 / (r * rr);
+    C4 = -4.0 * a7 * rr * rr - 3.0 * a3 * rr + 16.0 * a5 * rr + 1.5 * a - 2.0 * a3 - 3.0 * a / rr;
+  } else {
+    C1 = 1.0 - 0.28125 * r;
+    C2 = 64.0 * a7 + 12.0 * a3 - 80.0 * a5 - 4.5 * a + 14.0 * a3 + 0.25 * a;
+    C3 = 0.09375 * r;
+    C4 = -64.0 * a7 - 12.0 * a3 + 64.0 * a5 + 1.5 * a - 2.0 * a3 - 0.75 * a;
+  }
+  double ec = erfc(a * r), ex = exp(-a2 * rr) / sqrt(M_PI);
+  t1 = C1 * ec + C2 * ex;
+  t2 = C3 * ec + C4 * ex;
+}
+
+// Cells of the real-space list (fractional, width >= rc).
+struct RGeom {
+  int n[3];
+};
+
+__device__ __forceinline__ int rcell(const Cell& cell, const RGeom& g, double x, double y, double z,
+                                     int* cd) {
+  double s[3];
+  frac_of(cell, x, y, z, s);
+  for (int d = 0; d < 3; d++) {
+    double sd = s[d] - floor(s[d]);
+    int c = (sd >= 0.0 && sd <= 1.0) ? (int)(sd * g.n[d]) : 0;  // 0 for non-finite input
+    cd[d] = c >= g.n[d] ? g.n[d] - 1 : c;
+  }
+  return (cd[0] * g.n[1] + cd[1]) * g.n[2] + cd[2];
+}
+
+__global__ void k_rl_count(Cell cell, RGeom g, const double* __restrict__ rx,
+                           const double* __restrict__ ry, const double* __restrict__ rz,
+                           double cr, double sr, int N, int* cell_of, int* cell_count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int cd[3];
+  double x = rx[i] * cr - ry[i] * sr, y = rx[i] * sr + ry[i] * cr;
+  int c = rcell(cell, g, x, y, rz[i], cd);
+  cell_of[i] = c;
+  atomicAdd(&cell_count[c], 1);
+}
+
+__global__ void k_rl_scan(int ncell, int* cell_count, int* cell_start, int* cursor) {
+  __shared__ int part[1024];
+  int t = threadIdx.x, nt = blockDim.x;
+  int per = (ncell + nt - 1) / nt, lo = t * per, hi = min(ncell, lo + per), s = 0;
+  for (int c = lo; c < hi; c++) s += cell_count[c];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < nt; o <<= 1) {
+    int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int b = part[t] - s;
+  for (int c = lo; c < hi; c++) {
+    cell_start[c] = b;
+    cursor[c] = 0;
+    b += cell_count[c];
+    cell_count[c] = 0;
+  }
+  if (t == nt - 1) cell_start[ncell] = part[t];
+}
+
+__global__ void k_rl_fill(const int* __restrict__ cell_of, const int* __restrict__ cell_start,
+                          int* cursor, int* beads, int N) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int c = cell_of[i];
+  beads[cell_start[c] + atomicAdd(&cursor[c], 1)] = i;
+}
+
+// Pairs within rc (lattice minimum image) and their 3x3 real-space tensors.
+template <typename R>
+__global__ void k_rl_rows(Cell cell, RGeom g, const double* __restrict__ rx,
+                          const double* __restrict__ ry, const double* __restrict__ rz,
+                          double cr, double sr, int N, const int* __restrict__ cell_start,
+                          const int* __restrict__ beads, double rc2, double alpha,
+                          double alpha_ref, int rcap, int* cnt, int* rows, R* T, int* err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double xi = rx[i] * cr - ry[i] * sr, yi = rx[i] * sr + ry[i] * cr, zi = rz[i];
+  int cd[3];
+  rcell(cell, g, xi, yi, zi, cd);
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; d++) {
+    lo[d] = g.n[d] >= 3 ? -1 : 0;
+    hi[d] = g.n[d] >= 3 ? 1 : g.n[d] - 1;
+  }
+  int n = 0;
+  bool over = false;
+  for (int a = lo[0]; a <= hi[0]; a++)
+    for (int b = lo[1]; b <= hi[1]; b++)
+      for (int c = lo[2]; c <= hi[2]; c++) {
+        int e0 = g.n[0] >= 3 ? (cd[0] + a + g.n[0]) % g.n[0] : a;
+        int e1 = g.n[1] >= 3 ? (cd[1] + b + g.n[1]) % g.n[1] : b;
+        int e2 = g.n[2] >= 3 ? (cd[2] + c + g.n[2]) % g.n[2] : c;
+        int cc = (e0 * g.n[1] + e1) * g.n[2] + e2;
+        for (int q = cell_start[cc]; q < cell_start[cc + 1]; q++) {
+          int j = beads[q];
+          if (j == i) continue;
+          double dx = (rx[j] * cr - ry[j] * sr) - xi, dy = (rx[j] * sr + ry[j] * cr) - yi;
+          double dz = rz[j] - zi, s[3];
+          frac_of(cell, dx, dy, dz, s);
+          for (int d = 0; d < 3; d++) s[d] -= rint(s[d]);
+          dx = cell.H[0] * s[0] + cell.H[1] * s[1] + cell.H[2] * s[2];
+          dy = cell.H[3] * s[0] + cell.H[4] * s[1] + cell.H[5] * s[2];
+          dz = cell.H[6] * s[0] + cell.H[7] * s[1] + cell.H[8] * s[2];
+          double rr = dx * dx + dy * dy + dz * dz;
+          if (rr >= rc2) continue;
+          if (n >= rcap) {
+            over = true;
+            continue;
+          }
+          double t1, t2;
+          real_kernel(alpha, rr, false, t1, t2);
+          if (rr < 4.0) {
+            // overlap: far form at alpha plus calcHI's overlap correction at
+            // its own split parameter
+            double f1, f2, o1, o2, g1, g2;
+            real_kernel(alpha, rr, true, f1, f2);
+            real_kernel(alpha_ref, rr, false, o1, o2);
+            real_kernel(alpha_ref, rr, true, g1, g2);
+            t1 = f1 + (o1 - g1);
+            t2 = f2 + (o2 - g2);
+          }
+          R* o = T + ((size_t)i * rcap + n) * 6;
+          o[0] = (R)(t1 + t2 * dx * dx / rr);
+          o[1] = (R)(t2 * dx * dy / rr);
+          o[2] = (R)(t2 * dx * dz / rr);
+          o[3] = (R)(t1 + t2 * dy * dy / rr);
+          o[4] = (R)(t2 * dy * dz / rr);
+          o[5] = (R)(t1 + t2 * dz * dz / rr);
+          rows[(size_t)i * rcap + n] = j;
+          n++;
+        }
+      }
+  cnt[i] = n;
+  if (over) atomicOr(err, ERRB_NBR_OVERFLOW);
+}
+
+static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
+
+// Lab-frame cell of the current lattice: columns b1, b2, L e_z with (b1, b2)
+// the Gauss-reduced basis of the lattice spanned by L1 and L2
+// (|b1| <= |b2|, |b1.b2| <= |b1|^2/2).
+static Cell make_cell(const Lat& l) {
+  Cell c;
+  double a[2] = {l.L1x, l.L1y}, b[2] = {l.L2x, l.L2y};
+  for (int it = 0; it < 64; it++) {
+    double aa = a[0] * a[0] + a[1] * a[1], bb = b[0] * b[0] + b[1] * b[1];
+    if (aa > bb) {
+      std::swap(a[0], b[0]);
+      std::swap(a[1], b[1]);
+      std::swap(aa, bb);
+    }
+    double mu = rint((a[0] * b[0] + a[1] * b[1]) / aa);
+    if (mu == 0.0) break;
+    b[0] -= mu * a[0];
+    b[1] -= mu * a[1];
+  }
+  double H[9] = {a[0], b[0], 0.0, a[1], b[1], 0.0, 0.0, 0.0, l.L};
+  memcpy(c.H, H, sizeof(H));
+  double det = H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
+               H[2] * (H[3] * H[7] - H[4] * H[6]);
+  c.V = fabs(det);
+  double* I = c.Hi;
+  I[0] = (H[4] * H[8] - H[5] * H[7]) / det;
+  I[1] = (H[2] * H[7] - H[1] * H[8]) / det;
+  I[2] = (H[1] * H[5] - H[2] * H[4]) / det;
+  I[3] = (H[5] * H[6] - H[3] * H[8]) / det;
+  I[4] = (H[0] * H[8] - H[2] * H[6]) / det;
+  I[5] = (H[2] * H[3] - H[0] * H[5]) / det;
+  I[6] = (H[3] * H[7] - H[4] * H[6]) / det;
+  I[7] = (H[1] * H[6] - H[0] * H[7]) / det;
+  I[8] = (H[0] * H[4] - H[1] * H[3]) / det;
+  return c;
+}
+
+// |b(m)|^2 = 1/|sum_{k=0}^{p-2} M_p(k+1) exp(2 pi i m k / K)|^2
+static void bspline_moduli(int K, int p, double* out) {
+  std::vector<double> Mk(p + 1, 0.0);
+  // M_p at the integers 1..p-1 from the same recursion (f = 0)
+  std::vector<double> a = {0.0, 1.0};
+  for (int n = 3; n <= p; n++) {
+    std::vector<double> b(n, 0.0);
+    for (int k = 0; k < n; k++) {
+      double hi = k < n - 1 ? a[k] : 0.0, lo = k >= 1 ? a[k - 1] : 0.0;
+      b[k] = (k * hi + (n - k) * lo) / (n - 1);
+    }
+    a = b;
+  }
+  for (int m = 0; m < K; m++) {
+    double re = 0, im = 0;
+    for (int k = 0; k <= p - 2; k++) {
+      double w = a[k + 1];  // M_p(k + 1)
+      re += w * cos(2 * M_PI * m * k / K);
+      im += w * sin(2 * M_PI * m * k / K);
+    }
+    double d = re * re + im * im;
+    out[m] = d > 1e-300 ? 1.0 / d : 0.0;
+  }
+}
+
+namespace bd {
+
+int pme_alloc(bd_ctx* c) {
+  if (c->pme_grid) return BD_OK;
+  int K = c->pmeK, N = c->N;
+  size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
+  c->pme_f32 = c->p.precision == BD_PREC_FP32;
+  size_t es = c->pme_f32 ? 4 : 8;  // grid, spectrum, influence and pair tensors
+  CU(cudaMalloc(&c->pme_grid, es * 3 * K3));
+  CU(cudaMalloc(&c->pme_spec, 2 * es * 3 * Ks));
+  CU(cudaMalloc(&c->pme_infl, es * 6 * Ks));
+  CU(cudaMalloc(&c->pme_bsq, 8 * 3 * (size_t)K));
+  c->pme_nblk = (int)((Ks + 255) / 256);
+  CU(cudaMalloc(&c->pme_soff, 8 * (3 * (size_t)c->pme_nblk + 3)));
+  CU(cudaMalloc(&c->pme_base, 4 * 3 * (size_t)N));
+  CU(cudaMalloc(&c->pme_w, 8 * 3 * (size_t)N * kMaxOrder));
+  c->rl_cap = c->p.pme_max_pairs > 0 ? c->p.pme_max_pairs : 512;
+  CU(cudaMalloc(&c->rl_cnt, 4 * (size_t)N));
+  CU(cudaMalloc(&c->rl_rows, 4 * (size_t)N * c->rl_cap));
+  CU(cudaMalloc(&c->rl_T, es * 6 * (size_t)N * c->rl_cap));
+  c->rl_ncell_cap = 4096;
+  CU(cudaMalloc(&c->rl_cell_of, 4 * (size_t)N));
+  CU(cudaMalloc(&c->rl_beads, 4 * (size_t)N));
+  CU(cudaMalloc(&c->rl_cell_count, 4 * (size_t)c->rl_ncell_cap));
+  CU(cudaMalloc(&c->rl_cell_start, 4 * (size_t)(c->rl_ncell_cap + 1)));
+  CU(cudaMalloc(&c->rl_cursor, 4 * (size_t)c->rl_ncell_cap));
+  CU(cudaMemsetAsync(c->rl_cell_count, 0, 4 * (size_t)c->rl_ncell_cap, c->stream));
+  c->bytes += es * (3 * K3 + 6 * Ks + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
+              24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 6 * es) +
+              8 * (size_t)N + 12 * (size_t)c->rl_ncell_cap;
+  int n[3] = {K, K, K};
+  cufftHandle f, b;
+  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
+                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3));
+  CF(cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
+                   c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3));
+  CF(cufftSetStream(f, c->stream));
+  CF(cufftSetStream(b, c->stream));
+  c->pme_plan_f = (int)f;
+  c->pme_plan_b = (int)b;
+  std::vector<double> bs(3 * (size_t)K);
+  bspline_moduli(K, c->pme_p, bs.data());
+  for (int d = 1; d < 3; d++)
+    for (int m = 0; m < K; m++) bs[(size_t)d * K + m] = bs[m];
+  CU(cudaMemcpyAsync(c->pme_bsq, bs.data(), 8 * bs.size(), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return BD_OK;
+}
+
+void pme_free(bd_ctx* c) {
+  if (c->pme_plan_f) cufftDestroy((cufftHandle)c->pme_plan_f);
+  if (c->pme_plan_b) cufftDestroy((cufftHandle)c->pme_plan_b);
+  void* ptrs[] = {c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
+                  c->rl_cnt, c->rl_rows, c->rl_T, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
+                  c->rl_cell_start, c->rl_cursor};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+}
+
+// Preparation for the current positions, in the frame calcHI reads them
+// (extension: rotated by the lattice angle, taken to the lab frame here):
+// spline weights, influence tensor of the current cell, self off-diagonal
+// sums, real-space pair list and tensors.  The products that follow use this
+// configuration until the next preparation, as the dense matrix does.
+int pme_prepare(bd_ctx* c, const Lat& l) {
+  int s;
+  if ((s = pme_alloc(c)) != BD_OK) return s;
+  Cell cell = make_cell(l);
+  double cr = 1.0, sr = 0.0;
+  if (l.flow == BD_FLOW_EXT) {
+    cr = l.cth;
+    sr = l.sth;
+  }
+  double rc = c->pme_rc, alpha = c->pme_alpha;
+  int K = c->pmeK, N = c->N;
+  // calcHI's split parameter at this step, for its overlap convention
+  double rce = l.treal <= c->tp / 2 ? l.L2yp : 2.0 * l.L2yp;
+  double alpha_ref = 4.0 / rce;
+  c->launches += 3;
+  k_pme_weights<<<nblk(N, 256), 256, 0, c->stream>>>(cell, c->rx, c->ry, c->rz, cr, sr, N, K,
+                                                     c->pme_p, c->pme_base, c->pme_w, c->err);
+  if (c->pme_f32)
+    k_pme_influence<float><<<c->pme_nblk, 256, 0, c->stream>>>(
+        cell, K, alpha, c->pme_bsq, (float*)c->pme_infl, c->pme_soff + 3);
+  else
+    k_pme_influence<double><<<c->pme_nblk, 256, 0, c->stream>>>(
+        cell, K, alpha, c->pme_bsq, (double*)c->pme_infl, c->pme_soff + 3);
+  k_pme_soff_fin<<<1, 256, 0, c->stream>>>(c->pme_soff + 3, c->pme_nblk, c->pme_soff);
+  // real-space cells: perpendicular widths V/|a_j x a_k|
+  double w[3];
+  {
+    const double* H = cell.H;
+    double a[3][3];
+    for (int j = 0; j < 3; j++)
+      for (int d = 0; d < 3; d++) a[j][d] = H[d * 3 + j];
+    for (int j = 0; j < 3; j++) {
+      const double* u = a[(j + 1) % 3];
+      const double* v = a[(j + 2) % 3];
+      double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2],
+             cz = u[0] * v[1] - u[1] * v[0];
+      w[j] = cell.V / sqrt(cx * cx + cy * cy + cz * cz);
+    }
+  }
+  if (2 * rc > std::min(w[0], std::min(w[1], w[2]))) return BD_ERR_ARG;  // rc beyond half a width
+  RGeom g;
+  for (int d = 0; d < 3; d++) g.n[d] = std::max(1, (int)floor(w[d] / rc));
+  while ((long)g.n[0] * g.n[1] * g.n[2] > c->rl_ncell_cap) {
+    int d = g.n[0] >= g.n[1] && g.n[0] >= g.n[2] ? 0 : (g.n[1] >= g.n[2] ? 1 : 2);
+    g.n[d]--;
+  }
+  int ncell = g.n[0] * g.n[1] * g.n[2];
+  c->launches += 4;
+  k_rl_count<<<nblk(N, 256), 256, 0, c->stream>>>(cell, g, c->rx, c->ry, c->rz, cr, sr, N,
+                                                  c->rl_cell_of, c->rl_cell_count);
+  k_rl_scan<<<1, 1024, 0, c->stream>>>(ncell, c->rl_cell_count, c->rl_cell_start, c->rl_cursor);
+  k_rl_fill<<<nblk(N, 256), 256, 0, c->stream>>>(c->rl_cell_of, c->rl_cell_start, c->rl_cursor,
+                                                 c->rl_beads, N);
+#define PME_ROWS(R_)                                                                        \
+  k_rl_rows<R_><<<nblk(N, 128), 128, 0, c->stream>>>(                                      \
+      cell, g, c->rx, c->ry, c->rz, cr, sr, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha, \
+      alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (R_*)c->rl_T, c->err)
+  if (c->pme_f32)
+    PME_ROWS(float);
+  else
+    PME_ROWS(double);
+#undef PME_ROWS
+  double a = alpha;
+  c->pme_self = 1.0 - 6.0 / sqrt(M_PI) * a + 40.0 / (3.0 * sqrt(M_PI)) * a * a * a;
+  c->Dtr[0] = c->Dtr[1] = c->Dtr[2] = c->pme_self;
+  c->pme_ready = true;
+  c->hi_built = true;
+  return launch_ok(c);
+}
+
+// out = M v by PME for one vector given by component pointers (VecIn).
+template <typename R, typename Cx>
+static int pme_apply_t(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2,
+                       int ostride) {
+  int K = c->pmeK, N = c->N, p = c->pme_p;
+  size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
+  R* grid = (R*)c->pme_grid;
+  Cx* spec = (Cx*)c->pme_spec;
+  CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3, c->stream));
+  c->launches += 3;  // spread, influence, gather (the transforms are cuFFT's)
+  int nb8 = nblk(N, 8);
+#define PME_SPREAD(P_) \
+  k_pme_spread<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, grid)
+  switch (p) {
+    case 4: PME_SPREAD(4); break;
+    case 6: PME_SPREAD(6); break;
+    default: PME_SPREAD(8);
+  }
+#undef PME_SPREAD
+  if constexpr (sizeof(R) == 4)
+    CF(cufftExecR2C((cufftHandle)c->pme_plan_f, (cufftReal*)grid, (cufftComplex*)spec));
+  else
+    CF(cufftExecD2Z((cufftHandle)c->pme_plan_f, (cufftDoubleReal*)grid,
+                    (cufftDoubleComplex*)spec));
+  k_pme_apply_influence<R, Cx><<<nblk((long long)Ks, 256), 256, 0, c->stream>>>(
+      (const R*)c->pme_infl, spec, Ks);
+  if constexpr (sizeof(R) == 4)
+    CF(cufftExecC2R((cufftHandle)c->pme_plan_b, (cufftComplex*)spec, (cufftReal*)grid));
+  else
+    CF(cufftExecZ2D((cufftHandle)c->pme_plan_b, (cufftDoubleComplex*)spec,
+                    (cufftDoubleReal*)grid));
+#define PME_GATHER(P_)                                                                        \
+  k_pme_gather<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, grid,           \
+                                                  c->pme_self, c->pme_soff, v, c->rl_cnt,       \
+                                                  c->rl_rows, (const R*)c->rl_T, c->rl_cap, o0, \
+                                                  o1, o2, ostride)
+  switch (p) {
+    case 4: PME_GATHER(4); break;
+    case 6: PME_GATHER(6); break;
+    default: PME_GATHER(8);
+  }
+#undef PME_GATHER
+  return BD_OK;
+}
+
+int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride) {
+  if (!c->pme_ready) return BD_ERR_STATE;
+  prof_begin(c, BD_PROF_MATVEC);
+  int s = c->pme_f32 ? pme_apply_t<float, cufftComplex>(c, v, o0, o1, o2, ostride)
+                     : pme_apply_t<double, cufftDoubleComplex>(c, v, o0, o1, o2, ostride);
+  prof_end(c, BD_PROF_MATVEC);
+  if (s != BD_OK) return s;
+  return launch_ok(c);
+}
+
+}  // namespace bd
