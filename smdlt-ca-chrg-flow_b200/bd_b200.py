@@ -153,8 +153,8 @@ def _chk(status: int, where: str) -> None:
 
 def pme_default_grid(L):
     """bd_create's default particle-mesh grid: the smallest 2^a 3^b 5^c 7^d
-    at or above 1.9 L."""
-    K = int(np.ceil(1.9 * L))
+    at or above 1.5 L."""
+    K = int(np.ceil(1.5 * L))
     while True:
         r = K
         for f in (2, 3, 5, 7):
@@ -170,7 +170,7 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
                 MStep=100, nt_avg=8, bin_size=2.0, srpy=100, sbins=20, strain_ss=10.0,
                 max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0,
                 noise="ran1", philox_seed=20261203, mobility="hybrid", precision="fp64",
-                lanczos_tol=1e-6, lanczos_max=80, pme_grid=0, pme_order=0, pme_rc=0.0,
+                lanczos_tol=1e-6, lanczos_max=0, pme_grid=0, pme_order=0, pme_rc=0.0,
                 pme_alpha=0.0, pme_max_pairs=0) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt

@@ -583,7 +583,7 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   c->strain_ss = p->strain_ss > 0 ? p->strain_ss : 10.0;
   c->strain_interval = c->strain_ss / c->sbins;
   c->maxnb = p->max_neighbors > 0 ? p->max_neighbors : 256;
-  if (p->lanczos_max > 120 || p->mobility < 0 || p->mobility > 2 || p->precision < 0 ||
+  if (p->lanczos_max > kMaxKrylov || p->mobility < 0 || p->mobility > 2 || p->precision < 0 ||
       p->precision > 1) {
     bd_destroy(c);
     return BD_ERR_ARG;
@@ -592,7 +592,7 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   {
     int K = p->pme_grid;
     if (K <= 0) {
-      K = (int)ceil(1.9 * p->L);
+      K = (int)ceil(1.5 * p->L);
       for (;; K++) {
         int r = K;
         for (int f : {2, 3, 5, 7})

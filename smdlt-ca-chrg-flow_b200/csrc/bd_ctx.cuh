@@ -18,6 +18,9 @@
 
 #include "bd_internal.cuh"
 
+// Largest Krylov dimension of the Lanczos square root.
+constexpr int kMaxKrylov = 400;
+
 struct bd_ctx {
   bd_params p;
   int N, Nb, Nc;

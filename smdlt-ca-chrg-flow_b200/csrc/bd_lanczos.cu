@@ -31,13 +31,24 @@ using namespace bd;
 
 static const int kDotBlocks = 148;  // one CTA per SM for the vector reductions
 
-// sc[0] = sqrt(sum of part) = |w|, sc[1] = 1/|w|
-__global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc) {
-  if (threadIdx.x) return;
+// Fixed-order sum of n partials by one warp: lane-strided sums, then a
+// butterfly; every lane returns the same value.
+__device__ __forceinline__ double warp_sum_parts(const double* __restrict__ part, int n,
+                                                 int stride) {
+  int lane = threadIdx.x & 31;
   double s = 0;
-  for (int b = 0; b < nblk; b++) s += part[b];
-  sc[0] = sqrt(s);
-  sc[1] = sc[0] > 0 ? 1.0 / sc[0] : 0.0;
+  for (int b = lane; b < n; b += 32) s += part[(size_t)b * stride];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// sc[0] = sqrt(sum of part) = |w|, sc[1] = 1/|w| (one warp)
+__global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc) {
+  double s = warp_sum_parts(part, nblk, 1);
+  if (threadIdx.x == 0) {
+    sc[0] = sqrt(s);
+    sc[1] = sc[0] > 0 ? 1.0 / sc[0] : 0.0;
+  }
 }
 
 // v (SoA, padded) = z (bead-interleaved) / |z|; padding entries are zero
@@ -75,26 +86,65 @@ __device__ __forceinline__ void chunk_range(int n, int& lo, int& hi) {
   hi = min(n, lo + per);
 }
 
-// one warp per vector k (strided): lanes over the chunk, shuffle reduction
+// Dots of four vectors at a time per warp (vectors k0..k0+3, warps strided
+// by groups): lanes over the chunk, so each lane keeps several independent
+// loads in flight; butterfly reductions.
 __device__ __forceinline__ void chunk_dots(const double* __restrict__ V, size_t vs, int nv,
                                            const double* __restrict__ w, int lo, int hi,
                                            double* part) {
   int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k = wp; k < nv; k += nw) {
-    const double* v = V + (size_t)k * vs;
-    double s = 0;
-    for (int i = lo + lane; i < hi; i += 32) s += v[i] * w[i];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) part[(size_t)k * gridDim.x + blockIdx.x] = s;
+  for (int k0 = 4 * wp; k0 < nv; k0 += 4 * nw) {
+    const double* v0 = V + (size_t)k0 * vs;
+    const double* v1 = V + (size_t)min(k0 + 1, nv - 1) * vs;
+    const double* v2 = V + (size_t)min(k0 + 2, nv - 1) * vs;
+    const double* v3 = V + (size_t)min(k0 + 3, nv - 1) * vs;
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i = lo + lane; i < hi; i += 32) {
+      double x = w[i];
+      s0 += v0[i] * x;
+      s1 += v1[i] * x;
+      s2 += v2[i] * x;
+      s3 += v3[i] * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+    }
+    if (lane == 0) {
+      part[(size_t)k0 * gridDim.x + blockIdx.x] = s0;
+      if (k0 + 1 < nv) part[(size_t)(k0 + 1) * gridDim.x + blockIdx.x] = s1;
+      if (k0 + 2 < nv) part[(size_t)(k0 + 2) * gridDim.x + blockIdx.x] = s2;
+      if (k0 + 3 < nv) part[(size_t)(k0 + 3) * gridDim.x + blockIdx.x] = s3;
+    }
   }
 }
 
-// h[k] = sum_b part[k][b] into shared memory (every CTA, same order)
+// sum_k h[k] V_k[i] with eight independent partial sums (loads in flight),
+// combined in a fixed order.
+__device__ __forceinline__ double combo_row(const double* __restrict__ V, size_t vs,
+                                            const double* h, int nv, int i) {
+  double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int k = 0;
+  for (; k + 8 <= nv; k += 8) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) a[q] += h[k + q] * V[(size_t)(k + q) * vs + i];
+  }
+  double t = 0;
+  for (; k < nv; k++) t += h[k] * V[(size_t)k * vs + i];
+  a[0] += t;
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
+
+// h[k] = sum_b part[k][b] into shared memory, one warp per k (every CTA,
+// same order)
 __device__ __forceinline__ void sum_parts(const double* __restrict__ part, int nv, double* h) {
-  for (int k = threadIdx.x; k < nv; k += blockDim.x) {
-    double s = 0;
-    for (int b = 0; b < (int)gridDim.x; b++) s += part[(size_t)k * gridDim.x + b];
-    h[k] = s;
+  int wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = wp; k < nv; k += nw) {
+    double s = warp_sum_parts(part + (size_t)k * gridDim.x, gridDim.x, 1);
+    if ((threadIdx.x & 31) == 0) h[k] = s;
   }
   __syncthreads();
 }
@@ -110,17 +160,13 @@ __global__ void __launch_bounds__(256) k_orth0(const double* __restrict__ V, siz
 __global__ void __launch_bounds__(256) k_orth1(const double* __restrict__ V, size_t vs, int nv,
                                                double* w, int n, const double* __restrict__ part1,
                                                double* part2, double* hsave) {
-  __shared__ double h[128];
+  __shared__ double h[kMaxKrylov + 1];
   int lo, hi;
   chunk_range(n, lo, hi);
   sum_parts(part1, nv, h);
   if (blockIdx.x == 0)
     for (int k = threadIdx.x; k < nv; k += blockDim.x) hsave[k] = h[k];
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double s = 0;
-    for (int k = 0; k < nv; k++) s += h[k] * V[(size_t)k * vs + i];
-    w[i] -= s;
-  }
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) w[i] -= combo_row(V, vs, h, nv, i);
   __syncthreads();
   chunk_dots(V, vs, nv, w, lo, hi, part2);
 }
@@ -129,16 +175,14 @@ __global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, siz
                                                double* w, int n, const double* __restrict__ part2,
                                                double* part3, const double* __restrict__ hsave,
                                                double* alpha, int j) {
-  __shared__ double h[128];
+  __shared__ double h[kMaxKrylov + 1];
   __shared__ double red[8];
   int lo, hi;
   chunk_range(n, lo, hi);
   sum_parts(part2, nv, h);
   double s2 = 0;
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double s = 0;
-    for (int k = 0; k < nv; k++) s += h[k] * V[(size_t)k * vs + i];
-    double x = w[i] - s;
+    double x = w[i] - combo_row(V, vs, h, nv, i);
     w[i] = x;
     s2 += x * x;
   }
@@ -157,11 +201,12 @@ __global__ void __launch_bounds__(256) k_orth3(const double* __restrict__ w, int
                                                const double* __restrict__ part3, double* beta,
                                                int j, double* vnext, int write_next) {
   __shared__ double b;
-  if (threadIdx.x == 0) {
-    double s = 0;
-    for (int q = 0; q < (int)gridDim.x; q++) s += part3[q];
-    b = sqrt(s);
-    if (blockIdx.x == 0) beta[j] = b;
+  if (threadIdx.x < 32) {
+    double s = warp_sum_parts(part3, gridDim.x, 1);
+    if (threadIdx.x == 0) {
+      b = sqrt(s);
+      if (blockIdx.x == 0) beta[j] = b;
+    }
   }
   __syncthreads();
   if (!write_next) return;
@@ -290,7 +335,7 @@ namespace bd {
 
 int alloc_lanczos(bd_ctx* c) {
   if (c->LV) return BD_OK;
-  c->lmax = c->p.lanczos_max > 0 ? c->p.lanczos_max : 80;
+  c->lmax = c->p.lanczos_max > 0 ? c->p.lanczos_max : 200;
   c->ltol = c->p.lanczos_tol > 0 ? c->p.lanczos_tol : 1e-6;
   size_t n = 3 * (size_t)c->NT * 32;
   CU(cudaMalloc(&c->LV, 8 * n * (c->lmax + 1)));

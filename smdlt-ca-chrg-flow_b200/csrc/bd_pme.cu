@@ -130,7 +130,12 @@ __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
   int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
   size_t K3 = (size_t)K * K * K;
-  for (int q = lane; q < P * P * P; q += 32) {
+  // fully unrolled: the stencil index of each lane is a compile-time
+  // function of the iteration, so the weights stay in registers
+#pragma unroll
+  for (int it = 0; it < (P * P * P + 31) / 32; it++) {
+    int q = lane + 32 * it;
+    if (q >= P * P * P) break;
     int c = q % P, b = (q / P) % P, a = q / (P * P);
     int g0 = b0 - a, g1 = b1 - b, g2 = b2 - c;
     g0 += g0 < 0 ? K : 0;
@@ -256,7 +261,10 @@ __global__ void __launch_bounds__(256) k_pme_gather(
   int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
   size_t K3 = (size_t)K * K * K;
   double u0 = 0, u1 = 0, u2 = 0;
-  for (int q = lane; q < P * P * P; q += 32) {
+#pragma unroll
+  for (int it = 0; it < (P * P * P + 31) / 32; it++) {
+    int q = lane + 32 * it;
+    if (q >= P * P * P) break;
     int c = q % P, b = (q / P) % P, a = q / (P * P);
     int g0 = b0 - a, g1 = b1 - b, g2 = b2 - c;
     g0 += g0 < 0 ? K : 0;
