@@ -59,6 +59,18 @@ typedef enum { BD_NOISE_RAN1 = 0, BD_NOISE_PHILOX = 1 } bd_noise;
  * counterpart; O(N + K^3 log K) per product, for systems whose dense
  * matrix does not fit). */
 typedef enum { BD_MOB_HYBRID = 0, BD_MOB_EWALD = 1, BD_MOB_PME = 2 } bd_mobility_kind;
+/* Preconditioner of the Lanczos square root (no reference counterpart):
+ * none; segment blocks (G = L^-1 from the Cholesky factor of the free-space
+ * RPY mobility of S consecutive beads of a chain); per-bead 3x3 blocks
+ * predicted by the learned message-passing network; or per-bead blocks set
+ * by the caller.  The displacement is G^-1 sqrt(G M G^T) z. */
+typedef enum {
+  BD_PRECOND_NONE = 0,
+  BD_PRECOND_SEGMENT = 1,
+  BD_PRECOND_LEARNED = 2,
+  BD_PRECOND_BLOCKS = 3
+} bd_precond_kind;
+#define BD_PRECOND_MAX_SEGMENT 25
 /* Storage of the packed mobility tiles used by the products: FP64, or FP32
  * with FP64 accumulation. */
 typedef enum { BD_PREC_FP64 = 0, BD_PREC_FP32 = 1 } bd_precision;
@@ -247,6 +259,49 @@ int bd_step_lanczos(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 /* One reference-mode hydrodynamic step (the body of the step loop,
  * shear/src/main26.c:65-151, extensional/src/main14.c:68-171, without file
  * output), repeated nsteps times from step t0. */
+/* ---- Lanczos preconditioner (no reference counterpart) ------------------
+ * kind: bd_precond_kind; segment: beads per block for BD_PRECOND_SEGMENT
+ * (must divide Nb, at most BD_PRECOND_MAX_SEGMENT; 0 -> 10 or the largest of
+ * 5, 4, 2, 1 dividing Nb).  Blocks are rebuilt with every mobility build.  A
+ * preconditioned solve that misses lanczos_tol within lanczos_max is redone
+ * without the preconditioner (counted as a fallback). */
+int bd_set_preconditioner(bd_ctx *ctx, int kind, int segment);
+/* per-bead blocks G (9 N, row-major 3x3) for BD_PRECOND_BLOCKS */
+int bd_set_precond_blocks(bd_ctx *ctx, const double *G9);
+/* current blocks: N/S blocks of (3S)^2 row-major values each */
+int bd_download_precond_blocks(bd_ctx *ctx, double *G, double *Ginv, int *block_beads);
+/* preconditioned calls, their Krylov iterations, fallbacks, identity blocks */
+int bd_precond_stats(bd_ctx *ctx, long *out4);
+/* M^-1/2 z by plain Lanczos (training targets of the learned preconditioner);
+ * BD_ERR_LANCZOS when the tolerance is missed */
+int bd_lanczos_inv_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
+
+/* ---- learned preconditioner network (no reference counterpart) ----------
+ * Per bead, the BD_MPNN_NEIGHBORS nearest beads within BD_MPNN_CUTOFF
+ * (minimum image) feed a three-layer message-passing network of width
+ * BD_MPNN_WIDTH (BF16 operands, FP32 accumulation on the tensor cores) whose
+ * heads give G_i = a_i (I + sum_j c_ij n_ij n_ij^T), n_ij the unit pair
+ * vectors, a_i > 0, |c_ij| <= 1/(2 BD_MPNN_NEIGHBORS).  Training minimises
+ * (1/N) sum_i |G_i z_i - u_i|^2 over pairs (z, u = M^-1/2 z), whose minimiser
+ * is the diagonal block of M^-1/2.  Parameters are FP32 masters, layout
+ * given by bd_mpnn_param_count (W1, b1, W2, b2, W3, W4, b3, wa, ca, wb, cb). */
+#define BD_MPNN_NEIGHBORS 12
+#define BD_MPNN_WIDTH 64
+#define BD_MPNN_RBF 16
+#define BD_MPNN_CUTOFF 6.0
+size_t bd_mpnn_param_count(void);
+int bd_mpnn_set_params(bd_ctx *ctx, const float *w);
+int bd_mpnn_get_params(bd_ctx *ctx, float *w);
+/* neighbour features of the current configuration (positions and lattice) */
+int bd_mpnn_features(bd_ctx *ctx);
+/* forward pass: the predicted blocks, 9 N row-major */
+int bd_mpnn_predict(bd_ctx *ctx, double *G9);
+/* loss and parameter gradient for one pair (z, u) of the current features;
+ * the gradient stays on the device unless grad is non-null */
+int bd_mpnn_loss_grad(bd_ctx *ctx, const double *z, const double *u, double *loss, float *grad);
+/* one Adam step (Kingma and Ba, 2015) with the last gradient */
+int bd_mpnn_adam(bd_ctx *ctx, float lr, float beta1, float beta2, float eps, int step);
+
 int bd_step_reference(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 
 #ifdef __cplusplus

@@ -24,7 +24,7 @@ ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
-           "bd_noalloc.cu", "bd_pme.cu"]
+           "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -135,6 +135,21 @@ def _lib() -> C.CDLL:
         L.bd_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
         L.bd_launch_count.argtypes = [vp]
         L.bd_launch_count.restype = C.c_longlong
+        _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+        _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+        L.bd_set_preconditioner.argtypes = [vp, C.c_int, C.c_int]
+        L.bd_set_precond_blocks.argtypes = [vp, _dp]
+        L.bd_download_precond_blocks.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
+        L.bd_precond_stats.argtypes = [vp, _lp]
+        L.bd_lanczos_inv_sqrt.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
+        L.bd_mpnn_param_count.restype = C.c_size_t
+        L.bd_mpnn_param_count.argtypes = []
+        L.bd_mpnn_set_params.argtypes = [vp, _fp]
+        L.bd_mpnn_get_params.argtypes = [vp, _fp]
+        L.bd_mpnn_features.argtypes = [vp]
+        L.bd_mpnn_predict.argtypes = [vp, _dp]
+        L.bd_mpnn_loss_grad.argtypes = [vp, _dp, _dp, C.POINTER(C.c_double), C.c_void_p]
+        L.bd_mpnn_adam.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
         _LIB = L
     return _LIB
 
@@ -149,6 +164,72 @@ def exported_symbols() -> list[str]:
 def _chk(status: int, where: str) -> None:
     if status != 0:
         raise BDError(status, where)
+
+
+def mpnn_param_count() -> int:
+    return int(_lib().bd_mpnn_param_count())
+
+
+# parameter layout of the learned preconditioner network (FP32):
+# (name, shape) in storage order
+MPNN_LAYOUT = [("W1", (64, 16)), ("b1", (64,)), ("W2", (64, 64)), ("b2", (64,)),
+               ("W34", (64, 128)), ("b3", (64,)), ("wa", (64,)), ("ca", (1,)),
+               ("wb", (64,)), ("cb", (1,))]
+
+
+def mpnn_unpack(w):
+    out, o = {}, 0
+    for name, shp in MPNN_LAYOUT:
+        n = int(np.prod(shp))
+        out[name] = np.asarray(w[o:o + n]).reshape(shp)
+        o += n
+    return out
+
+
+def mpnn_pack(d):
+    return np.concatenate([np.asarray(d[name], np.float32).reshape(-1) for name, _ in MPNN_LAYOUT])
+
+
+def mpnn_init(seed=0):
+    """Seeded initial parameters: fan-in scaled Gaussian weights, zero heads
+    (the initial blocks are the identity)."""
+    r = np.random.default_rng(seed)
+    d = {}
+    for name, shp in MPNN_LAYOUT:
+        if name.startswith("W"):
+            d[name] = r.normal(0, 1 / np.sqrt(shp[1]), shp)
+        else:
+            d[name] = np.zeros(shp)
+    return mpnn_pack(d)
+
+
+def train_preconditioner(ctx, configs, steps_per_config=20, lr=3e-3, seed=0, step0=0):
+    """Train the learned preconditioner network of ctx on the GPU.
+
+    configs: iterable of (x, y, z, t) with positions in the frame bd_calc_hi
+    reads them (PBC applied) at lattice step t.  For each configuration the
+    mobility and the neighbour features are built; each training step draws
+    z ~ N(0, I), forms the target M^-1/2 z by plain Lanczos and takes one Adam
+    step on (1/N) sum_i |G_i z_i - (M^-1/2 z)_i|^2 (forward, backward and
+    update are the library's own kernels).  ctx must have its network
+    parameters set (bd_mpnn_set_params) and no preconditioner active.
+    Returns the per-step losses."""
+    r = np.random.default_rng(seed)
+    losses, step = [], step0
+    for (x, y, z, t) in configs:
+        ctx.set_positions(x, y, z)
+        ctx.set_time(t, t)
+        ctx.update_lattice(t)
+        ctx.build_neighbors()
+        ctx.calc_hi()
+        ctx.mpnn_features()
+        for _ in range(steps_per_config):
+            zz = r.normal(size=3 * ctx.N)
+            tgt, _ = ctx.lanczos_inv_sqrt(zz)
+            losses.append(ctx.mpnn_loss_grad(zz, tgt))
+            step += 1
+            ctx.mpnn_adam(lr, step)
+    return losses
 
 
 def pme_default_grid(L):
@@ -356,6 +437,62 @@ class Context:
         self._call("bd_sync")
 
     PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP = 0, 1, 2, 3, 4
+
+    # Lanczos preconditioner
+    PRECOND = {"none": 0, "segment": 1, "learned": 2, "blocks": 3}
+
+    def set_preconditioner(self, kind, segment=0):
+        self._call("bd_set_preconditioner", self.PRECOND[kind], int(segment))
+
+    def set_precond_blocks(self, G9):
+        self._call("bd_set_precond_blocks", np.ascontiguousarray(G9, np.float64).reshape(-1))
+
+    def precond_blocks(self, S):
+        n = (self.N // S) * 9 * S * S
+        G, Gi, s = np.zeros(n), np.zeros(n), C.c_int()
+        self._call("bd_download_precond_blocks", G, Gi, C.byref(s))
+        assert s.value == S
+        return G.reshape(self.N // S, 3 * S, 3 * S), Gi.reshape(self.N // S, 3 * S, 3 * S)
+
+    def precond_stats(self):
+        o = np.zeros(4, np.int64)
+        self._call("bd_precond_stats", o)
+        return dict(calls=int(o[0]), iterations=int(o[1]), fallbacks=int(o[2]),
+                    identity_blocks=int(o[3]))
+
+    def lanczos_inv_sqrt(self, z):
+        out = np.zeros(3 * self.N)
+        it = C.c_int()
+        self._call("bd_lanczos_inv_sqrt", np.ascontiguousarray(z, np.float64), out, C.byref(it))
+        return out, it.value
+
+    # learned preconditioner network
+    def mpnn_set_params(self, w):
+        self._call("bd_mpnn_set_params", np.ascontiguousarray(w, np.float32))
+
+    def mpnn_params(self):
+        w = np.zeros(mpnn_param_count(), np.float32)
+        self._call("bd_mpnn_get_params", w)
+        return w
+
+    def mpnn_features(self):
+        self._call("bd_mpnn_features")
+
+    def mpnn_predict(self):
+        G = np.zeros(9 * self.N)
+        self._call("bd_mpnn_predict", G)
+        return G.reshape(self.N, 3, 3)
+
+    def mpnn_loss_grad(self, z, t, want_grad=False):
+        loss = C.c_double()
+        g = np.zeros(mpnn_param_count(), np.float32) if want_grad else None
+        self._call("bd_mpnn_loss_grad", np.ascontiguousarray(z, np.float64),
+                   np.ascontiguousarray(t, np.float64), C.byref(loss),
+                   g.ctypes.data_as(C.c_void_p) if want_grad else None)
+        return (loss.value, g) if want_grad else loss.value
+
+    def mpnn_adam(self, lr, step, beta1=0.9, beta2=0.999, eps=1e-8):
+        self._call("bd_mpnn_adam", float(lr), float(beta1), float(beta2), float(eps), int(step))
 
     def profile(self, on=True):
         self._call("bd_profile_enable", int(bool(on)))

@@ -708,6 +708,10 @@ int bd_destroy(bd_ctx* c) {
   for (void* q : ptrs)
     if (q) cudaFree(q);
   pme_free(c);
+  precond_free(c);
+  mpnn_free(c);
+  if (c->Lt1) cudaFree(c->Lt1);
+  if (c->Lt2) cudaFree(c->Lt2);
   prof_clear(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -20,6 +20,8 @@
 
 // Largest Krylov dimension of the Lanczos square root.
 constexpr int kMaxKrylov = 400;
+// Largest block of the segment preconditioner, in beads.
+constexpr int kMaxSegment = BD_PRECOND_MAX_SEGMENT;
 
 struct bd_ctx {
   bd_params p;
@@ -89,8 +91,22 @@ struct bd_ctx {
   double *Lc;     // Ritz combination coefficients, lmax+1
   double *MF;     // M F, 3 x NTp
   double *Yz;     // sqrt(M) z, 3 x NTp
+  double *Lt1, *Lt2;  // work vectors of the preconditioned products, 3 x NTp
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
-  int lan_last;
+  int lan_last, pre_last;
+
+  // block preconditioner of the Lanczos solve
+  int pre_kind;       // bd_precond_kind
+  int pre_S;          // beads per block
+  bool pre_ready;
+  double *pre_G, *pre_Gi;  // per block 3S x 3S row-major G and G^-1
+  int *pre_bad;       // blocks replaced by the identity
+  size_t pre_cap;
+  long long pre_calls, pre_iters, pre_fallbacks;
+
+  // learned preconditioner network (bd_mpnn.cu)
+  void *mpnn;
+  bool mpnn_ready;
 
   // smooth-PME mobility (BD_MOB_PME)
   int pmeK, pme_p;
@@ -154,6 +170,13 @@ int charge_hop(bd_ctx* c);
 int pme_prepare(bd_ctx* c, const Lat& l);
 int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride);
 void pme_free(bd_ctx* c);
+
+// block preconditioner
+int precond_build(bd_ctx* c, const Lat& l);
+int precond_apply(bd_ctx* c, int which, const double* x, double* y);
+void precond_free(bd_ctx* c);
+int mpnn_blocks(bd_ctx* c, const Lat& l, double* G9);
+void mpnn_free(bd_ctx* c);
 
 // Krylov square root
 int alloc_lanczos(bd_ctx* c);

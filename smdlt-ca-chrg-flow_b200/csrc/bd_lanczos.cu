@@ -310,22 +310,25 @@ static void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e,
   }
 }
 
-// c = T^(1/2) e_1 for T = tridiag(beta, alpha, beta) of size m; negative
-// Ritz values are clamped to zero and counted.
+// c = T^q e_1 for T = tridiag(beta, alpha, beta) of size m, q = +1/2 or
+// -1/2; non-positive Ritz values are clamped (to zero for q > 0, to 1e-12 of
+// the largest for q < 0) and counted.
 static int sqrt_e1(const std::vector<double>& alpha, const std::vector<double>& beta, int m,
-                   std::vector<double>& c) {
+                   std::vector<double>& c, double q = 0.5) {
   std::vector<double> d(alpha.begin(), alpha.begin() + m), e(beta.begin(), beta.begin() + (m - 1));
   std::vector<double> Z;
   tridiag_eig(m, d, e, Z);
   int neg = 0;
+  double lmax = 0;
+  for (int k = 0; k < m; k++) lmax = std::max(lmax, d[k]);
   c.assign(m, 0.0);
   for (int k = 0; k < m; k++) {
     double lam = d[k];
-    if (lam < 0) {
+    if (lam <= 0) {
       neg++;
-      lam = 0;
+      lam = q > 0 ? 0.0 : 1e-12 * lmax;
     }
-    double w = sqrt(lam) * Z[(size_t)0 * m + k];
+    double w = (q > 0 ? sqrt(lam) : 1.0 / sqrt(lam)) * Z[(size_t)0 * m + k];
     for (int i = 0; i < m; i++) c[i] += Z[(size_t)i * m + k] * w;
   }
   return neg;
@@ -346,17 +349,27 @@ int alloc_lanczos(bd_ctx* c) {
   CU(cudaMalloc(&c->Lc, 8 * (size_t)(c->lmax + 1)));
   CU(cudaMalloc(&c->MF, 8 * n));
   CU(cudaMalloc(&c->Yz, 8 * n));
-  c->bytes += 8 * n * (c->lmax + 4) + 8 * (size_t)(c->lmax + 1) * (3 * kDotBlocks + 2) +
+  CU(cudaMalloc(&c->Lt1, 8 * n));
+  CU(cudaMalloc(&c->Lt2, 8 * n));
+  // the padding entries (beads N..NTp-1) of the work vectors stay zero: the
+  // orthogonalisation runs over all 3 NTp entries and the particle-mesh
+  // product and the preconditioner write only the N beads
+  for (double* q : {c->Lw, c->MF, c->Yz, c->Lt1, c->Lt2})
+    CU(cudaMemsetAsync(q, 0, 8 * n, c->stream));
+  c->bytes += 8 * n * (c->lmax + 6) + 8 * (size_t)(c->lmax + 1) * (3 * kDotBlocks + 2) +
               8 * (size_t)(c->lmax + 16);
   return BD_OK;
 }
 
-// sqrt(M) z for the bead-interleaved z on the device (c->R): result in c->Yz.
-// With with_force the first product also forms M F into c->MF.
-int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
+// Lanczos for f(A) z, f(x) = x^q (q = +-1/2), z bead-interleaved on the
+// device; A = M, or A = G M G^T with the block preconditioner G when pre.
+// The result |z| V_m f(T_m) e_1 goes to out (Lanczos layout).  With
+// with_force the first product also forms M F into c->MF.  *conv reports
+// whether the tolerance was met within the Krylov cap.
+static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, double q,
+                       double* out, int* iters, bool* conv_out) {
   int s;
-  if (!c->hi_built) return BD_ERR_STATE;
-  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  if (!out || !c->LV) return BD_ERR_STATE;
   int N = c->N, NTp = c->NT * 32, n = 3 * NTp, blk = kDotBlocks;
   size_t vs = (size_t)n;
   cudaStream_t st = c->stream;
@@ -375,15 +388,28 @@ int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
   // Krylov dimension on, every second iteration
   double* d_alpha = c->Lh;
   double* d_beta = c->Lsc + 8;
-  int next_check = std::max(4, c->lan_last - 2);
+  int& last = pre ? c->pre_last : c->lan_last;
+  int next_check = std::max(4, last - 2);
   for (int j = 0; j < c->lmax; j++) {
     double* vj = c->LV + (size_t)j * vs;
     VecIn vin_j = {{vj, vj + NTp, vj + 2 * NTp}, 1};
-    if (j == 0 && with_force) {
-      VecIn vf = {{c->fx, c->fy, c->fz}, 1};
-      if ((s = sym_matvec(c, 2, vf, vin_j, c->MF, c->Lw, true)) != BD_OK) return s;
+    VecIn vf = {{c->fx, c->fy, c->fz}, 1};
+    if (!pre) {
+      if (j == 0 && with_force) {
+        if ((s = sym_matvec(c, 2, vf, vin_j, c->MF, c->Lw, true)) != BD_OK) return s;
+      } else {
+        if ((s = sym_matvec(c, 1, vin_j, vin_j, c->Lw, c->Lw, true)) != BD_OK) return s;
+      }
     } else {
-      if ((s = sym_matvec(c, 1, vin_j, vin_j, c->Lw, c->Lw, true)) != BD_OK) return s;
+      // w = G M G^T v_j
+      precond_apply(c, 1, vj, c->Lt1);
+      VecIn vt = {{c->Lt1, c->Lt1 + NTp, c->Lt1 + 2 * NTp}, 1};
+      if (j == 0 && with_force) {
+        if ((s = sym_matvec(c, 2, vf, vt, c->MF, c->Lt2, true)) != BD_OK) return s;
+      } else {
+        if ((s = sym_matvec(c, 1, vt, vt, c->Lt2, c->Lt2, true)) != BD_OK) return s;
+      }
+      precond_apply(c, 0, c->Lt2, c->Lw);
     }
     int nv = j + 1;
     double* part1 = c->Lpart;
@@ -403,8 +429,8 @@ int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
     CU(cudaMemcpyAsync(alpha.data(), d_alpha, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
     CU(cudaMemcpyAsync(beta.data(), d_beta, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    neg = sqrt_e1(alpha, beta, m, cc);
-    sqrt_e1(alpha, beta, m - 1, cprev);
+    neg = sqrt_e1(alpha, beta, m, cc, q);
+    sqrt_e1(alpha, beta, m - 1, cprev, q);
     double dn = 0, cn = 0;
     for (int i = 0; i < m; i++) {
       double prev = i < m - 1 ? cprev[i] : 0.0;
@@ -419,15 +445,57 @@ int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
   }
   CU(cudaMemcpyAsync(c->Lc, cc.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, st));
   c->launches++;
-  k_combo<<<blk * 2, 256, 0, st>>>(c->LV, vs, c->Lc, m, zn, c->Yz, n);
-  c->lan_calls++;
-  c->lan_iters += m;
-  c->lan_last = m;
-  if (!conv) c->lan_maxed++;
+  k_combo<<<blk * 2, 256, 0, st>>>(c->LV, vs, c->Lc, m, zn, out, n);
+  last = m;
   c->lan_negative += neg;
   if (iters) *iters = m;
+  *conv_out = conv;
   CU(cudaStreamSynchronize(st));  // cc is a host vector read by the copy above
   return launch_ok(c);
+}
+
+// sqrt(M) z for the bead-interleaved z on the device (c->R): result in c->Yz.
+// With with_force the first product also forms M F into c->MF.  With a block
+// preconditioner G the result is G^(-1) sqrt(G M G^T) z; when that solve
+// misses the tolerance within the Krylov cap the plain method recomputes the
+// step (a fallback, counted).
+int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
+  int s;
+  if (!c->hi_built) return BD_ERR_STATE;
+  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  bool conv = false;
+  int m = 0;
+  if (c->pre_kind != BD_PRECOND_NONE && c->pre_ready) {
+    if ((s = lanczos_run(c, z, with_force, true, 0.5, c->Lt1, &m, &conv)) != BD_OK) return s;
+    c->pre_calls++;
+    c->pre_iters += m;
+    if (conv) {
+      precond_apply(c, 2, c->Lt1, c->Yz);
+      c->lan_calls++;
+      c->lan_iters += m;
+      if (iters) *iters = m;
+      return launch_ok(c);
+    }
+    c->pre_fallbacks++;
+  }
+  if ((s = lanczos_run(c, z, with_force, false, 0.5, c->Yz, &m, &conv)) != BD_OK) return s;
+  c->lan_calls++;
+  c->lan_iters += m;
+  if (!conv) c->lan_maxed++;
+  if (iters) *iters = m;
+  return BD_OK;
+}
+
+// M^(-1/2) z (plain Lanczos, no preconditioner) into out (Lanczos layout).
+int lanczos_inv_sqrt(bd_ctx* c, const double* z, double* out, int* iters, bool* conv) {
+  int s;
+  if (!c->hi_built) return BD_ERR_STATE;
+  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  if (!out) return BD_ERR_ARG;
+  int keep = c->lan_last;
+  s = lanczos_run(c, z, false, false, -0.5, out, iters, conv);
+  c->lan_last = keep;
+  return s;
 }
 
 }  // namespace bd
@@ -465,6 +533,24 @@ int bd_lanczos_sqrt(bd_ctx* c, const double* z, double* out, int* iters) {
   for (int i = 0; i < N; i++)
     for (int a = 0; a < 3; a++) out[3 * i + a] = res[(size_t)a * NTp + i];
   return BD_OK;
+}
+
+int bd_lanczos_inv_sqrt(bd_ctx* c, const double* z, double* out, int* iters) {
+  if (!c || !z || !out) return BD_ERR_ARG;
+  int s;
+  bool conv = false;
+  if (!c->hi_built) return BD_ERR_STATE;
+  // the work vectors exist only after the first allocation; Lt2 is read below
+  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  CU(cudaMemcpyAsync(c->R, z, 24 * (size_t)c->N, cudaMemcpyHostToDevice, c->stream));
+  if ((s = lanczos_inv_sqrt(c, c->R, c->Lt2, iters, &conv)) != BD_OK) return s;
+  int N = c->N, NTp = c->NT * 32;
+  std::vector<double> res(3 * (size_t)NTp);
+  CU(cudaMemcpyAsync(res.data(), c->Lt2, 8 * res.size(), cudaMemcpyDeviceToHost, c->stream));
+  if ((s = check(c)) != BD_OK) return s;
+  for (int i = 0; i < N; i++)
+    for (int a = 0; a < 3; a++) out[3 * i + a] = res[(size_t)a * NTp + i];
+  return conv ? BD_OK : BD_ERR_LANCZOS;
 }
 
 int bd_lanczos_stats(bd_ctx* c, long* o) {

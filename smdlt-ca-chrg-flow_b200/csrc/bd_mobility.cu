@@ -748,6 +748,7 @@ int calc_hi(bd_ctx* c) {
   if (c->p.mobility == BD_MOB_PME) {
     prof_begin(c, BD_PROF_HI_BUILD);
     s = pme_prepare(c, step_lat(c));
+    if (s == BD_OK) s = precond_build(c, step_lat(c));
     prof_end(c, BD_PROF_HI_BUILD);
     return s;
   }
@@ -800,6 +801,7 @@ int calc_hi(bd_ctx* c) {
     c->launches++;
     k_to_fp32<<<148 * 16, 256, 0, c->stream>>>(c->Mt, c->Mt32, c->ntiles * 6144);
   }
+  if ((s = precond_build(c, l)) != BD_OK) return s;
   prof_end(c, BD_PROF_HI_BUILD);
   c->hi_built = true;
   return launch_ok(c);

@@ -1,0 +1,200 @@
+"""Preconditioned Lanczos and the learned preconditioner on the GPU.
+
+No reference counterpart.  Checked against numpy:
+
+* segment blocks: G_b = L_b^-1 for the Cholesky factor of the free-space RPY
+  mobility of 10 consecutive beads (minimum-image pair vectors from the
+  oracle's getNID), 1e-10 relative;
+* the displacement G^-1 sqrt(G M G^T) z against numpy.linalg.eigh of the
+  dense Ewald matrix (oracle/bd_oracle.c's bdo_calc_hi_ewald), 1e-5 relative
+  (the Lanczos tolerance is 1e-6 on successive iterates), for segment blocks,
+  caller-supplied bead blocks and the network's blocks; the segment blocks
+  take fewer Krylov iterations than the plain method;
+* a preconditioned solve that misses the Krylov cap falls back to the plain
+  method and is counted;
+* the network: features, blocks, loss and parameter gradient against
+  oracle/mpnn_oracle.py with the same BF16 operand rounding (blocks and loss
+  1e-4, gradient 2e-3 relative per parameter group);
+* training on the GPU lowers the loss, and the trained network's effect on the
+  Krylov iteration count against the plain method is measured and bounded.
+"""
+import numpy as np
+import pytest
+
+import bd_b200 as B
+import mpnn_oracle as Q
+import oracle as O
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(flow, t, Nb=25, Nc=20, L=30.0, seed=31, mobility="ewald", **kw):
+    x, y, z = B.random_chains(Nb, Nc, L, seed, bond=2.0, min_sep=2.0)
+    x, y = B.lab_frame(flow, x, y)
+    o = O.Oracle(flow, Nb, Nc, L, 0.2, 5e-4)
+    c = B.Context(B.make_params(flow, Nb, Nc, L, 0.2, 5e-4, mobility=mobility, noise="philox",
+                                **kw))
+    o.lattice(t)
+    if flow == 1:
+        o.rotate(x, y, 0)
+    o.apply_pbc(x, y, z)
+    c.set_positions(x, y, z)
+    c.set_time(t, t)
+    c.update_lattice(t)
+    c.build_neighbors()
+    c.calc_hi()
+    return c, o, (x, y, z)
+
+
+def _rpy_free(d):
+    r = np.linalg.norm(d)
+    rr = np.outer(d, d) / r ** 2
+    if r >= 2:
+        return (0.75 / r + 0.5 / r ** 3) * np.eye(3) + (0.75 / r - 1.5 / r ** 3) * rr
+    return (1 - 9 * r / 32) * np.eye(3) + (3 * r / 32) * rr
+
+
+def _reference_displacement(M, Gfull, Gi_full, z):
+    A = Gfull @ M @ Gfull.T
+    w, V = np.linalg.eigh(A)
+    assert w.min() > 0
+    return Gi_full @ (V @ (np.sqrt(w) * (V.T @ z)))
+
+
+def _block_diag(blocks):
+    nb, n, _ = blocks.shape
+    F = np.zeros((nb * n, nb * n))
+    for b in range(nb):
+        F[b * n:(b + 1) * n, b * n:(b + 1) * n] = blocks[b]
+    return F
+
+
+@pytest.mark.parametrize("flow", [0, 1])
+def test_segment_preconditioner(flow):
+    c, o, (x, y, z) = _system(flow, 0)
+    N, S = o.N, 5
+    zz = np.random.default_rng(2).normal(size=3 * N)
+    _, it_plain = c.lanczos_sqrt(zz)
+    c.set_preconditioner("segment", S)
+    G, Gi = c.precond_blocks(S)
+    for b in range(N // S):
+        A = np.zeros((3 * S, 3 * S))
+        for a in range(S):
+            for q in range(S):
+                A[3 * a:3 * a + 3, 3 * q:3 * q + 3] = (
+                    np.eye(3) if a == q else _rpy_free(o.nid(x, y, z, b * S + a, b * S + q)))
+        Lc = np.linalg.cholesky(A)
+        assert rel_err(G[b], np.linalg.inv(Lc)) < 1e-10
+        assert rel_err(Gi[b], Lc) < 1e-10
+    M = O.full_mobility(o.calc_hi_ewald(x, y, z), N)
+    ref = _reference_displacement(M, _block_diag(G), _block_diag(Gi), zz)
+    got, it_pre = c.lanczos_sqrt(zz)
+    assert rel_err(got, ref) < 1e-5
+    assert it_pre < it_plain, (it_pre, it_plain)
+    st = c.precond_stats()
+    assert st["calls"] == 1 and st["fallbacks"] == 0 and st["identity_blocks"] == 0
+
+
+def test_bead_blocks_preconditioner():
+    c, o, (x, y, z) = _system(1, 0)
+    N = o.N
+    r = np.random.default_rng(4)
+    Bk = r.normal(size=(N, 3, 3)) * 0.2
+    G = np.eye(3)[None] * 1.3 + 0.5 * (Bk + Bk.transpose(0, 2, 1))
+    c.set_precond_blocks(G.reshape(-1))
+    Gd, Gi = c.precond_blocks(1)
+    assert rel_err(Gd, G) == 0.0
+    assert rel_err(np.einsum("ipq,iqr->ipr", Gd, Gi), np.broadcast_to(np.eye(3), G.shape)) < 1e-12
+    M = O.full_mobility(o.calc_hi_ewald(x, y, z), N)
+    zz = r.normal(size=3 * N)
+    ref = _reference_displacement(M, _block_diag(Gd), _block_diag(Gi), zz)
+    got, _ = c.lanczos_sqrt(zz)
+    assert rel_err(got, ref) < 1e-5
+
+
+def test_preconditioned_fallback_counted():
+    c, o, _ = _system(0, 0, lanczos_max=6)
+    c.set_preconditioner("segment", 5)
+    zz = np.random.default_rng(5).normal(size=3 * o.N)
+    c.lanczos_sqrt(zz)
+    st = c.precond_stats()
+    assert st["calls"] == 1 and st["fallbacks"] == 1
+    assert c.lanczos_stats()["maxed"] == 1
+
+
+def _oracle_features(o, x, y, z):
+    # every other bead is a candidate: the Verlet rows the kernel reads were
+    # built at the same positions with the same cutoff (6)
+    cand = [[j for j in range(o.N) if j != i] for i in range(o.N)]
+    return Q.features(lambda i, j: o.nid(x, y, z, i, j), cand, o.N)
+
+
+@pytest.mark.parametrize("flow", [0, 1])
+def test_network_forward_and_gradient_vs_model(flow):
+    c, o, (x, y, z) = _system(flow, 0, Nb=25, Nc=8)
+    N = o.N
+    r = np.random.default_rng(6)
+    w = B.mpnn_init(7).astype(np.float64)
+    w += r.normal(0, 0.05, w.size)  # non-trivial heads
+    w = w.astype(np.float32)
+    c.mpnn_set_params(w)
+    c.mpnn_features()
+    nbr, nvec, rbf = _oracle_features(o, x, y, z)
+    Gg = c.mpnn_predict()
+    cm = Q.forward(w.astype(np.float64), nbr, nvec, rbf)
+    assert rel_err(Gg, cm["G"]) < 1e-4
+    zz = r.normal(size=(N, 3))
+    tt = r.normal(size=(N, 3)) * 0.5
+    loss, g = c.mpnn_loss_grad(zz.reshape(-1), tt.reshape(-1), want_grad=True)
+    lm, gm, _ = Q.loss_grad(w.astype(np.float64), nbr, nvec, rbf, zz, tt)
+    assert abs(loss - lm) < 1e-4 * abs(lm)
+    o_ = 0
+    for name, shp in Q.LAYOUT:
+        n = int(np.prod(shp))
+        assert rel_err(g[o_:o_ + n], gm[o_:o_ + n]) < 2e-3, name
+        o_ += n
+
+
+def test_training_and_iteration_gain():
+    """Trains on four 500-bead configurations (shear and extension), then
+    compares Krylov iterations with and without the network on held-out
+    configurations; the gain of per-bead blocks is small (the diagonal
+    blocks of M^-1/2 vary little between beads), so the bound is that the
+    learned blocks never cost more than one extra iteration, with no
+    fallback, and that the loss falls."""
+    Nb, Nc, L = 25, 20, 30.0
+    c, o, _ = _system(1, 0, Nb=Nb, Nc=Nc, L=L)
+    c.mpnn_set_params(B.mpnn_init(11))
+    configs = []
+    for s in range(4):
+        x, y, z = B.random_chains(Nb, Nc, L, 100 + s, bond=2.0, min_sep=2.0)
+        x, y = B.lab_frame(1, x, y)
+        o.lattice(0)
+        o.rotate(x, y, 0)
+        o.apply_pbc(x, y, z)
+        configs.append((x, y, z, 0))
+    losses = B.train_preconditioner(c, configs, steps_per_config=40, lr=3e-3, seed=1)
+    assert np.mean(losses[-20:]) < 0.8 * np.mean(losses[:5])
+    gains = []
+    for s in range(2):
+        x, y, z = B.random_chains(Nb, Nc, L, 200 + s, bond=2.0, min_sep=2.0)
+        x, y = B.lab_frame(1, x, y)
+        o.rotate(x, y, 0)
+        o.apply_pbc(x, y, z)
+        c.set_positions(x, y, z)
+        c.build_neighbors()
+        c.set_preconditioner("none")
+        c.calc_hi()
+        zz = np.random.default_rng(300 + s).normal(size=3 * o.N)
+        _, it_plain = c.lanczos_sqrt(zz)
+        c.set_preconditioner("learned")
+        got, it_learned = c.lanczos_sqrt(zz)
+        gains.append((it_plain, it_learned))
+        Gd, Gi = c.precond_blocks(1)
+        M = O.full_mobility(o.calc_hi_ewald(x, y, z), o.N)
+        ref = _reference_displacement(M, _block_diag(Gd), _block_diag(Gi), zz)
+        assert rel_err(got, ref) < 1e-5
+    print("plain vs learned Krylov iterations:", gains)
+    assert all(l <= p + 1 for p, l in gains)
+    assert c.precond_stats()["fallbacks"] == 0
