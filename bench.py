@@ -112,7 +112,28 @@ def host_threads():
         return os.cpu_count() or 1
 
 
+class _StdoutToStderr:
+    """Sends what C code writes to file descriptor 1 (the reference routines
+    print status lines) to stderr, so stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def time_reference(w, steps, warmup, threads):
+    with _StdoutToStderr():
+        return _time_reference(w, steps, warmup, threads)
+
+
+def _time_reference(w, steps, warmup, threads):
     """Per-step wall time of the reference's own routines (oracle/_ref) on the
     workload: plain steps at full size, plus the amortised mobility rebuild
     (timed once at full size) and charge-hop sweep.  The reference's sweep is
@@ -248,6 +269,15 @@ PATHS = {
     # the same in FP32 storage (grids, FFTs, influence, pair tensors) with FP64
     # accumulation of the interpolation and pair sums
     "pme32": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None),
+    # FP32 particle-mesh products with a preconditioned Krylov solve: segment
+    # blocks (Cholesky of the free-space RPY mobility of 10 consecutive
+    # beads), or those with the learned per-bead blocks on top (parameters
+    # from smdlt-ca-chrg-flow_b200/mpnn_params.npy, made by
+    # train_preconditioner.py)
+    "pme32-seg": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None,
+                      precond="segment"),
+    "pme32-learned": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None,
+                          precond="learned"),
     # the reference's own algorithm: hybrid mobility + CA-TEA displacement
     "tea": dict(mobility="hybrid", precision="fp64", step="reference", bytes_per_block=48),
 }
@@ -274,6 +304,11 @@ def build_context(w, seed, path="lanczos32", device_noise="philox"):
     c.apply_pbc()
     c.build_neighbors()
     c.inverse_coords()
+    if pp.get("precond") == "segment":
+        c.set_preconditioner("segment", 10)
+    elif pp.get("precond") == "learned":
+        c.mpnn_set_params(np.load(os.path.join(PKG, "mpnn_params.npy")))
+        c.set_preconditioner("learned", 10)
     return c
 
 
@@ -298,6 +333,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
         dist.barrier()
     torch.cuda.synchronize()
     lan0 = c.lanczos_stats()
+    pre0 = c.precond_stats()
     c.profile(True)
     n0 = c.launches()
     dev = int(os.environ.get("LOCAL_RANK", 0))
@@ -309,6 +345,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
             ("STEP", "MATVEC", "HI_BUILD", "HOP", "FORCES")}
     c.profile(False)
     lan1 = c.lanczos_stats()
+    pre1 = c.precond_stats()
     step_ms = prof["STEP"][0]
     t_max = step_ms
     if dist:
@@ -353,6 +390,8 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
                achieved_gbs=alg_bytes / (avg_ms / 1e3) / 1e9 if mv_n else None,
                lanczos_iters_per_step=(iters / calls) if calls else None,
                lanczos_maxed=lan1["maxed"] - lan0["maxed"],
+               precond_fallbacks=pre1["fallbacks"] - pre0["fallbacks"],
+               precond_calls=pre1["calls"] - pre0["calls"],
                breakdown={"mobility_build_ms": prof["HI_BUILD"][0], "mobility_builds": prof["HI_BUILD"][1],
                           "hop_sweep_ms": prof["HOP"][0], "hop_sweeps": prof["HOP"][1],
                           "forces_ms": prof["FORCES"][0], "matvec_ms": mv_ms,
@@ -391,7 +430,11 @@ def run_ours(args, rank, world, dist):
                                     % __import__("bd_b200").pme_default_grid(w["L"]) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
                        "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation",
-                       "preconditioner": "none",
+                       "preconditioner": {None: "none", "segment": "segment blocks of 10 beads",
+                                          "learned": "learned bead blocks on segment blocks "
+                                                     "of 10 beads"}[
+                                              PATHS[args.path].get("precond")],
+                       "precond_fallbacks": main["precond_fallbacks"],
                        "lanczos_iters_per_step": main["lanczos_iters_per_step"],
                        "lanczos_fallbacks": main["lanczos_maxed"],
                        "edot": edot_of(w), "tau_estimate": tau_estimate(w["Nb"]),
@@ -401,9 +444,11 @@ def run_ours(args, rank, world, dist):
                        "parallelism": "replicas only" if world > 1 else "single GPU"},
             "roofline": roof, "e2e": e2e, "clocks": main["clocks"],
             "gpu_launches": main["launches"], "breakdown": main["breakdown"]}
-    if args.compare and args.path != "lanczos64":
-        ref64 = measure(w, "lanczos64", K, W, rank, dist, 1)
-        line["plain_fp64"] = {"value": world * N * K / (ref64["t_max_ms"] / 1e3),
+    plain = "pme64" if pme else "lanczos64"
+    if args.compare and args.path != plain:
+        # the plain method: same mobility in FP64, no preconditioner
+        ref64 = measure(w, plain, K, W, rank, dist, 1)
+        line["plain_fp64"] = {"path": plain, "value": world * N * K / (ref64["t_max_ms"] / 1e3),
                               "ms_per_step": ref64["t_max_ms"] / K,
                               "lanczos_iters_per_step": ref64["lanczos_iters_per_step"],
                               "matvec_gbs": ref64["achieved_gbs"]}
@@ -420,7 +465,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
-    ap.add_argument("--path", choices=sorted(PATHS), default="lanczos32")
+    ap.add_argument("--path", choices=sorted(PATHS), default="pme32-learned")
     ap.add_argument("--compare", type=int, default=1,
                     help="also time the plain FP64 Krylov path (reported as plain_fp64)")
     args = ap.parse_args()

@@ -111,8 +111,8 @@ typedef struct {
   int lanczos_max;           /* Krylov dimension cap, at most 400; 0 -> 200 */
   /* BD_MOB_PME discretisation (no reference counterpart): grid points per
    * reduced lattice direction (0 -> smallest 2^a 3^b 5^c 7^d >= 1.5 L),
-   * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> 10, at
-   * most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
+   * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> the smaller
+   * of 10 and 0.43 L; at most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
    * real-space pairs per bead (0 -> 512). */
   int pme_grid;
   int pme_order;
@@ -262,9 +262,12 @@ int bd_step_lanczos(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 /* ---- Lanczos preconditioner (no reference counterpart) ------------------
  * kind: bd_precond_kind; segment: beads per block for BD_PRECOND_SEGMENT
  * (must divide Nb, at most BD_PRECOND_MAX_SEGMENT; 0 -> 10 or the largest of
- * 5, 4, 2, 1 dividing Nb).  Blocks are rebuilt with every mobility build.  A
- * preconditioned solve that misses lanczos_tol within lanczos_max is redone
- * without the preconditioner (counted as a fallback). */
+ * 5, 4, 2, 1 dividing Nb).  For BD_PRECOND_LEARNED, segment > 1 applies the
+ * learned bead blocks B on top of segment blocks (G = B L^-1, the network
+ * then being trained on targets of the segment-preconditioned operator);
+ * segment <= 1 uses the bead blocks alone.  Blocks are rebuilt with every
+ * mobility build.  A preconditioned solve that misses lanczos_tol within
+ * lanczos_max is redone without the preconditioner (counted as a fallback). */
 int bd_set_preconditioner(bd_ctx *ctx, int kind, int segment);
 /* per-bead blocks G (9 N, row-major 3x3) for BD_PRECOND_BLOCKS */
 int bd_set_precond_blocks(bd_ctx *ctx, const double *G9);
@@ -272,8 +275,9 @@ int bd_set_precond_blocks(bd_ctx *ctx, const double *G9);
 int bd_download_precond_blocks(bd_ctx *ctx, double *G, double *Ginv, int *block_beads);
 /* preconditioned calls, their Krylov iterations, fallbacks, identity blocks */
 int bd_precond_stats(bd_ctx *ctx, long *out4);
-/* M^-1/2 z by plain Lanczos (training targets of the learned preconditioner);
- * BD_ERR_LANCZOS when the tolerance is missed */
+/* A^-1/2 z by Lanczos, A = M, or G M G^T while the segment preconditioner is
+ * active (training targets of the learned preconditioner); BD_ERR_LANCZOS
+ * when the tolerance is missed */
 int bd_lanczos_inv_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
 
 /* ---- learned preconditioner network (no reference counterpart) ----------

@@ -212,7 +212,10 @@ def train_preconditioner(ctx, configs, steps_per_config=20, lr=3e-3, seed=0, ste
     z ~ N(0, I), forms the target M^-1/2 z by plain Lanczos and takes one Adam
     step on (1/N) sum_i |G_i z_i - (M^-1/2 z)_i|^2 (forward, backward and
     update are the library's own kernels).  ctx must have its network
-    parameters set (bd_mpnn_set_params) and no preconditioner active.
+    parameters set (bd_mpnn_set_params) and either no preconditioner active
+    or the segment preconditioner, in which case the targets are
+    (G M G^T)^-1/2 z and the network learns bead blocks to apply on top of
+    the segment blocks (bd_set_preconditioner(LEARNED, segment)).
     Returns the per-step losses."""
     r = np.random.default_rng(seed)
     losses, step = [], step0

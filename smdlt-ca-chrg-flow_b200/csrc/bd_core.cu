@@ -602,10 +602,11 @@ int bd_create(const bd_params* p, bd_ctx** out) {
     }
     c->pmeK = K;
     c->pme_p = p->pme_order > 0 ? p->pme_order : 8;
-    c->pme_rc = p->pme_rc > 0 ? p->pme_rc : 10.0;
+    c->pme_rc = p->pme_rc > 0 ? p->pme_rc : std::min(10.0, 0.43 * p->L);
     c->pme_alpha = p->pme_alpha > 0 ? p->pme_alpha : 4.0 / c->pme_rc;
-    if (K < 8 || K > 1024 || c->pme_p < 4 || c->pme_p > 8 || (c->pme_p & 1) ||
-        c->pme_p > K || c->pme_rc > 0.43 * p->L) {
+    if (p->mobility == BD_MOB_PME &&
+        (K < 8 || K > 1024 || c->pme_p < 4 || c->pme_p > 8 || (c->pme_p & 1) || c->pme_p > K ||
+         c->pme_rc > 0.43 * p->L)) {
       bd_destroy(c);
       return BD_ERR_ARG;
     }

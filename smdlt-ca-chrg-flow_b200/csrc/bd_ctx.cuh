@@ -100,6 +100,7 @@ struct bd_ctx {
   int pre_S;          // beads per block
   bool pre_ready;
   double *pre_G, *pre_Gi;  // per block 3S x 3S row-major G and G^-1
+  double *pre_B, *pre_Bi;  // learned bead blocks on top of segment blocks
   int *pre_bad;       // blocks replaced by the identity
   size_t pre_cap;
   long long pre_calls, pre_iters, pre_fallbacks;

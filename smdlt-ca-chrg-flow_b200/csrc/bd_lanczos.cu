@@ -486,15 +486,19 @@ int lanczos_sqrt(bd_ctx* c, const double* z, bool with_force, int* iters) {
   return BD_OK;
 }
 
-// M^(-1/2) z (plain Lanczos, no preconditioner) into out (Lanczos layout).
+// A^(-1/2) z into out (Lanczos layout), A = M, or A = G M G^T when the
+// segment preconditioner is active (the targets for learned blocks applied
+// on top of it).
 int lanczos_inv_sqrt(bd_ctx* c, const double* z, double* out, int* iters, bool* conv) {
   int s;
   if (!c->hi_built) return BD_ERR_STATE;
   if ((s = alloc_lanczos(c)) != BD_OK) return s;
   if (!out) return BD_ERR_ARG;
-  int keep = c->lan_last;
-  s = lanczos_run(c, z, false, false, -0.5, out, iters, conv);
+  bool pre = c->pre_kind == BD_PRECOND_SEGMENT && c->pre_ready;
+  int keep = c->lan_last, keep_pre = c->pre_last;
+  s = lanczos_run(c, z, false, pre, -0.5, out, iters, conv);
   c->lan_last = keep;
+  c->pre_last = keep_pre;
   return s;
 }
 

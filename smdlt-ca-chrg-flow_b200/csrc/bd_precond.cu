@@ -191,6 +191,35 @@ __global__ void k_bead_invert(double* G, double* Gi, int N, int* bad) {
   O[8] = (a * e - b * d) * id;
 }
 
+// Learned bead blocks on top of segment blocks: G'_b = B_b G_b and
+// G'_b^-1 = G_b^-1 B_b^-1 with B_b the block diagonal of the segment's bead
+// blocks (9 per bead in Bb, inverses in Bi).  One thread per matrix entry.
+__global__ void k_combine_blocks(const double* __restrict__ Bb, const double* __restrict__ Bi,
+                                 int S, int nblk, double* G, double* Gi) {
+  int n = 3 * S;
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)nblk * n) return;
+  // one thread per (block, column): the column of G'_b and the row of G'^-1_b
+  int b = (int)(e / n), j = (int)(e % n);
+  double* Gb = G + (size_t)b * n * n;
+  double* Gib = Gi + (size_t)b * n * n;
+  double col[3 * BD_PRECOND_MAX_SEGMENT], row[3 * BD_PRECOND_MAX_SEGMENT];
+  for (int i = 0; i < n; i++) {
+    col[i] = Gb[(size_t)i * n + j];
+    row[i] = Gib[(size_t)j * n + i];
+  }
+  for (int a = 0; a < S; a++) {
+    const double* B = Bb + 9 * ((size_t)b * S + a);
+    const double* Binv = Bi + 9 * ((size_t)b * S + a);
+    for (int p = 0; p < 3; p++) {
+      Gb[(size_t)(3 * a + p) * n + j] =
+          B[3 * p] * col[3 * a] + B[3 * p + 1] * col[3 * a + 1] + B[3 * p + 2] * col[3 * a + 2];
+      Gib[(size_t)j * n + 3 * a + p] = row[3 * a] * Binv[p] + row[3 * a + 1] * Binv[3 + p] +
+                                      row[3 * a + 2] * Binv[6 + p];
+    }
+  }
+}
+
 namespace bd {
 
 static int pre_alloc(bd_ctx* c, int S) {
@@ -225,12 +254,35 @@ int precond_build(bd_ctx* c, const Lat& l) {
     c->pre_ready = true;
     return launch_ok(c);
   }
-  if (c->pre_kind == BD_PRECOND_LEARNED) {
+  if (c->pre_kind == BD_PRECOND_LEARNED && c->pre_S == 1) {
     if ((s = pre_alloc(c, 1)) != BD_OK) return s;
     if ((s = mpnn_blocks(c, l, c->pre_G)) != BD_OK) return s;
     c->launches++;
     k_bead_invert<<<(c->N + 127) / 128, 128, 0, c->stream>>>(c->pre_G, c->pre_Gi, c->N,
                                                              c->pre_bad);
+    c->pre_ready = true;
+    return launch_ok(c);
+  }
+  if (c->pre_kind == BD_PRECOND_LEARNED) {
+    // segment blocks first, then the learned bead blocks applied on top
+    int S = c->pre_S;
+    if ((s = pre_alloc(c, S)) != BD_OK) return s;
+    if (!c->pre_B) {
+      CU(cudaMalloc(&c->pre_B, 72 * (size_t)c->N));
+      CU(cudaMalloc(&c->pre_Bi, 72 * (size_t)c->N));
+      c->bytes += 144 * (size_t)c->N;
+    }
+    size_t smem = 2 * 8 * (size_t)(3 * S) * (3 * S);
+    cudaFuncSetAttribute(k_seg_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    c->launches += 3;
+    k_seg_blocks<<<c->N / S, 128, smem, c->stream>>>(l, c->rx, c->ry, c->rz, S, c->pre_G,
+                                                     c->pre_Gi, c->pre_bad);
+    if ((s = mpnn_blocks(c, l, c->pre_B)) != BD_OK) return s;
+    k_bead_invert<<<(c->N + 127) / 128, 128, 0, c->stream>>>(c->pre_B, c->pre_Bi, c->N,
+                                                             c->pre_bad);
+    int nb = c->N / S;
+    k_combine_blocks<<<(nb * 3 * S + 127) / 128, 128, 0, c->stream>>>(c->pre_B, c->pre_Bi, S,
+                                                                       nb, c->pre_G, c->pre_Gi);
     c->pre_ready = true;
     return launch_ok(c);
   }
@@ -252,6 +304,8 @@ int precond_apply(bd_ctx* c, int which, const double* x, double* y) {
 }
 
 void precond_free(bd_ctx* c) {
+  if (c->pre_B) cudaFree(c->pre_B);
+  if (c->pre_Bi) cudaFree(c->pre_Bi);
   if (c->pre_G) cudaFree(c->pre_G);
   if (c->pre_Gi) cudaFree(c->pre_Gi);
   if (c->pre_bad) cudaFree(c->pre_bad);
@@ -267,7 +321,7 @@ int bd_set_preconditioner(bd_ctx* c, int kind, int segment) {
   if (!c) return BD_ERR_ARG;
   if (kind < BD_PRECOND_NONE || kind > BD_PRECOND_BLOCKS) return BD_ERR_ARG;
   int S = 1;
-  if (kind == BD_PRECOND_SEGMENT) {
+  if (kind == BD_PRECOND_SEGMENT || (kind == BD_PRECOND_LEARNED && segment > 1)) {
     if (segment <= 0) {
       // 10 beads, or the largest of 5, 4, 2, 1 that divides the chain length
       const int cand[] = {10, 5, 4, 2, 1};

@@ -156,6 +156,29 @@ def test_network_forward_and_gradient_vs_model(flow):
         o_ += n
 
 
+def test_learned_on_segment_blocks():
+    """G' = B L^-1 per segment: the learned bead blocks B applied on top of
+    the segment blocks, and the displacement with it against numpy."""
+    c, o, (x, y, z) = _system(1, 0)
+    N, S = o.N, 5
+    c.mpnn_set_params(B.mpnn_init(3) + np.random.default_rng(1).normal(0, 0.05, B.mpnn_param_count()).astype(np.float32))
+    c.set_preconditioner("segment", S)
+    G0, Gi0 = c.precond_blocks(S)
+    c.mpnn_features()
+    Bb = c.mpnn_predict()
+    c.set_preconditioner("learned", S)
+    G, Gi = c.precond_blocks(S)
+    for b in range(N // S):
+        Bs = _block_diag(Bb[b * S:(b + 1) * S])
+        assert rel_err(G[b], Bs @ G0[b]) < 1e-12
+        assert rel_err(Gi[b], Gi0[b] @ np.linalg.inv(Bs)) < 1e-10
+    M = O.full_mobility(o.calc_hi_ewald(x, y, z), N)
+    zz = np.random.default_rng(8).normal(size=3 * N)
+    ref = _reference_displacement(M, _block_diag(G), _block_diag(Gi), zz)
+    got, _ = c.lanczos_sqrt(zz)
+    assert rel_err(got, ref) < 1e-5
+
+
 def test_training_and_iteration_gain():
     """Trains on four 500-bead configurations (shear and extension), then
     compares Krylov iterations with and without the network on held-out
