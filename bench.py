@@ -264,7 +264,7 @@ PATHS = {
     "lanczos32": dict(mobility="ewald", precision="fp32", step="lanczos", bytes_per_block=24),
     "lanczos64": dict(mobility="ewald", precision="fp64", step="lanczos", bytes_per_block=48),
     # the same Ewald sum applied matrix-free by smooth particle-mesh Ewald
-    # (grid 1.5 L, B-spline order 8, real-space cutoff 10)
+    # (grid 1.45 L, B-spline order 8, real-space cutoff 10)
     "pme64": dict(mobility="pme", precision="fp64", step="lanczos", bytes_per_block=None),
     # the same in FP32 storage (grids, FFTs, influence, pair tensors) with FP64
     # accumulation of the interpolation and pair sums

@@ -592,10 +592,10 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   {
     int K = p->pme_grid;
     if (K <= 0) {
-      K = (int)ceil(1.5 * p->L);
+      K = (int)ceil(1.45 * p->L);
       for (;; K++) {
         int r = K;
-        for (int f : {2, 3, 5, 7})
+        for (int f : {2, 3, 5})
           while (r % f == 0) r /= f;
         if (r == 1) break;
       }

@@ -9,7 +9,7 @@
   longer holds every k inside its cutoff once the cell is strongly skewed:
   there the dense sum is 1e-4 to 2e-3 from the converged one, which the
   model (and the CUDA particle-mesh path) follow instead;
-* its smooth-PME sum at the default discretisation (grid 1.5 L, order 8,
+* its smooth-PME sum at the default discretisation (grid 1.45 L, order 8,
   cutoff 10, split 0.4) against that Ewald sum, 1e-5 relative, in shear and
   in planar extension at several points of the lattice period;
 * the Gauss-reduced cell spans the same lattice.
