@@ -75,6 +75,12 @@ typedef enum {
  * with FP64 accumulation. */
 typedef enum { BD_PREC_FP64 = 0, BD_PREC_FP32 = 1 } bd_precision;
 typedef enum { BD_SPRING_HOOKEAN = 0, BD_SPRING_FENE = 1 } bd_spring;
+/* Electrostatics: the reference's Debye-Hueckel pair force over all charged
+ * pairs (coulombForce, shear/src/main26.c:1891-1925), or the unscreened
+ * Coulomb interaction Ewald-summed over the periodic lattice (no reference
+ * counterpart; real-space pairs within coulomb_rc plus a particle-mesh
+ * reciprocal sum on the pme_grid / pme_order grid). */
+typedef enum { BD_COULOMB_DH = 0, BD_COULOMB_EWALD = 1 } bd_coulomb_kind;
 
 /* System parameters.  The names follow the reference's globals
  * (shear/src/Parameters.h:57-199) and Input.txt keys
@@ -119,6 +125,9 @@ typedef struct {
   double pme_rc;
   double pme_alpha;
   int pme_max_pairs;
+  int coulomb;               /* bd_coulomb_kind */
+  double coulomb_beta;       /* Ewald split; 0 -> 3.5 / coulomb_rc (erfc(3.5) = 7e-7) */
+  double coulomb_rc;         /* real-space cutoff; 0 -> the smaller of 10 and 0.43 L */
 } bd_params;
 
 typedef struct bd_ctx bd_ctx;
@@ -259,6 +268,16 @@ int bd_step_lanczos(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 /* One reference-mode hydrodynamic step (the body of the step loop,
  * shear/src/main26.c:65-151, extensional/src/main14.c:68-171, without file
  * output), repeated nsteps times from step t0. */
+/* ---- signed charges and the Ewald Coulomb energy (no reference counterpart)
+ * bd_set_charges gives every charge the value +1, as the reference's charge
+ * flags do; bd_set_charge_values sets signed values per charge (in the order
+ * of the track passed to bd_set_charges; the values move with the charges
+ * when they hop).  bd_coulomb_energy returns, for the last bd_coulomb_force
+ * with coulomb = BD_COULOMB_EWALD: real-space, reciprocal, self plus
+ * neutralising-background, and total energy (kT). */
+int bd_set_charge_values(bd_ctx *ctx, const double *qk);
+int bd_coulomb_energy(bd_ctx *ctx, double *out4);
+
 /* ---- Lanczos preconditioner (no reference counterpart) ------------------
  * kind: bd_precond_kind; segment: beads per block for BD_PRECOND_SEGMENT
  * (must divide Nb, at most BD_PRECOND_MAX_SEGMENT; 0 -> 10 or the largest of

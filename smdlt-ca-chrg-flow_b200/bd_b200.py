@@ -24,7 +24,7 @@ ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
-           "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu"]
+           "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu", "bd_coulomb.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -69,6 +69,7 @@ class Params(C.Structure):
         ("mobility", C.c_int), ("precision", C.c_int), ("lanczos_tol", C.c_double),
         ("lanczos_max", C.c_int), ("pme_grid", C.c_int), ("pme_order", C.c_int),
         ("pme_rc", C.c_double), ("pme_alpha", C.c_double), ("pme_max_pairs", C.c_int),
+        ("coulomb", C.c_int), ("coulomb_beta", C.c_double), ("coulomb_rc", C.c_double),
     ]
 
 
@@ -138,6 +139,8 @@ def _lib() -> C.CDLL:
         _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
         _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
         L.bd_set_preconditioner.argtypes = [vp, C.c_int, C.c_int]
+        L.bd_set_charge_values.argtypes = [vp, _dp]
+        L.bd_coulomb_energy.argtypes = [vp, _dp]
         L.bd_set_precond_blocks.argtypes = [vp, _dp]
         L.bd_download_precond_blocks.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
         L.bd_precond_stats.argtypes = [vp, _lp]
@@ -255,7 +258,8 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
                 max_neighbors=256, seed=None, shear_kappas_override=0, box_volume=0.0,
                 noise="ran1", philox_seed=20261203, mobility="hybrid", precision="fp64",
                 lanczos_tol=1e-6, lanczos_max=0, pme_grid=0, pme_order=0, pme_rc=0.0,
-                pme_alpha=0.0, pme_max_pairs=0) -> Params:
+                pme_alpha=0.0, pme_max_pairs=0, coulomb="dh", coulomb_beta=0.0,
+                coulomb_rc=0.0) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
     p.box_volume = box_volume
@@ -274,6 +278,8 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
     p.lanczos_tol, p.lanczos_max = lanczos_tol, lanczos_max
     p.pme_grid, p.pme_order, p.pme_rc = pme_grid, pme_order, pme_rc
     p.pme_alpha, p.pme_max_pairs = pme_alpha, pme_max_pairs
+    p.coulomb = {"dh": 0, "ewald": 1}[coulomb]
+    p.coulomb_beta, p.coulomb_rc = coulomb_beta, coulomb_rc
     return p
 
 
@@ -440,6 +446,14 @@ class Context:
         self._call("bd_sync")
 
     PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP = 0, 1, 2, 3, 4
+
+    def set_charge_values(self, qk):
+        self._call("bd_set_charge_values", np.ascontiguousarray(qk, np.float64))
+
+    def coulomb_energy(self):
+        o = np.zeros(4)
+        self._call("bd_coulomb_energy", o)
+        return dict(real=o[0], reciprocal=o[1], self=o[2], total=o[3])
 
     # Lanczos preconditioner
     PRECOND = {"none": 0, "segment": 1, "learned": 2, "blocks": 3}

@@ -604,6 +604,14 @@ int bd_create(const bd_params* p, bd_ctx** out) {
     c->pme_p = p->pme_order > 0 ? p->pme_order : 8;
     c->pme_rc = p->pme_rc > 0 ? p->pme_rc : std::min(10.0, 0.43 * p->L);
     c->pme_alpha = p->pme_alpha > 0 ? p->pme_alpha : 4.0 / c->pme_rc;
+    c->cw_rc = p->coulomb_rc > 0 ? p->coulomb_rc : std::min(10.0, 0.43 * p->L);
+    c->cw_beta = p->coulomb_beta > 0 ? p->coulomb_beta : 3.5 / c->cw_rc;
+    if (p->coulomb < 0 || p->coulomb > 1 ||
+        (p->coulomb == BD_COULOMB_EWALD && (K < 8 || K > 1024 || c->pme_p < 4 || c->pme_p > 8 ||
+                                            (c->pme_p & 1) || c->cw_rc > 0.43 * p->L))) {
+      bd_destroy(c);
+      return BD_ERR_ARG;
+    }
     if (p->mobility == BD_MOB_PME &&
         (K < 8 || K > 1024 || c->pme_p < 4 || c->pme_p > 8 || (c->pme_p & 1) || c->pme_p > K ||
          c->pme_rc > 0.43 * p->L)) {
@@ -709,6 +717,7 @@ int bd_destroy(bd_ctx* c) {
   for (void* q : ptrs)
     if (q) cudaFree(q);
   pme_free(c);
+  coulomb_free(c);
   precond_free(c);
   mpnn_free(c);
   if (c->Lt1) cudaFree(c->Lt1);
@@ -827,6 +836,8 @@ int bd_set_charges(bd_ctx* c, const int* track, int nch) {
     q[track[k]] = 1.0;
   }
   c->nch = nch;
+  c->cw_q2 = nch;
+  c->cw_Q = nch;
   if (nch) {
     CU(cudaMemcpyAsync(c->track, track, 4 * (size_t)nch, cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemcpyAsync(c->old, track, 4 * (size_t)nch, cudaMemcpyHostToDevice, c->stream));
@@ -992,11 +1003,13 @@ int bd_ev_force(bd_ctx* c) {
 
 int bd_coulomb_force(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
-  if (c->nch < 2) return BD_OK;
+  bool ewald = c->p.coulomb == BD_COULOMB_EWALD;
+  if (c->nch < (ewald ? 1 : 2)) return BD_OK;
   double4* cq = (double4*)c->dE;
   c->launches++;
   k_gather_charges<<<nblk(c->nch, 256), 256, 0, c->stream>>>(c->rx, c->ry, c->rz, c->q, c->track,
                                                              c->nch, cq);
+  if (ewald) return coulomb_ewald(c, kernel_lat(c), cq);
   c->launches++;
   k_coulomb<<<nblk(c->nch * 32, 256), 256, 0, c->stream>>>(kernel_lat(c), cq, c->track, c->nch,
                                                            c->fx, c->fy, c->fz, c->p.lambda_b,

@@ -95,6 +95,13 @@ struct bd_ctx {
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
   int lan_last, pre_last;
 
+  // Ewald Coulomb (bd_coulomb.cu)
+  double cw_beta, cw_rc, cw_q2, cw_Q, cw_cell_V;
+  double *cw_grid, *cw_bsq, *cw_epart, *cw_energy, *cw_w;
+  void *cw_spec;
+  int *cw_base, *cw_cell_of, *cw_idx, *cw_count, *cw_start, *cw_cursor;
+  int cw_nblk, cw_plan_f, cw_plan_b;
+
   // block preconditioner of the Lanczos solve
   int pre_kind;       // bd_precond_kind
   int pre_S;          // beads per block
@@ -171,6 +178,10 @@ int charge_hop(bd_ctx* c);
 int pme_prepare(bd_ctx* c, const Lat& l);
 int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride);
 void pme_free(bd_ctx* c);
+
+// Ewald Coulomb
+int coulomb_ewald(bd_ctx* c, const Lat& l, const double4* cq);
+void coulomb_free(bd_ctx* c);
 
 // block preconditioner
 int precond_build(bd_ctx* c, const Lat& l);
