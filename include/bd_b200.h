@@ -81,6 +81,11 @@ typedef enum { BD_SPRING_HOOKEAN = 0, BD_SPRING_FENE = 1 } bd_spring;
  * counterpart; real-space pairs within coulomb_rc plus a particle-mesh
  * reciprocal sum on the pme_grid / pme_order grid). */
 typedef enum { BD_COULOMB_DH = 0, BD_COULOMB_EWALD = 1 } bd_coulomb_kind;
+/* Charge-hop sweep: the reference's sequential sweep (chargeHop,
+ * shear/src/main26.c:1926-2390, ran1 draws, bit-exact), or a parallel sweep
+ * on independent sets of cells at least hop_radius apart with Philox draws
+ * (no reference counterpart; bd_charge_hop documents its approximation). */
+typedef enum { BD_HOP_SEQUENTIAL = 0, BD_HOP_PARALLEL = 1 } bd_hop_kind;
 
 /* System parameters.  The names follow the reference's globals
  * (shear/src/Parameters.h:57-199) and Input.txt keys
@@ -128,6 +133,9 @@ typedef struct {
   int coulomb;               /* bd_coulomb_kind */
   double coulomb_beta;       /* Ewald split; 0 -> 3.5 / coulomb_rc (erfc(3.5) = 7e-7) */
   double coulomb_rc;         /* real-space cutoff; 0 -> the smaller of 10 and 0.43 L */
+  int hop;                   /* bd_hop_kind */
+  double hop_radius;         /* parallel sweep: minimum distance between cells that
+                                move at once; 0 -> 3 lambda_d */
 } bd_params;
 
 typedef struct bd_ctx bd_ctx;

@@ -70,6 +70,7 @@ class Params(C.Structure):
         ("lanczos_max", C.c_int), ("pme_grid", C.c_int), ("pme_order", C.c_int),
         ("pme_rc", C.c_double), ("pme_alpha", C.c_double), ("pme_max_pairs", C.c_int),
         ("coulomb", C.c_int), ("coulomb_beta", C.c_double), ("coulomb_rc", C.c_double),
+        ("hop", C.c_int), ("hop_radius", C.c_double),
     ]
 
 
@@ -259,7 +260,7 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
                 noise="ran1", philox_seed=20261203, mobility="hybrid", precision="fp64",
                 lanczos_tol=1e-6, lanczos_max=0, pme_grid=0, pme_order=0, pme_rc=0.0,
                 pme_alpha=0.0, pme_max_pairs=0, coulomb="dh", coulomb_beta=0.0,
-                coulomb_rc=0.0) -> Params:
+                coulomb_rc=0.0, hop="sequential", hop_radius=0.0) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
     p.box_volume = box_volume
@@ -280,6 +281,8 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
     p.pme_alpha, p.pme_max_pairs = pme_alpha, pme_max_pairs
     p.coulomb = {"dh": 0, "ewald": 1}[coulomb]
     p.coulomb_beta, p.coulomb_rc = coulomb_beta, coulomb_rc
+    p.hop = {"sequential": 0, "parallel": 1}[hop]
+    p.hop_radius = hop_radius
     return p
 
 

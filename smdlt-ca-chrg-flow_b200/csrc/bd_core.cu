@@ -452,21 +452,6 @@ __device__ float gasdev_dev(Ran1& g) {
   return g.gset;
 }
 
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
-// as 1, 2, 3", SC'11): ten rounds of two 32x32->64 multiplies with a Weyl key
-// schedule.
-__device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
-  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-#pragma unroll
-  for (int r = 0; r < 10; r++) {
-    uint32_t hi0 = __umulhi(M0, ctr.x), lo0 = M0 * ctr.x;
-    uint32_t hi1 = __umulhi(M1, ctr.z), lo1 = M1 * ctr.z;
-    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
-    key.x += W0;
-    key.y += W1;
-  }
-  return ctr;
-}
 
 // Gaussian noise from Philox: counter (pair index, step, stream), key = seed;
 // two 53-bit uniforms per draw, Box-Muller (u1 in (0,1]) for two deviates.
@@ -604,6 +589,11 @@ int bd_create(const bd_params* p, bd_ctx** out) {
     c->pme_p = p->pme_order > 0 ? p->pme_order : 8;
     c->pme_rc = p->pme_rc > 0 ? p->pme_rc : std::min(10.0, 0.43 * p->L);
     c->pme_alpha = p->pme_alpha > 0 ? p->pme_alpha : 4.0 / c->pme_rc;
+    c->hop_R = p->hop_radius > 0 ? p->hop_radius : 3.0 * p->lambda_d;
+    if (p->hop < 0 || p->hop > 1) {
+      bd_destroy(c);
+      return BD_ERR_ARG;
+    }
     c->cw_rc = p->coulomb_rc > 0 ? p->coulomb_rc : std::min(10.0, 0.43 * p->L);
     c->cw_beta = p->coulomb_beta > 0 ? p->coulomb_beta : 3.5 / c->cw_rc;
     if (p->coulomb < 0 || p->coulomb > 1 ||
@@ -718,6 +708,7 @@ int bd_destroy(bd_ctx* c) {
     if (q) cudaFree(q);
   pme_free(c);
   coulomb_free(c);
+  if (c->hop_cells) cudaFree(c->hop_cells);
   precond_free(c);
   mpnn_free(c);
   if (c->Lt1) cudaFree(c->Lt1);

@@ -95,6 +95,11 @@ struct bd_ctx {
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
   int lan_last, pre_last;
 
+  // parallel charge-hop sweep
+  double hop_R;
+  int *hop_cells;
+  unsigned long long hop_sweeps;
+
   // Ewald Coulomb (bd_coulomb.cu)
   double cw_beta, cw_rc, cw_q2, cw_Q, cw_cell_V;
   double *cw_grid, *cw_bsq, *cw_epart, *cw_energy, *cw_w;

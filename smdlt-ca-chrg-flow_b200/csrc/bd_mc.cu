@@ -19,8 +19,7 @@
 #include <math.h>
 
 #include "bd_ctx.cuh"
-
-using namespace bd;
+#include "bd_cell.cuh"
 
 #define CU(call)                                  \
   do {                                            \
@@ -233,9 +232,12 @@ __global__ void k_gather_charges_mc(const double* __restrict__ rx, const double*
 
 namespace bd {
 
+int charge_hop_parallel(bd_ctx* c);
+
 int charge_hop(bd_ctx* c) {
   if (c->nch == 0) return BD_OK;
   if (c->t % (unsigned long)c->p.MStep != 0) return BD_OK;
+  if (c->p.hop == BD_HOP_PARALLEL) return charge_hop_parallel(c);
   int nch = c->nch, N = c->N;
   size_t smem = (((size_t)nch * 4 + 15) & ~(size_t)15) + 8 * (size_t)nch;
   // scratch in dE (64 N doubles): [0, 4 nch) gathered (x,y,z,q); then row
@@ -274,6 +276,266 @@ int charge_hop(bd_ctx* c) {
   c->launches++;
   k_clear_charges<<<(N + 255) / 256, 256, 0, c->stream>>>(c->cflags, c->q, N);
   c->launches++;
+  k_scatter_charges<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->track, qk, nch, c->cflags, c->q);
+  return launch_ok(c);
+}
+
+}  // namespace bd
+
+// ---------------------------------------------------------------------------
+// Parallel sweep on independent sets (no reference counterpart).
+//
+// The charges are binned into cells of the Gauss-reduced cell at least R
+// wide (R = hop_radius, default 3 Debye lengths), with an even number of
+// cells per direction; the parity of the three cell indices gives eight
+// colours, and cells of one colour are at least R apart.  A sweep runs the
+// eight colours in turn; within a colour every cell is one CTA that visits its
+// charges in index order, each exactly once.  A trial follows the reference's
+// proposal rules (partner search, chain ends, occupancy, the two barriers) and
+// accepts with min(1, exp(-barrier - dE/2)), dE the Debye-Hueckel energy change
+// of the move against every other charge (the reference's energy and factor;
+// without its stale starting energy).  The other charges are taken at their
+// sites at the start of the colour, those of the own cell at their current
+// sites; a move therefore ignores only the change of its interaction with
+// charges moved in the same colour, which are at least R away
+// (|dU| <= lambda_B exp(-R kappa)/R per pair).  The draws are Philox4x32-10
+// counters (charge, sweep, purpose) under philox_seed, so a sweep does not
+// depend on the launch order.  The partner is the first bead of the charge's
+// Verlet row (sorted ascending, radius 6 > 2.1 plus twice the skin) within
+// |NID|^2 < 4.41, as the reference's scan over all beads finds it.
+
+namespace {
+
+constexpr int kHopCellCap = 8192;
+
+struct HGeom {
+  int n[3];
+};
+
+__device__ __forceinline__ double philox_u01(int k, unsigned long long sweep, int tag,
+                                             unsigned long long seed) {
+  uint4 c = make_uint4((uint32_t)k, (uint32_t)sweep, (uint32_t)(sweep >> 32),
+                       0x4d430000u | (uint32_t)tag);
+  uint4 x = philox4x32_10(c, make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  return (double)(((unsigned long long)(x.x >> 5) << 26) | (x.y >> 6)) *
+         (1.0 / 9007199254740992.0);
+}
+
+__global__ void k_hop_cells(Cell cell, HGeom g, const double* __restrict__ rx,
+                            const double* __restrict__ ry, const double* __restrict__ rz,
+                            const int* __restrict__ track, int nch, double cr, double sr,
+                            int* cell_of, int* count) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nch) return;
+  int b = track[k];
+  double x = rx[b] * cr - ry[b] * sr, y = rx[b] * sr + ry[b] * cr, s[3];
+  frac_of(cell, x, y, rz[b], s);
+  int cd[3];
+  for (int d = 0; d < 3; d++) {
+    double sd = s[d] - floor(s[d]);
+    int c = (sd >= 0.0 && sd <= 1.0) ? (int)(sd * g.n[d]) : 0;
+    cd[d] = c >= g.n[d] ? g.n[d] - 1 : c;
+  }
+  int c = (cd[0] * g.n[1] + cd[1]) * g.n[2] + cd[2];
+  cell_of[k] = c;
+  atomicAdd(&count[c], 1);
+}
+
+__global__ void k_hop_scan(int ncell, int* count, int* start) {
+  __shared__ int part[1024];
+  int t = threadIdx.x, nt = blockDim.x;
+  int per = (ncell + nt - 1) / nt, lo = t * per, hi = min(ncell, lo + per), s = 0;
+  for (int c = lo; c < hi; c++) s += count[c];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < nt; o <<= 1) {
+    int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int b = part[t] - s;
+  for (int c = lo; c < hi; c++) {
+    start[c] = b;
+    b += count[c];
+    count[c] = 0;
+  }
+  if (t == nt - 1) start[ncell] = part[t];
+}
+
+// One thread per cell lists its charges in increasing index (a fixed order).
+__global__ void k_hop_fill(const int* __restrict__ cell_of, const int* __restrict__ start,
+                           int ncell, int nch, int* idx) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int p = start[c];
+  for (int k = 0; k < nch; k++)
+    if (cell_of[k] == c) idx[p++] = k;
+}
+
+__global__ void __launch_bounds__(256) k_hop_colour(
+    Lat l, HGeom g, int colour, const double* __restrict__ rx, const double* __restrict__ ry,
+    const double* __restrict__ rz, int N, int Nb, int nch, const int* __restrict__ start,
+    const int* __restrict__ idx, const int* __restrict__ cell_of,
+    const int* __restrict__ site0, const double* __restrict__ qk, int* track, int* old,
+    int* flags, const int* __restrict__ nb_count, const int* __restrict__ nb_rows, int maxnb,
+    double lambda_b, double kappa_d, double barrier, double barrier2, unsigned long long seed,
+    unsigned long long sweep, int* log) {
+  int cell = blockIdx.x;
+  int cz = cell % g.n[2], cy = (cell / g.n[2]) % g.n[1], cx = cell / (g.n[1] * g.n[2]);
+  int col = ((g.n[0] > 1 ? cx & 1 : 0) << 2) | ((g.n[1] > 1 ? cy & 1 : 0) << 1) |
+            (g.n[2] > 1 ? cz & 1 : 0);
+  if (col != colour) return;
+  __shared__ double red[33];
+  __shared__ int s_first, s_c2, s_test, s_block;
+  int t = threadIdx.x, nt = blockDim.x;
+  for (int q = start[cell]; q < start[cell + 1]; q++) {
+    int k = idx[q];
+    int c = track[k];
+    if (t == 0) s_first = 0x7fffffff;
+    __syncthreads();
+    double xc = rx[c], yc = ry[c], zc = rz[c];
+    int nr = min(nb_count[c], maxnb);
+    for (int e = t; e < nr; e += nt) {
+      int j = nb_rows[(size_t)c * maxnb + e];
+      if (j == c || j == c + 1 || j == c - 1) continue;
+      double vx, vy, vz;
+      min_image(l, subx(xc, rx[j]), subx(yc, ry[j]), subx(zc, rz[j]), vx, vy, vz);
+      if (rr3(vx, vy, vz) < 4.41) atomicMin(&s_first, j);
+    }
+    __syncthreads();
+    if (t == 0) {
+      double mm = philox_u01(k, sweep, 0, seed);
+      int c2, test = 0, sblock;
+      if (s_first != 0x7fffffff) {
+        if (mm < .33) {
+          c2 = c + 1;
+          sblock = (c == N - 1 || c % Nb == Nb - 1 || c == Nb - 1);
+          test = 1;
+        } else if (mm > 0.66) {
+          c2 = c - 1;
+          sblock = (c2 < 0 || c == 0 || c % Nb == 0);
+          test = 1;
+        } else {
+          c2 = s_first;
+          sblock = 0;
+          test = 2;
+        }
+      } else if (mm > .5) {
+        c2 = c + 1;
+        sblock = (c == N - 1 || c % Nb == Nb - 1 || c == Nb - 1);
+      } else {
+        c2 = c - 1;
+        sblock = (c2 < 0 || c == 0 || c % Nb == 0);
+      }
+      if (!sblock && flags[c2]) sblock = 1;  // occupied target
+      s_c2 = c2;
+      s_test = test;
+      s_block = sblock;
+    }
+    __syncthreads();
+    int c2 = s_c2;
+    if (s_block) {
+      if (t == 0) {
+        log[3 * k] = 0;
+        log[3 * k + 1] = c2;
+        log[3 * k + 2] = 0;
+      }
+      __syncthreads();
+      continue;
+    }
+    double x2 = rx[c2], y2 = ry[c2], z2 = rz[c2], de = 0, qme = qk[k];
+    for (int o = t; o < nch; o += nt) {
+      if (o == k) continue;
+      int b = cell_of[o] == cell ? track[o] : site0[o];
+      double xb = rx[b], yb = ry[b], zb = rz[b];
+      de += qme * qk[o] *
+            (dh_pair(l, x2, y2, z2, xb, yb, zb, lambda_b, kappa_d) -
+             dh_pair(l, xc, yc, zc, xb, yb, zb, lambda_b, kappa_d));
+    }
+    de = block_sum(de, red);
+    if (t == 0) {
+      double bar = (s_test == 2) ? barrier2 : barrier;
+      double x = exp(-bar - 0.5 * de);
+      int acc = (1 <= x) ? 1 : (philox_u01(k, sweep, 1, seed) <= x);
+      old[k] = c;
+      if (acc) {
+        flags[c] = 0;
+        flags[c2] = 1;
+        track[k] = c2;
+      }
+      log[3 * k] = acc ? 1 : 2;
+      log[3 * k + 1] = c2;
+      log[3 * k + 2] = s_test;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+namespace bd {
+
+int charge_hop_parallel(bd_ctx* c) {
+  int nch = c->nch, N = c->N;
+  if (!c->hop_cells) {
+    CU(cudaMalloc(&c->hop_cells, 4 * ((size_t)3 * N + 2 * (kHopCellCap + 1))));
+    c->bytes += 4 * ((size_t)3 * N + 2 * (kHopCellCap + 1));
+    CU(cudaMemsetAsync(c->hop_cells, 0, 4 * ((size_t)3 * N + 2 * (kHopCellCap + 1)), c->stream));
+  }
+  int* cell_of = c->hop_cells;
+  int* idx = cell_of + N;
+  int* site0 = idx + N;
+  int* count = site0 + N;
+  int* start = count + kHopCellCap + 1;
+  Lat l = c->lat;
+  int treal = (int)(c->t % (unsigned long)c->tp);
+  l.treal = treal;
+  l.delx = c->p.edot * treal * c->p.dt;
+  Cell cell = make_cell(l);
+  double cr = 1.0, sr = 0.0;
+  if (l.flow == BD_FLOW_EXT) {
+    cr = l.cth;
+    sr = l.sth;
+  }
+  double R = c->hop_R;
+  HGeom g;
+  for (int j = 0; j < 3; j++) {
+    double a[3][3];
+    for (int q = 0; q < 3; q++)
+      for (int d = 0; d < 3; d++) a[q][d] = cell.H[d * 3 + q];
+    const double* u = a[(j + 1) % 3];
+    const double* v = a[(j + 2) % 3];
+    double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2],
+           cz = u[0] * v[1] - u[1] * v[0];
+    int n = (int)floor(cell.V / sqrt(cx * cx + cy * cy + cz * cz) / R);
+    g.n[j] = n >= 2 ? n - (n & 1) : 1;
+  }
+  while ((long)g.n[0] * g.n[1] * g.n[2] > kHopCellCap) {
+    int d = g.n[0] >= g.n[1] && g.n[0] >= g.n[2] ? 0 : (g.n[1] >= g.n[2] ? 1 : 2);
+    g.n[d] -= 2;
+  }
+  int ncell = g.n[0] * g.n[1] * g.n[2];
+  double* qk = c->dE + 6 * (size_t)nch;  // charge values in track order
+  c->launches += 4;
+  k_charge_values<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->q, c->track, nch, qk);
+  k_hop_cells<<<(nch + 255) / 256, 256, 0, c->stream>>>(cell, g, c->rx, c->ry, c->rz, c->track,
+                                                        nch, cr, sr, cell_of, count);
+  k_hop_scan<<<1, 1024, 0, c->stream>>>(ncell, count, start);
+  k_hop_fill<<<(ncell + 127) / 128, 128, 0, c->stream>>>(cell_of, start, ncell, nch, idx);
+  unsigned long long sweep = c->hop_sweeps++;
+  prof_begin(c, BD_PROF_HOP);
+  for (int colour = 0; colour < 8; colour++) {
+    CU(cudaMemcpyAsync(site0, c->track, 4 * (size_t)nch, cudaMemcpyDeviceToDevice, c->stream));
+    c->launches++;
+    k_hop_colour<<<ncell, 256, 0, c->stream>>>(
+        l, g, colour, c->rx, c->ry, c->rz, N, c->Nb, nch, start, idx, cell_of, site0, qk,
+        c->track, c->old, c->cflags, c->nb_count, c->nb_rows, c->maxnb, c->p.lambda_b,
+        c->kappa_d, c->p.barrier, c->p.barrier2, c->p.philox_seed, sweep, c->hoplog);
+  }
+  prof_end(c, BD_PROF_HOP);
+  c->launches += 2;
+  k_clear_charges<<<(N + 255) / 256, 256, 0, c->stream>>>(c->cflags, c->q, N);
   k_scatter_charges<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->track, qk, nch, c->cflags, c->q);
   return launch_ok(c);
 }
