@@ -263,21 +263,28 @@ PATHS = {
     # (products accumulated in FP64) or FP64
     "lanczos32": dict(mobility="ewald", precision="fp32", step="lanczos", bytes_per_block=24),
     "lanczos64": dict(mobility="ewald", precision="fp64", step="lanczos", bytes_per_block=48),
+    # The particle-mesh paths run the configs' own physics ("north"): chains
+    # alternately polyanion / polycation (charges -1 / +1 on the seeded half of
+    # each chain's beads), Coulomb by Ewald summation, and the parallel
+    # independent-set charge-hop sweep on Philox draws.  The dense-tile paths
+    # keep the reference's (Debye-Hueckel, unsigned charges, sequential sweep).
     # the same Ewald sum applied matrix-free by smooth particle-mesh Ewald
     # (grid 1.45 L, B-spline order 8, real-space cutoff 10)
-    "pme64": dict(mobility="pme", precision="fp64", step="lanczos", bytes_per_block=None),
+    "pme64": dict(mobility="pme", precision="fp64", step="lanczos", bytes_per_block=None,
+                  physics="north"),
     # the same in FP32 storage (grids, FFTs, influence, pair tensors) with FP64
     # accumulation of the interpolation and pair sums
-    "pme32": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None),
+    "pme32": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None,
+                  physics="north"),
     # FP32 particle-mesh products with a preconditioned Krylov solve: segment
     # blocks (Cholesky of the free-space RPY mobility of 10 consecutive
     # beads), or those with the learned per-bead blocks on top (parameters
     # from smdlt-ca-chrg-flow_b200/mpnn_params.npy, made by
     # train_preconditioner.py)
     "pme32-seg": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None,
-                      precond="segment"),
+                      precond="segment", physics="north"),
     "pme32-learned": dict(mobility="pme", precision="fp32", step="lanczos", bytes_per_block=None,
-                          precond="learned"),
+                          precond="learned", physics="north"),
     # the reference's own algorithm: hybrid mobility + CA-TEA displacement
     "tea": dict(mobility="hybrid", precision="fp64", step="reference", bytes_per_block=48),
 }
@@ -288,9 +295,12 @@ def build_context(w, seed, path="lanczos32", device_noise="philox"):
     edot = edot_of(w)
     x, y, z, q, beta, C = synth_inputs(w, seed)
     pp = PATHS[path]
+    north = pp.get("physics") == "north"
     p = B.make_params(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
                       noise=device_noise, philox_seed=seed, mobility=pp["mobility"],
-                      precision=pp["precision"], lanczos_tol=1e-6, **force_params(w))
+                      precision=pp["precision"], lanczos_tol=1e-6,
+                      coulomb="ewald" if north else "dh",
+                      hop="parallel" if north else "sequential", **force_params(w))
     c = B.Context(p)
     if pp["mobility"] == "hybrid":
         c.build_grid(0.001)
@@ -298,6 +308,8 @@ def build_context(w, seed, path="lanczos32", device_noise="philox"):
         c.set_tea(sb, beta[sb], C[sb])
     c.set_positions(x, y, z)
     c.set_charges(q)
+    if north:
+        c.set_charge_values(np.where((q // w["Nb"]) % 2 == 0, -1.0, 1.0))
     c.set_time(0, 0)
     c.update_lattice(0)
     c.transform_coords()
@@ -430,6 +442,13 @@ def run_ours(args, rank, world, dist):
                                     % __import__("bd_b200").pme_default_grid(w["L"]) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
                        "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation",
+                       "electrostatics": ("Ewald Coulomb, chains alternately -1 / +1 on half "
+                                          "their beads" if PATHS[args.path].get("physics") ==
+                                          "north" else "Debye-Hueckel, unsigned charges "
+                                          "(reference)"),
+                       "charge_hop": ("parallel independent sets, Philox draws, "
+                                      "Debye-Hueckel energies" if PATHS[args.path].get("physics")
+                                      == "north" else "reference sequential sweep"),
                        "preconditioner": {None: "none", "segment": "segment blocks of 10 beads",
                                           "learned": "learned bead blocks on segment blocks "
                                                      "of 10 beads"}[
