@@ -307,6 +307,23 @@ int bd_precond_stats(bd_ctx *ctx, long *out4);
  * when the tolerance is missed */
 int bd_lanczos_inv_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
 
+/* ---- ensembles of replicas (no reference counterpart) --------------------
+ * A batch advances independent contexts (any sizes, flows, strain rates)
+ * concurrently: one host worker thread per replica drives that context's
+ * own CUDA stream.  bd_batch_step_lanczos runs bd_step_lanczos(t0, nsteps,
+ * with_hop) on every replica and returns when all have finished, with the
+ * first non-zero status.  Contexts stay owned by the caller and must outlive
+ * the batch; a context must not be used elsewhere while a batch step runs. */
+typedef struct bd_batch bd_batch;
+int bd_batch_create(bd_ctx *const *ctxs, int n, bd_batch **out);
+int bd_batch_step_lanczos(bd_batch *batch, unsigned long t0, int nsteps, int with_hop);
+int bd_batch_destroy(bd_batch *batch);
+/* Particle-mesh grid for a box of edge L: of the 2^a 3^b 5^c sizes between
+ * 1.45 L (the accuracy bound of the default discretisation) and 25 % above,
+ * the one with the fastest three-component FFT round trip on the current
+ * device (bd_precision for the storage); results are cached per process. */
+int bd_autotune_pme_grid(double L, int precision, int *K_out);
+
 /* ---- learned preconditioner network (no reference counterpart) ----------
  * Per bead, the BD_MPNN_NEIGHBORS nearest beads within BD_MPNN_CUTOFF
  * (minimum image) feed a three-layer message-passing network of width

@@ -24,7 +24,8 @@ ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
-           "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu", "bd_coulomb.cu"]
+           "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu", "bd_coulomb.cu",
+           "bd_batch.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -140,6 +141,10 @@ def _lib() -> C.CDLL:
         _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
         _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
         L.bd_set_preconditioner.argtypes = [vp, C.c_int, C.c_int]
+        L.bd_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
+        L.bd_batch_step_lanczos.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
+        L.bd_batch_destroy.argtypes = [vp]
+        L.bd_autotune_pme_grid.argtypes = [C.c_double, C.c_int, C.POINTER(C.c_int)]
         L.bd_set_charge_values.argtypes = [vp, _dp]
         L.bd_coulomb_energy.argtypes = [vp, _dp]
         L.bd_set_precond_blocks.argtypes = [vp, _dp]
@@ -168,6 +173,41 @@ def exported_symbols() -> list[str]:
 def _chk(status: int, where: str) -> None:
     if status != 0:
         raise BDError(status, where)
+
+
+class Batch:
+    """Independent replicas advanced concurrently (bd_batch_*); the contexts
+    stay owned by the caller and must outlive the batch."""
+
+    def __init__(self, contexts):
+        self.L = _lib()
+        self.ctxs = list(contexts)
+        arr = (C.c_void_p * len(self.ctxs))(*[c.h.value for c in self.ctxs])
+        h = C.c_void_p()
+        _chk(self.L.bd_batch_create(arr, len(self.ctxs), C.byref(h)), "bd_batch_create")
+        self.h = h
+
+    def step_lanczos(self, t0, nsteps, with_hop=True):
+        _chk(self.L.bd_batch_step_lanczos(self.h, int(t0), int(nsteps), int(bool(with_hop))),
+             "bd_batch_step_lanczos")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_pme_grid(L, precision="fp32"):
+    K = C.c_int()
+    _chk(_lib().bd_autotune_pme_grid(float(L), 1 if precision == "fp32" else 0, C.byref(K)),
+         "bd_autotune_pme_grid")
+    return K.value
 
 
 def mpnn_param_count() -> int:
