@@ -276,6 +276,22 @@ int bd_step_lanczos(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 /* One reference-mode hydrodynamic step (the body of the step loop,
  * shear/src/main26.c:65-151, extensional/src/main14.c:68-171, without file
  * output), repeated nsteps times from step t0. */
+/* ---- CA-TEA sampling ---------------------------------------------------
+ * [ewaldBin] main26.c:975: eps and rowsum (3 N) for the positions as they
+ * are (the caller chooses the frame, as the reference does). */
+int bd_ewald_bin(bd_ctx *ctx, double *eps, double *rowsum);
+/* [ewaldBin + CATEA] main26.c:975, 1340: adds one sample at the given strain
+ * to the running sums of its strain bin; returns the sample's beta. */
+int bd_catea(bd_ctx *ctx, double strain, double *beta);
+/* running averages per strain bin (sbins + 1): counts, beta = brun/count,
+ * C = Crun/(Nc count) (3 Nb per bin); zeros for empty bins */
+int bd_catea_averages(bd_ctx *ctx, int *counts, double *beta, double *C);
+/* [printTEA] main26.c:1807: the decomp/DC file of the averages */
+int bd_write_decomp(bd_ctx *ctx, const char *path, unsigned long t);
+/* [resetAverage] main26.c:1827: load the averages as the TEA parameters of
+ * every bin (bd_set_tea) and restart the running sums */
+int bd_catea_apply(bd_ctx *ctx);
+
 /* ---- signed charges and the Ewald Coulomb energy (no reference counterpart)
  * bd_set_charges gives every charge the value +1, as the reference's charge
  * flags do; bd_set_charge_values sets signed values per charge (in the order

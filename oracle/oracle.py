@@ -259,6 +259,9 @@ class RefSim:
         L_.h_step_hi.argtypes = [C.c_ulong, C.c_int]
         L_.h_wtime.restype = C.c_double
         L_.h_tp.restype = C.c_ulong
+        L_.h_ewald_bin.argtypes = [C.POINTER(C.c_double), _dp]
+        L_.h_catea.argtypes = [C.c_double, C.c_char_p, _dp, _dp, _ip]
+        self.Nb_, self.sbins = Nb, 20
 
     def __getattr__(self, name):
         return getattr(self.lib, "h_" + name)
@@ -267,6 +270,19 @@ class RefSim:
         x, y, z = (np.zeros(self.N) for _ in range(3))
         self.lib.h_get_pos(x, y, z)
         return x, y, z
+
+    def ewald_bin(self):
+        eps = C.c_double()
+        rs = np.zeros(3 * self.N)
+        self.lib.h_ewald_bin(C.byref(eps), rs)
+        return eps.value, rs
+
+    def catea(self, strain, beta_path):
+        brun = np.zeros(self.sbins + 1)
+        crun = np.zeros((self.sbins + 1) * 3 * self.Nb_)
+        gw = np.zeros(self.sbins + 1, np.int32)
+        self.lib.h_catea(float(strain), beta_path.encode(), brun, crun, gw)
+        return brun, crun.reshape(self.sbins + 1, 3 * self.Nb_), gw
 
     def set_pos(self, x, y, z):
         self.lib.h_set_pos(*(np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)))

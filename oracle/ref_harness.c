@@ -345,3 +345,31 @@ void h_begin_iteration(void) {
 /* Wall-clock seconds, for timing the reference on the host cores. */
 double h_wtime(void) { return omp_get_wtime(); }
 int h_max_threads(void) { return omp_get_max_threads(); }
+
+/* ewaldBin (shear/src/main26.c:975-1291): eps and rowsum (3N) for the current
+ * positions, with the accumulators cleared first and after. */
+void h_ewald_bin(double *eps_out, double *rowsum_out) {
+  eps = 0.0;
+  for (int i = 0; i < 3 * N; i++) rowsum[i] = 0.0;
+  ewaldBin();
+  *eps_out = eps;
+  memcpy(rowsum_out, rowsum, sizeof(double) * 3 * N);
+  eps = 0.0;
+  for (int i = 0; i < 3 * N; i++) rowsum[i] = 0.0;
+}
+
+/* ewaldBin + CATEA (shear/src/main26.c:1340-1381) at the given strain; CATEA
+ * appends its beta line to beta_path.  Returns the running sums brun
+ * (sbins+1), Crun ((sbins+1) x 3Nb) and gwcount (sbins+1). */
+void h_catea(double strain_, const char *beta_path, double *brun_out, double *crun_out,
+             int *gw_out) {
+  strain = strain_;
+  beta = (char *)beta_path;
+  ewaldBin();
+  CATEA();
+  for (int i = 0; i < sbins + 1; i++) {
+    brun_out[i] = brun[i];
+    gw_out[i] = gwcount[i];
+    for (int j = 0; j < 3 * Nb; j++) crun_out[(size_t)i * 3 * Nb + j] = Crun[i][j];
+  }
+}

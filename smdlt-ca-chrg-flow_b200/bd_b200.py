@@ -25,7 +25,7 @@ LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
            "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu", "bd_coulomb.cu",
-           "bd_batch.cu"]
+           "bd_batch.cu", "bd_catea.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -146,6 +146,11 @@ def _lib() -> C.CDLL:
         L.bd_batch_destroy.argtypes = [vp]
         L.bd_autotune_pme_grid.argtypes = [C.c_double, C.c_int, C.POINTER(C.c_int)]
         L.bd_set_charge_values.argtypes = [vp, _dp]
+        L.bd_ewald_bin.argtypes = [vp, C.POINTER(C.c_double), _dp]
+        L.bd_catea.argtypes = [vp, C.c_double, C.POINTER(C.c_double)]
+        L.bd_catea_averages.argtypes = [vp, _ip, _dp, _dp]
+        L.bd_write_decomp.argtypes = [vp, C.c_char_p, C.c_ulong]
+        L.bd_catea_apply.argtypes = [vp]
         L.bd_coulomb_energy.argtypes = [vp, _dp]
         L.bd_set_precond_blocks.argtypes = [vp, _dp]
         L.bd_download_precond_blocks.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
@@ -489,6 +494,30 @@ class Context:
         self._call("bd_sync")
 
     PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP = 0, 1, 2, 3, 4
+
+    def ewald_bin(self):
+        eps = C.c_double()
+        rs = np.zeros(3 * self.N)
+        self._call("bd_ewald_bin", C.byref(eps), rs)
+        return eps.value, rs
+
+    def catea(self, strain):
+        b = C.c_double()
+        self._call("bd_catea", float(strain), C.byref(b))
+        return b.value
+
+    def catea_averages(self, sbins=20):
+        n = np.zeros(sbins + 1, np.int32)
+        b = np.zeros(sbins + 1)
+        Cc = np.zeros((sbins + 1) * 3 * self.p.Nb)
+        self._call("bd_catea_averages", n, b, Cc)
+        return n, b, Cc.reshape(sbins + 1, 3 * self.p.Nb)
+
+    def write_decomp(self, path, t):
+        self._call("bd_write_decomp", path.encode(), int(t))
+
+    def catea_apply(self):
+        self._call("bd_catea_apply")
 
     def set_charge_values(self, qk):
         self._call("bd_set_charge_values", np.ascontiguousarray(qk, np.float64))

@@ -709,6 +709,8 @@ int bd_destroy(bd_ctx* c) {
   pme_free(c);
   coulomb_free(c);
   if (c->hop_cells) cudaFree(c->hop_cells);
+  if (c->cb_part) cudaFree(c->cb_part);
+  if (c->cb_tileI) cudaFree(c->cb_tileI);
   precond_free(c);
   mpnn_free(c);
   if (c->Lt1) cudaFree(c->Lt1);

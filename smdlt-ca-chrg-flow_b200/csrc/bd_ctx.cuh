@@ -95,6 +95,12 @@ struct bd_ctx {
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
   int lan_last, pre_last;
 
+  // CA-TEA sampling (bd_catea.cu)
+  double *cb_part;
+  int *cb_tileI;
+  std::vector<double> cat_brun, cat_crun;
+  std::vector<int> cat_gw;
+
   // parallel charge-hop sweep
   double hop_R;
   int *hop_cells;
@@ -183,6 +189,9 @@ int charge_hop(bd_ctx* c);
 int pme_prepare(bd_ctx* c, const Lat& l);
 int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride);
 void pme_free(bd_ctx* c);
+
+// CA-TEA sampling
+int ewald_bin(bd_ctx* c, double* eps, std::vector<double>& rowsum);
 
 // Ewald Coulomb
 int coulomb_ewald(bd_ctx* c, const Lat& l, const double4* cq);

@@ -996,3 +996,190 @@ extern "C" int bd_load_grid(bd_ctx* c, int nt, const double* D9) {
   CU(cudaStreamSynchronize(c->stream));
   return BD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// CA-TEA sampling: ewaldBin + CATEA (shear/src/main26.c:975-1381,
+// extensional/src/main14.c:1009-1415).
+//
+// ewaldBin evaluates the Ewald-summed RPY tensor of every bead pair i < j
+// with its own split (M_HI = 3.5; the images, k-vector box and self sums of
+// calcHI, including the self-image quirks) on the positions as they are
+// (no rotation) and accumulates eps = sum_pairs 2 sum_a D_a / Dtr_(a/3) over
+// the nine entries and rowsum[3i + a/3], rowsum[3j + a/3] += (D_a/Dtr)^2.
+// Here one CTA per packed tile computes the tensors as k_hi_ewald_tiles does
+// and writes per-tile partial sums (eps, row and column contributions), which
+// a second kernel adds per bead in a fixed order.
+
+template <bool kSmem>
+__global__ void __launch_bounds__(256) k_ewald_bin_tiles(Lat l, Ewald ew,
+                                                         const double* __restrict__ rx,
+                                                         const double* __restrict__ ry,
+                                                         const double* __restrict__ rz, int N,
+                                                         int NT, const int* __restrict__ tileI,
+                                                         const double* __restrict__ kvec_g,
+                                                         double D0, double D1, double D2,
+                                                         double* part) {
+  extern __shared__ double ksh[];
+  __shared__ double colacc[8][96];
+  __shared__ double eacc[8];
+  long long tile = blockIdx.x;
+  int I = tileI[tile];
+  int J = I + (int)(tile - tile_off(I, NT));
+  const double* kvec = kvec_g;
+  if (kSmem) {
+    for (int e = threadIdx.x; e < 9 * ew.nk; e += blockDim.x) ksh[e] = kvec_g[e];
+    __syncthreads();
+    kvec = ksh;
+  }
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int j = J * 32 + lane;
+  double rxj = 0, ryj = 0, rzj = 0;
+  if (j < N) {
+    rxj = rx[j];
+    ryj = ry[j];
+    rzj = rz[j];
+  }
+  const double Dd[3] = {D0, D1, D2};
+  const int sym[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+  int side = 2 * ew.nmax + 1, nimg = side * side * side;
+  double* P = part + (size_t)tile * 193;
+  double col[3] = {0, 0, 0}, epsl = 0;
+  for (int q = 0; q < 4; q++) {
+    int il = w + 8 * q, i = I * 32 + il;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    bool pair = i < j && j < N;
+    if (pair) {
+      double dxo = rxj - rx[i], dyo = ryj - ry[i], dzo = rzj - rz[i];
+      for (int m = 0; m < nimg; m++) {
+        int nz = m % side - ew.nmax, ny = (m / side) % side - ew.nmax;
+        int nx = m / (side * side) - ew.nmax;
+        double dx = dxo + nx * l.L1x + ny * l.L2x;
+        double dy = dyo + nx * l.L1y + ny * l.L2y;
+        double dz = dzo + nz * l.L;
+        double rr = dx * dx + dy * dy + dz * dz;
+        if (sqrt(rr) < ew.rce) {
+          double t1, t2;
+          rpy_real(ew, rr, t1, t2);
+          acc[0] += t1 + t2 * dx * dx / rr;
+          acc[1] += t2 * dx * dy / rr;
+          acc[2] += t2 * dx * dz / rr;
+          acc[3] += t1 + t2 * dy * dy / rr;
+          acc[4] += t2 * dy * dz / rr;
+          acc[5] += t1 + t2 * dz * dz / rr;
+        }
+      }
+      for (int c = 0; c < ew.nk; c++) {
+        const double* kv = kvec + 9 * c;
+        double ck = cos(kv[0] * dxo + kv[1] * dyo + kv[2] * dzo);
+        acc[0] += kv[3] * ck;
+        acc[1] += kv[4] * ck;
+        acc[2] += kv[5] * ck;
+        acc[3] += kv[6] * ck;
+        acc[4] += kv[7] * ck;
+        acc[5] += kv[8] * ck;
+      }
+    }
+    double row[3] = {0, 0, 0};
+    if (pair) {
+      for (int a = 0; a < 9; a++) {
+        double incr = acc[sym[a]] / Dd[a / 3];
+        epsl += 2.0 * incr;
+        row[a / 3] += incr * incr;
+        col[a / 3] += incr * incr;
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      double v = row[a];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) P[1 + a * 32 + il] = v;
+    }
+  }
+  for (int a = 0; a < 3; a++) colacc[w][a * 32 + lane] = col[a];
+  for (int o = 16; o > 0; o >>= 1) epsl += __shfl_xor_sync(0xffffffffu, epsl, o);
+  if (lane == 0) eacc[w] = epsl;
+  __syncthreads();
+  if (threadIdx.x < 96) {
+    double s = 0;
+    for (int ww = 0; ww < 8; ww++) s += colacc[ww][threadIdx.x];
+    P[97 + threadIdx.x] = s;
+  }
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int ww = 0; ww < 8; ww++) s += eacc[ww];
+    P[0] = s;
+  }
+}
+
+// rowsum[3i + a] = sum of the row parts of tiles (K, J >= K) and the column
+// parts of tiles (I <= K, K); one CTA per bead block K, fixed order.
+__global__ void k_ewald_bin_reduce(const double* __restrict__ part, int NT, int N,
+                                   double* rowsum) {
+  int K = blockIdx.x, e = threadIdx.x;  // e = a * 32 + bead
+  if (e >= 96) return;
+  double s = 0;
+  for (int J = K; J < NT; J++) s += part[(size_t)(tile_off(K, NT) + (J - K)) * 193 + 1 + e];
+  for (int I = 0; I <= K; I++) s += part[(size_t)(tile_off(I, NT) + (K - I)) * 193 + 97 + e];
+  int a = e / 32, i = K * 32 + (e & 31);
+  if (i < N) rowsum[3 * i + a] = s;
+}
+
+__global__ void k_ewald_bin_eps(const double* __restrict__ part, long long ntiles, double* eps) {
+  double s = 0;
+  for (long long t = threadIdx.x; t < ntiles; t += 32) s += part[(size_t)t * 193];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) *eps = s;
+}
+
+namespace bd {
+
+// eps and rowsum (3N) of ewaldBin for the current positions and lattice.
+int ewald_bin(bd_ctx* c, double* eps, std::vector<double>& rowsum) {
+  int N = c->N, NT = (N + 31) / 32;
+  long long ntl = (long long)NT * (NT + 1) / 2;
+  if (!c->cb_part) {
+    CU(cudaMalloc(&c->cb_part, 8 * (size_t)ntl * 193 + 8 * (3 * (size_t)N + 1)));
+    CU(cudaMalloc(&c->cb_tileI, 4 * (size_t)ntl));
+    std::vector<int> ti(ntl);
+    size_t k = 0;
+    for (int I = 0; I < NT; I++)
+      for (int J = I; J < NT; J++) ti[k++] = I;
+    CU(cudaMemcpyAsync(c->cb_tileI, ti.data(), 4 * (size_t)ntl, cudaMemcpyHostToDevice,
+                       c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    c->bytes += 8 * (size_t)ntl * 193 + 8 * (3 * (size_t)N + 1) + 4 * (size_t)ntl;
+  }
+  Lat l = step_lat(c);
+  Ewald ew;
+  std::vector<double> kv;
+  double Dtr[3];
+  hi_setup(c, l, &ew, &kv, Dtr, 3.5, 0, false);
+  double* kdev = nullptr;
+  if (!kv.empty()) {
+    CU(cudaMalloc(&kdev, 8 * kv.size()));
+    CU(cudaMemcpyAsync(kdev, kv.data(), 8 * kv.size(), cudaMemcpyHostToDevice, c->stream));
+  }
+  double* rs = c->cb_part + (size_t)ntl * 193;
+  size_t smem = 8 * 9 * (size_t)ew.nk;
+  c->launches += 3;
+  if (smem <= 96 * 1024) {
+    cudaFuncSetAttribute(k_ewald_bin_tiles<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         96 * 1024);
+    k_ewald_bin_tiles<true><<<(unsigned)ntl, 256, smem, c->stream>>>(
+        l, ew, c->rx, c->ry, c->rz, N, NT, c->cb_tileI, kdev, Dtr[0], Dtr[1], Dtr[2],
+        c->cb_part);
+  } else {
+    k_ewald_bin_tiles<false><<<(unsigned)ntl, 256, 0, c->stream>>>(
+        l, ew, c->rx, c->ry, c->rz, N, NT, c->cb_tileI, kdev, Dtr[0], Dtr[1], Dtr[2],
+        c->cb_part);
+  }
+  k_ewald_bin_reduce<<<NT, 96, 0, c->stream>>>(c->cb_part, NT, N, rs);
+  k_ewald_bin_eps<<<1, 32, 0, c->stream>>>(c->cb_part, ntl, rs + 3 * (size_t)N);
+  rowsum.resize(3 * (size_t)N);
+  CU(cudaMemcpyAsync(rowsum.data(), rs, 24 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaMemcpyAsync(eps, rs + 3 * (size_t)N, 8, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  if (kdev) cudaFree(kdev);
+  return launch_ok(c);
+}
+
+}  // namespace bd
