@@ -292,6 +292,13 @@ int bd_write_decomp(bd_ctx *ctx, const char *path, unsigned long t);
  * every bin (bd_set_tea) and restart the running sums */
 int bd_catea_apply(bd_ctx *ctx);
 
+/* [calcMSD] main26.c:2494: mean-squared displacement of the charges from
+ * the displacement log w (Ncharges (Tmax + 1) records x, y, z in the order of
+ * the reference's CH file), with the reference's data layout; avg gets, for
+ * lags 1 .. Tmax - MSDstart, the rows {MSD, MSD_x, MSD_y, MSD_z} that
+ * calcMSD writes (the caller adds the lag time lag dt printprops). */
+int bd_msd(const double *w, int ncharges, int Tmax, int MSDstart, double *avg);
+
 /* ---- signed charges and the Ewald Coulomb energy (no reference counterpart)
  * bd_set_charges gives every charge the value +1, as the reference's charge
  * flags do; bd_set_charge_values sets signed values per charge (in the order

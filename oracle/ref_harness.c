@@ -373,3 +373,17 @@ void h_catea(double strain_, const char *beta_path, double *brun_out, double *cr
     for (int j = 0; j < 3 * Nb; j++) crun_out[(size_t)i * 3 * Nb + j] = Crun[i][j];
   }
 }
+
+/* calcMSD (shear/src/main26.c:2494-2637) on the CH file at ch_path, writing
+ * its MSD rows to out_path. */
+void h_msd(const char *ch_path, const char *out_path, int ncharges, unsigned long tmax_,
+           int printprops_, int msdstart, double dt_) {
+  str2 = (char *)ch_path;
+  outp1 = (char *)out_path;
+  Ncharges = ncharges;
+  tmax = tmax_;
+  printprops = printprops_;
+  MSDstart = msdstart;
+  dt = dt_;
+  calcMSD();
+}

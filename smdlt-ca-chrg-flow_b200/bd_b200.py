@@ -25,7 +25,7 @@ LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
            "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu", "bd_coulomb.cu",
-           "bd_batch.cu", "bd_catea.cu"]
+           "bd_batch.cu", "bd_catea.cu", "bd_msd.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -151,6 +151,7 @@ def _lib() -> C.CDLL:
         L.bd_catea_averages.argtypes = [vp, _ip, _dp, _dp]
         L.bd_write_decomp.argtypes = [vp, C.c_char_p, C.c_ulong]
         L.bd_catea_apply.argtypes = [vp]
+        L.bd_msd.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp]
         L.bd_coulomb_energy.argtypes = [vp, _dp]
         L.bd_set_precond_blocks.argtypes = [vp, _dp]
         L.bd_download_precond_blocks.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
@@ -206,6 +207,15 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def msd(w, ncharges, Tmax, MSDstart=0):
+    """calcMSD's rows {MSD, x, y, z} for lags 1..Tmax-MSDstart from the CH-file
+    ordered displacement log w (Ncharges (Tmax+1) x 3)."""
+    out = np.zeros(4 * (Tmax - MSDstart))
+    _chk(_lib().bd_msd(np.ascontiguousarray(w, np.float64).reshape(-1), int(ncharges), int(Tmax),
+                       int(MSDstart), out), "bd_msd")
+    return out.reshape(-1, 4)
 
 
 def autotune_pme_grid(L, precision="fp32"):
