@@ -299,6 +299,17 @@ int bd_catea_apply(bd_ctx *ctx);
  * calcMSD writes (the caller adds the lag time lag dt printprops). */
 int bd_msd(const double *w, int ncharges, int Tmax, int MSDstart, double *avg);
 
+/* ---- output files in the reference's formats --------------------------
+ * Unwrapped coordinates (3 N: px, py, pz as the reference's main builds
+ * them, shear/src/main26.c:75-85), per-chain x extension (Nc), centre of
+ * mass (3 Nc) and gyration tensor (6 Nc: xx xy xz yy yz zz); any pointer
+ * may be null. */
+int bd_chain_props(bd_ctx *ctx, double *p3N, double *ext, double *com, double *rg);
+int bd_write_trajectory(bd_ctx *ctx, const char *path, unsigned long t); /* [printTrajectory] main26.c:870 */
+int bd_write_restart(bd_ctx *ctx, const char *path, unsigned long t);    /* [printRestart] main26.c:902 */
+int bd_write_ext(bd_ctx *ctx, const char *path, unsigned long t, double strain); /* [calcExt+printExt] main26.c:926, 963 */
+int bd_write_visc(bd_ctx *ctx, const char *path, unsigned long t, int printperiod); /* [printVisc] main26.c:1866 */
+
 /* ---- signed charges and the Ewald Coulomb energy (no reference counterpart)
  * bd_set_charges gives every charge the value +1, as the reference's charge
  * flags do; bd_set_charge_values sets signed values per charge (in the order

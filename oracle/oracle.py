@@ -261,6 +261,11 @@ class RefSim:
         L_.h_tp.restype = C.c_ulong
         L_.h_ewald_bin.argtypes = [C.POINTER(C.c_double), _dp]
         L_.h_catea.argtypes = [C.c_double, C.c_char_p, _dp, _dp, _ip]
+        for name in ("h_print_traj", "h_print_ext"):
+            getattr(L_, name).argtypes = [C.c_char_p]
+        L_.h_print_visc.argtypes = [C.c_char_p, C.c_int]
+        L_.h_print_restart.argtypes = [C.c_char_p]
+        L_.h_get_unwrapped.argtypes = [_dp, _dp, _dp]
         L_.h_msd.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_ulong, C.c_int, C.c_int,
                              C.c_double]
         self.Nb_, self.sbins = Nb, 20

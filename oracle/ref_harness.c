@@ -387,3 +387,48 @@ void h_msd(const char *ch_path, const char *out_path, int ncharges, unsigned lon
   dt = dt_;
   calcMSD();
 }
+
+/* Output routines of the reference (shear/src/main26.c:870-974, 1866-1880)
+ * writing to the given paths. */
+#include <unistd.h>
+void h_print_traj(const char *path) {
+  xyz = (char *)path;
+  printTrajectory();
+}
+void h_print_ext(const char *path) {
+  /* the unwrapping loop of the reference's main (shear/src/main26.c:75-85) */
+  for (int i = 0; i < Nc; i++) {
+    px[i * Nb] = 0.0;
+    py[i * Nb] = 0.0;
+    pz[i * Nb] = 0.0;
+    for (int j = 0; j < Nb - 1; j++) {
+      Vector3D_t d = getNID(i * Nb + j, i * Nb + j + 1);
+      px[i * Nb + j + 1] = px[i * Nb + j] + d.x;
+      py[i * Nb + j + 1] = py[i * Nb + j] + d.y;
+      pz[i * Nb + j + 1] = pz[i * Nb + j] + d.z;
+    }
+  }
+  ext = (char *)path;
+  calcExt();
+  printExt();
+}
+void h_get_unwrapped(double *x, double *y, double *z) {
+  memcpy(x, px, sizeof(double) * N);
+  memcpy(y, py, sizeof(double) * N);
+  memcpy(z, pz, sizeof(double) * N);
+}
+void h_print_visc(const char *path, int period) {
+  visc = (char *)path;
+  printperiod = period;
+  printVisc();
+}
+/* printRestart names its file itself (res/R...xyz relative to the working
+ * directory): run it inside dir. */
+int h_print_restart(const char *dir) {
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(dir) != 0) return 1;
+  xyz = malloc(400);
+  xyzstart = 0;
+  printRestart();
+  return chdir(cwd);
+}

@@ -25,7 +25,7 @@ LIB = os.path.join(PKG, "libbd_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["bd_core.cu", "bd_neighbors.cu", "bd_mobility.cu", "bd_mc.cu", "bd_lanczos.cu",
            "bd_noalloc.cu", "bd_pme.cu", "bd_precond.cu", "bd_mpnn.cu", "bd_coulomb.cu",
-           "bd_batch.cu", "bd_catea.cu", "bd_msd.cu"]
+           "bd_batch.cu", "bd_catea.cu", "bd_msd.cu", "bd_output.cu"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -152,6 +152,11 @@ def _lib() -> C.CDLL:
         L.bd_write_decomp.argtypes = [vp, C.c_char_p, C.c_ulong]
         L.bd_catea_apply.argtypes = [vp]
         L.bd_msd.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp]
+        L.bd_chain_props.argtypes = [vp, _dp, _dp, _dp, _dp]
+        for n in ("bd_write_trajectory", "bd_write_restart"):
+            getattr(L, n).argtypes = [vp, C.c_char_p, C.c_ulong]
+        L.bd_write_ext.argtypes = [vp, C.c_char_p, C.c_ulong, C.c_double]
+        L.bd_write_visc.argtypes = [vp, C.c_char_p, C.c_ulong, C.c_int]
         L.bd_coulomb_energy.argtypes = [vp, _dp]
         L.bd_set_precond_blocks.argtypes = [vp, _dp]
         L.bd_download_precond_blocks.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
@@ -504,6 +509,24 @@ class Context:
         self._call("bd_sync")
 
     PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP = 0, 1, 2, 3, 4
+
+    def chain_props(self):
+        Nc = self.p.Nc
+        p, e, cm, rg = np.zeros(3 * self.N), np.zeros(Nc), np.zeros(3 * Nc), np.zeros(6 * Nc)
+        self._call("bd_chain_props", p, e, cm, rg)
+        return p.reshape(3, self.N), e, cm.reshape(Nc, 3), rg.reshape(Nc, 6)
+
+    def write_trajectory(self, path, t):
+        self._call("bd_write_trajectory", path.encode(), int(t))
+
+    def write_restart(self, path, t):
+        self._call("bd_write_restart", path.encode(), int(t))
+
+    def write_ext(self, path, t, strain):
+        self._call("bd_write_ext", path.encode(), int(t), float(strain))
+
+    def write_visc(self, path, t, printperiod):
+        self._call("bd_write_visc", path.encode(), int(t), int(printperiod))
 
     def ewald_bin(self):
         eps = C.c_double()
