@@ -234,6 +234,10 @@ enum {
   BD_PROF_STEP = 4,     /* one whole bd_step_reference call */
   BD_PROF_SLOTS = 8
 };
+/* Replay each Lanczos iteration (product and orthogonalisation) as a CUDA
+ * graph captured on first use (default on; off launches the kernels one by
+ * one).  Captured products do not record BD_PROF_MATVEC events. */
+int bd_enable_graphs(bd_ctx *ctx, int on);
 int bd_profile_enable(bd_ctx *ctx, int on); /* clears the accumulated events */
 int bd_profile_read(bd_ctx *ctx, int slot, double *total_ms, long *count);
 /* Number of kernels the library has launched on this context. */

@@ -141,6 +141,7 @@ def _lib() -> C.CDLL:
         _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
         _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
         L.bd_set_preconditioner.argtypes = [vp, C.c_int, C.c_int]
+        L.bd_enable_graphs.argtypes = [vp, C.c_int]
         L.bd_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.bd_batch_step_lanczos.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
         L.bd_batch_destroy.argtypes = [vp]
@@ -551,6 +552,9 @@ class Context:
 
     def catea_apply(self):
         self._call("bd_catea_apply")
+
+    def enable_graphs(self, on=True):
+        self._call("bd_enable_graphs", int(bool(on)))
 
     def set_charge_values(self, qk):
         self._call("bd_set_charge_values", np.ascontiguousarray(qk, np.float64))

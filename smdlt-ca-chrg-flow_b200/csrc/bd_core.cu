@@ -684,6 +684,7 @@ int bd_create(const bd_params* p, bd_ctx** out) {
     return s;
   }
   c->btab.assign(c->sbins + 1, 0.0);
+  c->use_graphs = true;
   c->t = 0;
   c->tstart = 0;
   host_lattice(c, 0, &c->lat);
@@ -715,9 +716,20 @@ int bd_destroy(bd_ctx* c) {
   mpnn_free(c);
   if (c->Lt1) cudaFree(c->Lt1);
   if (c->Lt2) cudaFree(c->Lt2);
+  if (c->Lvcur) cudaFree(c->Lvcur);
+  if (c->Ljd) cudaFree(c->Ljd);
+  lanczos_graphs_reset(c);
   prof_clear(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+  return BD_OK;
+}
+
+int bd_enable_graphs(bd_ctx* c, int on) {
+  if (!c) return BD_ERR_ARG;
+  CU(cudaStreamSynchronize(c->stream));
+  c->use_graphs = on != 0;
+  if (!c->use_graphs) lanczos_graphs_reset(c);
   return BD_OK;
 }
 
@@ -1122,14 +1134,14 @@ void rotate_coords(bd_ctx* c, int inverse) {
 
 namespace bd {
 void prof_begin(bd_ctx* c, int slot) {
-  if (!c->prof_on) return;
+  if (!c->prof_on || c->capturing) return;
   cudaEvent_t e;
   cudaEventCreate(&e);
   cudaEventRecord(e, c->stream);
   c->prof_ev[slot][0].push_back(e);
 }
 void prof_end(bd_ctx* c, int slot) {
-  if (!c->prof_on) return;
+  if (!c->prof_on || c->capturing) return;
   cudaEvent_t e;
   cudaEventCreate(&e);
   cudaEventRecord(e, c->stream);

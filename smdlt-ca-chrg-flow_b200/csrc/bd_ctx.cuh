@@ -92,6 +92,11 @@ struct bd_ctx {
   double *MF;     // M F, 3 x NTp
   double *Yz;     // sqrt(M) z, 3 x NTp
   double *Lt1, *Lt2;  // work vectors of the preconditioned products, 3 x NTp
+  double *Lvcur;      // input of the next product (v_j), 3 x NTp
+  int *Ljd;           // Lanczos iteration index on the device
+  void *lan_graph[2]; // captured iteration (plain, preconditioned), cudaGraphExec_t
+  long long lan_graph_launches[2];
+  bool use_graphs, capturing;
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
   int lan_last, pre_last;
 
@@ -205,6 +210,7 @@ int mpnn_blocks(bd_ctx* c, const Lat& l, double* G9);
 void mpnn_free(bd_ctx* c);
 
 // Krylov square root
+void lanczos_graphs_reset(bd_ctx* c);
 int alloc_lanczos(bd_ctx* c);
 int lanczos_sqrt(bd_ctx* c, const double* zdev_interleaved, bool with_force, int* iters);
 

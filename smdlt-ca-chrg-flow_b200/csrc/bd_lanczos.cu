@@ -149,19 +149,24 @@ __device__ __forceinline__ void sum_parts(const double* __restrict__ part, int n
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_orth0(const double* __restrict__ V, size_t vs, int nv,
+// The iteration index j lives on the device (*jd) so that one iteration's
+// launches are the same every iteration and can be replayed as a CUDA graph;
+// k_next_j advances it at the end of the iteration.
+__global__ void __launch_bounds__(256) k_orth0(const double* __restrict__ V, size_t vs,
+                                               const int* __restrict__ jd,
                                                const double* __restrict__ w, int n,
                                                double* part1) {
-  int lo, hi;
+  int nv = *jd + 1, lo, hi;
   chunk_range(n, lo, hi);
   chunk_dots(V, vs, nv, w, lo, hi, part1);
 }
 
-__global__ void __launch_bounds__(256) k_orth1(const double* __restrict__ V, size_t vs, int nv,
-                                               double* w, int n, const double* __restrict__ part1,
+__global__ void __launch_bounds__(256) k_orth1(const double* __restrict__ V, size_t vs,
+                                               const int* __restrict__ jd, double* w, int n,
+                                               const double* __restrict__ part1,
                                                double* part2, double* hsave) {
   __shared__ double h[kMaxKrylov + 1];
-  int lo, hi;
+  int nv = *jd + 1, lo, hi;
   chunk_range(n, lo, hi);
   sum_parts(part1, nv, h);
   if (blockIdx.x == 0)
@@ -171,13 +176,14 @@ __global__ void __launch_bounds__(256) k_orth1(const double* __restrict__ V, siz
   chunk_dots(V, vs, nv, w, lo, hi, part2);
 }
 
-__global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, size_t vs, int nv,
-                                               double* w, int n, const double* __restrict__ part2,
+__global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, size_t vs,
+                                               const int* __restrict__ jd, double* w, int n,
+                                               const double* __restrict__ part2,
                                                double* part3, const double* __restrict__ hsave,
-                                               double* alpha, int j) {
+                                               double* alpha) {
   __shared__ double h[kMaxKrylov + 1];
   __shared__ double red[8];
-  int lo, hi;
+  int j = *jd, nv = j + 1, lo, hi;
   chunk_range(n, lo, hi);
   sum_parts(part2, nv, h);
   double s2 = 0;
@@ -197,10 +203,14 @@ __global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, siz
   }
 }
 
+// beta_j = |w|; v_{j+1} = w / beta_j into the basis and into vcur (the
+// fixed input of the next iteration's product)
 __global__ void __launch_bounds__(256) k_orth3(const double* __restrict__ w, int n,
                                                const double* __restrict__ part3, double* beta,
-                                               int j, double* vnext, int write_next) {
+                                               const int* __restrict__ jd, double* V, size_t vs,
+                                               double* vcur) {
   __shared__ double b;
+  int j = *jd;
   if (threadIdx.x < 32) {
     double s = warp_sum_parts(part3, gridDim.x, 1);
     if (threadIdx.x == 0) {
@@ -209,11 +219,19 @@ __global__ void __launch_bounds__(256) k_orth3(const double* __restrict__ w, int
     }
   }
   __syncthreads();
-  if (!write_next) return;
   double f = b > 0 ? 1.0 / b : 0.0;
+  double* vnext = V + (size_t)(j + 1) * vs;
   int lo, hi;
   chunk_range(n, lo, hi);
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) vnext[i] = w[i] * f;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    double x = w[i] * f;
+    vnext[i] = x;
+    vcur[i] = x;
+  }
+}
+
+__global__ void k_next_j(int* jd) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *jd += 1;
 }
 
 // |z|^2 partials over the bead-interleaved noise
@@ -351,13 +369,82 @@ int alloc_lanczos(bd_ctx* c) {
   CU(cudaMalloc(&c->Yz, 8 * n));
   CU(cudaMalloc(&c->Lt1, 8 * n));
   CU(cudaMalloc(&c->Lt2, 8 * n));
+  CU(cudaMalloc(&c->Lvcur, 8 * n));
+  CU(cudaMalloc(&c->Ljd, 16));
   // the padding entries (beads N..NTp-1) of the work vectors stay zero: the
   // orthogonalisation runs over all 3 NTp entries and the particle-mesh
   // product and the preconditioner write only the N beads
-  for (double* q : {c->Lw, c->MF, c->Yz, c->Lt1, c->Lt2})
+  for (double* q : {c->Lw, c->MF, c->Yz, c->Lt1, c->Lt2, c->Lvcur})
     CU(cudaMemsetAsync(q, 0, 8 * n, c->stream));
   c->bytes += 8 * n * (c->lmax + 6) + 8 * (size_t)(c->lmax + 1) * (3 * kDotBlocks + 2) +
               8 * (size_t)(c->lmax + 16);
+  return BD_OK;
+}
+
+// One Lanczos iteration's launches: w = A v with v = vcur (A = M, or
+// G M G^T with the block preconditioner when pre; with force also M F into
+// c->MF), CGS2 against the basis, beta, v_{j+1}, j += 1.  Every argument is
+// the same in every iteration (the index j is read on the device), so the
+// launches can be captured once and replayed as a CUDA graph.
+static int lanczos_iteration(bd_ctx* c, bool pre, bool force) {
+  int s, NTp = c->NT * 32, n = 3 * NTp, blk = kDotBlocks;
+  size_t vs = (size_t)n;
+  cudaStream_t st = c->stream;
+  double* vc = c->Lvcur;
+  VecIn vin = {{vc, vc + NTp, vc + 2 * NTp}, 1};
+  VecIn vf = {{c->fx, c->fy, c->fz}, 1};
+  if (!pre) {
+    if (force) {
+      if ((s = sym_matvec(c, 2, vf, vin, c->MF, c->Lw, true)) != BD_OK) return s;
+    } else {
+      if ((s = sym_matvec(c, 1, vin, vin, c->Lw, c->Lw, true)) != BD_OK) return s;
+    }
+  } else {
+    precond_apply(c, 1, vc, c->Lt1);
+    VecIn vt = {{c->Lt1, c->Lt1 + NTp, c->Lt1 + 2 * NTp}, 1};
+    if (force) {
+      if ((s = sym_matvec(c, 2, vf, vt, c->MF, c->Lt2, true)) != BD_OK) return s;
+    } else {
+      if ((s = sym_matvec(c, 1, vt, vt, c->Lt2, c->Lt2, true)) != BD_OK) return s;
+    }
+    precond_apply(c, 0, c->Lt2, c->Lw);
+  }
+  double* part1 = c->Lpart;
+  double* part2 = c->Lpart + (size_t)(c->lmax + 1) * blk;
+  double* part3 = c->Lpart + (size_t)2 * (c->lmax + 1) * blk;
+  c->launches += 5;
+  k_orth0<<<blk, 256, 0, st>>>(c->LV, vs, c->Ljd, c->Lw, n, part1);
+  k_orth1<<<blk, 256, 0, st>>>(c->LV, vs, c->Ljd, c->Lw, n, part1, part2, c->Lc);
+  k_orth2<<<blk, 256, 0, st>>>(c->LV, vs, c->Ljd, c->Lw, n, part2, part3, c->Lc, c->Lh);
+  k_orth3<<<blk, 256, 0, st>>>(c->Lw, n, part3, c->Lsc + 8, c->Ljd, c->LV, vs, vc);
+  k_next_j<<<1, 32, 0, st>>>(c->Ljd);
+  return launch_ok(c);
+}
+
+// Launches one iteration, from the context's captured graph when graphs are
+// on (capturing it on first use).
+static int lanczos_iteration_graph(bd_ctx* c, bool pre) {
+  int v = pre ? 1 : 0;
+  if (!c->lan_graph[v]) {
+    cudaGraph_t g;
+    long long l0 = c->launches;
+    c->capturing = true;
+    CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int s = lanczos_iteration(c, pre, false);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->capturing = false;
+    if (s != BD_OK) return s;
+    if (e != cudaSuccess) return BD_ERR_CUDA;
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return BD_ERR_CUDA;
+    c->lan_graph[v] = (void*)ex;
+    c->lan_graph_launches[v] = c->launches - l0;
+    c->launches = l0;
+  }
+  CU(cudaGraphLaunch((cudaGraphExec_t)c->lan_graph[v], c->stream));
+  c->launches += c->lan_graph_launches[v];
   return BD_OK;
 }
 
@@ -373,55 +460,33 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
   int N = c->N, NTp = c->NT * 32, n = 3 * NTp, blk = kDotBlocks;
   size_t vs = (size_t)n;
   cudaStream_t st = c->stream;
-  // |z| and v_0
+  // |z|, v_0 (into the basis and the product input), j = 0
   c->launches += 3;
   k_sumsq<<<blk, 256, 0, st>>>(z, 3 * N, c->Lpart);
   k_norm_fin<<<1, 32, 0, st>>>(c->Lpart, blk, c->Lsc);
   k_interleaved_to_soa<<<(NTp + 255) / 256, 256, 0, st>>>(z, c->Lsc, c->LV, N, NTp);
+  CU(cudaMemcpyAsync(c->Lvcur, c->LV, 8 * vs, cudaMemcpyDeviceToDevice, st));
+  CU(cudaMemsetAsync(c->Ljd, 0, sizeof(int), st));
   double zn = 0;
   CU(cudaMemcpyAsync(&zn, c->Lsc, 8, cudaMemcpyDeviceToHost, st));
   std::vector<double> alpha, beta, cc, cprev;
   int m = 0, neg = 0;
   bool conv = false;
-  // alpha_j, beta_j stay on the device (Lh[0..lmax), Lh[lmax+1..]); the host
-  // reads them only at checkpoints: from two before the previous call's
-  // Krylov dimension on, every second iteration
+  // alpha_j, beta_j stay on the device (Lh, Lsc + 8); the host reads them
+  // only at checkpoints: from two before the previous call's Krylov
+  // dimension on, every second iteration
   double* d_alpha = c->Lh;
   double* d_beta = c->Lsc + 8;
   int& last = pre ? c->pre_last : c->lan_last;
   int next_check = std::max(4, last - 2);
   for (int j = 0; j < c->lmax; j++) {
-    double* vj = c->LV + (size_t)j * vs;
-    VecIn vin_j = {{vj, vj + NTp, vj + 2 * NTp}, 1};
-    VecIn vf = {{c->fx, c->fy, c->fz}, 1};
-    if (!pre) {
-      if (j == 0 && with_force) {
-        if ((s = sym_matvec(c, 2, vf, vin_j, c->MF, c->Lw, true)) != BD_OK) return s;
-      } else {
-        if ((s = sym_matvec(c, 1, vin_j, vin_j, c->Lw, c->Lw, true)) != BD_OK) return s;
-      }
-    } else {
-      // w = G M G^T v_j
-      precond_apply(c, 1, vj, c->Lt1);
-      VecIn vt = {{c->Lt1, c->Lt1 + NTp, c->Lt1 + 2 * NTp}, 1};
-      if (j == 0 && with_force) {
-        if ((s = sym_matvec(c, 2, vf, vt, c->MF, c->Lt2, true)) != BD_OK) return s;
-      } else {
-        if ((s = sym_matvec(c, 1, vt, vt, c->Lt2, c->Lt2, true)) != BD_OK) return s;
-      }
-      precond_apply(c, 0, c->Lt2, c->Lw);
-    }
-    int nv = j + 1;
-    double* part1 = c->Lpart;
-    double* part2 = c->Lpart + (size_t)(c->lmax + 1) * blk;
-    double* part3 = c->Lpart + (size_t)2 * (c->lmax + 1) * blk;
-    double* hsave = c->Lc;
-    c->launches += 4;
-    k_orth0<<<blk, 256, 0, st>>>(c->LV, vs, nv, c->Lw, n, part1);
-    k_orth1<<<blk, 256, 0, st>>>(c->LV, vs, nv, c->Lw, n, part1, part2, hsave);
-    k_orth2<<<blk, 256, 0, st>>>(c->LV, vs, nv, c->Lw, n, part2, part3, hsave, d_alpha, j);
-    k_orth3<<<blk, 256, 0, st>>>(c->Lw, n, part3, d_beta, j, c->LV + (size_t)(j + 1) * vs,
-                                 j + 1 <= c->lmax ? 1 : 0);
+    if (j == 0 && with_force)
+      s = lanczos_iteration(c, pre, true);
+    else if (c->use_graphs)
+      s = lanczos_iteration_graph(c, pre);
+    else
+      s = lanczos_iteration(c, pre, false);
+    if (s != BD_OK) return s;
     m = j + 1;
     if (m < next_check && m < c->lmax) continue;
     alpha.resize(m);
@@ -452,6 +517,17 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
   *conv_out = conv;
   CU(cudaStreamSynchronize(st));  // cc is a host vector read by the copy above
   return launch_ok(c);
+}
+
+// Drops the captured Lanczos iterations (their kernels hold the mobility's
+// diagonal and the preconditioner's buffers by value); called whenever those
+// change.
+void lanczos_graphs_reset(bd_ctx* c) {
+  for (int v = 0; v < 2; v++)
+    if (c->lan_graph[v]) {
+      cudaGraphExecDestroy((cudaGraphExec_t)c->lan_graph[v]);
+      c->lan_graph[v] = nullptr;
+    }
 }
 
 // sqrt(M) z for the bead-interleaved z on the device (c->R): result in c->Yz.

@@ -745,6 +745,7 @@ static Lat step_lat(bd_ctx* c) {
 
 int calc_hi(bd_ctx* c) {
   int s;
+  lanczos_graphs_reset(c);  // captured products hold the diagonal by value
   if (c->p.mobility == BD_MOB_PME) {
     prof_begin(c, BD_PROF_HI_BUILD);
     s = pme_prepare(c, step_lat(c));

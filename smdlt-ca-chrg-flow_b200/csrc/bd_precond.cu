@@ -232,6 +232,7 @@ static int pre_alloc(bd_ctx* c, int S) {
   size_t nb = (size_t)c->N / S, n = 3 * (size_t)S;
   size_t need = nb * n * n;
   if (c->pre_G && c->pre_cap >= need) return BD_OK;
+  lanczos_graphs_reset(c);  // captured products hold the block pointers
   if (c->pre_G) cudaFree(c->pre_G);
   if (c->pre_Gi) cudaFree(c->pre_Gi);
   c->pre_G = c->pre_Gi = nullptr;
@@ -344,6 +345,7 @@ int bd_set_preconditioner(bd_ctx* c, int kind, int segment) {
   }
   if (kind == BD_PRECOND_LEARNED && !c->mpnn_ready) return BD_ERR_STATE;
   CU(cudaStreamSynchronize(c->stream));
+  lanczos_graphs_reset(c);
   c->pre_kind = kind;
   c->pre_S = S;
   c->pre_ready = false;
@@ -369,6 +371,7 @@ int bd_set_precond_blocks(bd_ctx* c, const double* G9) {
   c->launches++;
   k_bead_invert<<<(c->N + 127) / 128, 128, 0, c->stream>>>(c->pre_G, c->pre_Gi, c->N,
                                                            c->pre_bad);
+  lanczos_graphs_reset(c);
   c->pre_kind = BD_PRECOND_BLOCKS;
   c->pre_S = 1;
   c->pre_ready = true;
