@@ -148,7 +148,10 @@ struct bd_ctx {
   int pme_plan_f, pme_plan_b;
   int rl_cap, rl_ncell_cap;  // real-space pair rows
   int *rl_cnt, *rl_rows, *rl_cell_of, *rl_beads, *rl_cell_count, *rl_cell_start, *rl_cursor;
-  void *rl_T;        // pair tensors, 6 per pair (FP64 or FP32)
+  void *rl_pos;      // lab-frame positions of the last preparation (double4)
+  void *rl_tt;       // per pair t1 and t2 / r^2 of the real-space tensor (FP64 or FP32)
+  double pme_cellbuf[19];  // its cell: H, H^-1, volume
+  double pme_alpha_ref;    // calcHI's split parameter at that step
 
   size_t bytes;
 

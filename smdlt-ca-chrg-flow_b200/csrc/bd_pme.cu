@@ -62,10 +62,11 @@ using namespace bd;
 __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
                               const double* __restrict__ ry, const double* __restrict__ rz,
                               double cr, double sr, int N, int K, int p, int* base, double* w,
-                              int* err) {
+                              double4* pos, int* err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double x = rx[i] * cr - ry[i] * sr, y = rx[i] * sr + ry[i] * cr, z = rz[i];
+  pos[i] = make_double4(x, y, z, 0.0);
   double s[3];
   frac_of(cell, x, y, z, s);
   for (int d = 0; d < 3; d++) {
@@ -214,6 +215,54 @@ __global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size
   spec[2 * n + e] = w;
 }
 
+// Real-space Beenakker kernel t1 I + t2 r r^T/r^2 (shear/src/main26.c:
+// 1727-1741) at split parameter alpha; with far the r > 2 form at any r.
+__device__ __forceinline__ void real_kernel(double alpha, double rr, bool far, double& t1,
+                                            double& t2) {
+  double r = sqrt(rr), a = alpha, a2 = a * a, a3 = a2 * a, a5 = a3 * a2, a7 = a5 * a2;
+  double C1, C2, C3, C4;
+  if (far || r > 2.0) {
+    C1 = 0.75 / r + 0.5 / (r * rr);
+    C2 = 4.0 * a7 * rr * rr + 3.0 * a3 * rr - 20.0 * a5 * rr - 4.5 * a + 14.0 * a3 + a / rr;
+    C3 = 0.75 / r - 1.5 / (r * rr);
+    C4 = -4.0 * a7 * rr * rr - 3.0 * a3 * rr + 16.0 * a5 * rr + 1.5 * a - 2.0 * a3 - 3.0 * a / rr;
+  } else {
+    C1 = 1.0 - 0.28125 * r;
+    C2 = 64.0 * a7 + 12.0 * a3 - 80.0 * a5 - 4.5 * a + 14.0 * a3 + 0.25 * a;
+    C3 = 0.09375 * r;
+    C4 = -64.0 * a7 - 12.0 * a3 + 64.0 * a5 + 1.5 * a - 2.0 * a3 - 0.75 * a;
+  }
+  double ec = erfc(a * r), ex = exp(-a2 * rr) / sqrt(M_PI);
+  t1 = C1 * ec + C2 * ex;
+  t2 = C3 * ec + C4 * ex;
+}
+
+// The overlap branch (bonded and touching beads), kept out of line.
+__device__ __noinline__ void overlap_terms(double alpha, double alpha_ref, double rr,
+                                           double* t) {
+  double f1, f2, o1, o2, g1, g2;
+  real_kernel(alpha, rr, true, f1, f2);
+  real_kernel(alpha_ref, rr, false, o1, o2);
+  real_kernel(alpha_ref, rr, true, g1, g2);
+  t[0] = f1 + (o1 - g1);
+  t[1] = f2 + (o2 - g2);
+}
+
+// t1, t2 of the real-space pair tensor at split alpha, with calcHI's overlap
+// convention for r < 2 (the far form at alpha plus the overlap correction at
+// its own split parameter alpha_ref).
+__device__ __forceinline__ void pair_terms(double alpha, double alpha_ref, double rr, double& t1,
+                                           double& t2) {
+  if (rr < 4.0) {
+    double t[2];
+    overlap_terms(alpha, alpha_ref, rr, t);
+    t1 = t[0];
+    t2 = t[1];
+  } else {
+    real_kernel(alpha, rr, false, t1, t2);
+  }
+}
+
 // out_c(i) = sum_g W_i(g) grid_c(g) + self * v_c(i) - S_off v(i)
 //            + sum_j T_ij v_j (row list)
 // One warp per bead: lanes share the stencil points and the pair row, then a
@@ -222,8 +271,9 @@ template <int P, typename R>
 __global__ void __launch_bounds__(256) k_pme_gather(
     const int* __restrict__ base, const double* __restrict__ w, int N, int K,
     const R* __restrict__ grid, double self, const double* __restrict__ soff, VecIn v,
-    const int* __restrict__ rcnt, const int* __restrict__ rrows, const R* __restrict__ rT,
-    int rcap, double* o0, double* o1, double* o2, int ostride) {
+    const int* __restrict__ rcnt, const int* __restrict__ rrows,
+    const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
+    double* o0, double* o1, double* o2, int ostride) {
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
@@ -247,18 +297,35 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     u1 += wt * (double)grid[K3 + g];
     u2 += wt * (double)grid[2 * K3 + g];
   }
+  // real-space pairs: the tensor t1 I + t2 d d^T/r^2 of the minimum-image
+  // displacement d; t1 and t2/r^2 are stored per pair (8 or 16 bytes), d is
+  // recomputed from the frozen lab-frame positions (L2-resident)
   int n = rcnt[i];
   const int* row = rrows + (size_t)i * rcap;
-  const R* T = rT + (size_t)i * rcap * 6;
+  // the cell is (b1, b2) in the xy plane and L e_z: a 2 x 2 block and L
+  double4 pi = pos[i];
+  const double h00 = cell.H[0], h01 = cell.H[1], h10 = cell.H[3], h11 = cell.H[4];
+  const double g00 = cell.Hi[0], g01 = cell.Hi[1], g10 = cell.Hi[3], g11 = cell.Hi[4];
+  const double Lz = cell.H[8], iLz = cell.Hi[8];
   for (int k = lane; k < n; k += 32) {
     int j = row[k];
+    double4 pj = pos[j];
+    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
+    s0 -= rint(s0);
+    s1 -= rint(s1);
+    s2 -= rint(s2);
+    dx = h00 * s0 + h01 * s1;
+    dy = h10 * s0 + h11 * s1;
+    dz = Lz * s2;
+    const R* tk = tt + 2 * ((size_t)i * rcap + k);
+    double t1 = tk[0], t2r = tk[1];  // t1 and t2 / r^2 of the pair
     double x0 = v.p[0][(size_t)j * v.stride], x1 = v.p[1][(size_t)j * v.stride];
     double x2 = v.p[2][(size_t)j * v.stride];
-    const R* t = T + 6 * k;
-    double t0 = t[0], t1 = t[1], t2 = t[2], t3 = t[3], t4 = t[4], t5 = t[5];
-    u0 += t0 * x0 + t1 * x1 + t2 * x2;
-    u1 += t1 * x0 + t3 * x1 + t4 * x2;
-    u2 += t2 * x0 + t4 * x1 + t5 * x2;
+    double q = t2r * (dx * x0 + dy * x1 + dz * x2);
+    u0 += t1 * x0 + q * dx;
+    u1 += t1 * x1 + q * dy;
+    u2 += t1 * x2 + q * dz;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -274,28 +341,6 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     o1[(size_t)i * ostride] = u1 + self * vi1 - sxy * vi0 - syz * vi2;
     o2[(size_t)i * ostride] = u2 + self * vi2 - sxz * vi0 - syz * vi1;
   }
-}
-
-// Real-space Beenakker kernel t1 I + t2 r r^T/r^2 (shear/src/main26.c:
-// 1727-1741) at split parameter alpha; with far the r > 2 form at any r.
-__device__ __forceinline__ void real_kernel(double alpha, double rr, bool far, double& t1,
-                                            double& t2) {
-  double r = sqrt(rr), a = alpha, a2 = a * a, a3 = a2 * a, a5 = a3 * a2, a7 = a5 * a2;
-  double C1, C2, C3, C4;
-  if (far || r > 2.0) {
-    C1 = 0.75 / r + 0.5 / (r * rr);
-    C2 = 4.0 * a7 * rr * rr + 3.0 * a3 * rr - 20.0 * a5 * rr - 4.5 * a + 14.0 * a3 + a / rr;
-    C3 = 0.75 / r - 1.5 / (r * rr);
-    C4 = -4.0 * a7 * rr * rr - 3.0 * a3 * rr + 16.0 * a5 * rr + 1.5 * a - 2.0 * a3 - 3.0 * a / rr;
-  } else {
-    C1 = 1.0 - 0.28125 * r;
-    C2 = 64.0 * a7 + 12.0 * a3 - 80.0 * a5 - 4.5 * a + 14.0 * a3 + 0.25 * a;
-    C3 = 0.09375 * r;
-    C4 = -64.0 * a7 - 12.0 * a3 + 64.0 * a5 + 1.5 * a - 2.0 * a3 - 0.75 * a;
-  }
-  double ec = erfc(a * r), ex = exp(-a2 * rr) / sqrt(M_PI);
-  t1 = C1 * ec + C2 * ex;
-  t2 = C3 * ec + C4 * ex;
 }
 
 // Cells of the real-space list (fractional, width >= rc).
@@ -358,18 +403,18 @@ __global__ void k_rl_fill(const int* __restrict__ cell_of, const int* __restrict
   beads[cell_start[c] + atomicAdd(&cursor[c], 1)] = i;
 }
 
-// Pairs within rc (lattice minimum image) and their 3x3 real-space tensors.
+// Pairs within rc (lattice minimum image): rows of bead indices and, per
+// pair, t1 and t2 / r^2 of the real-space tensor.
 template <typename R>
-__global__ void k_rl_rows(Cell cell, RGeom g, const double* __restrict__ rx,
-                          const double* __restrict__ ry, const double* __restrict__ rz,
-                          double cr, double sr, int N, const int* __restrict__ cell_start,
-                          const int* __restrict__ beads, double rc2, double alpha,
-                          double alpha_ref, int rcap, int* cnt, int* rows, R* T, int* err) {
+__global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, int N,
+                          const int* __restrict__ cell_start, const int* __restrict__ beads,
+                          double rc2, double alpha, double alpha_ref, int rcap, int* cnt,
+                          int* rows, R* tt, int* err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  double xi = rx[i] * cr - ry[i] * sr, yi = rx[i] * sr + ry[i] * cr, zi = rz[i];
+  double4 p = pos[i];
   int cd[3];
-  rcell(cell, g, xi, yi, zi, cd);
+  rcell(cell, g, p.x, p.y, p.z, cd);
   int lo[3], hi[3];
   for (int d = 0; d < 3; d++) {
     lo[d] = g.n[d] >= 3 ? -1 : 0;
@@ -387,8 +432,8 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double* __restrict__ rx,
         for (int q = cell_start[cc]; q < cell_start[cc + 1]; q++) {
           int j = beads[q];
           if (j == i) continue;
-          double dx = (rx[j] * cr - ry[j] * sr) - xi, dy = (rx[j] * sr + ry[j] * cr) - yi;
-          double dz = rz[j] - zi, s[3];
+          double4 pj = pos[j];
+          double dx = pj.x - p.x, dy = pj.y - p.y, dz = pj.z - p.z, s[3];
           frac_of(cell, dx, dy, dz, s);
           for (int d = 0; d < 3; d++) s[d] -= rint(s[d]);
           dx = cell.H[0] * s[0] + cell.H[1] * s[1] + cell.H[2] * s[2];
@@ -401,32 +446,16 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double* __restrict__ rx,
             continue;
           }
           double t1, t2;
-          real_kernel(alpha, rr, false, t1, t2);
-          if (rr < 4.0) {
-            // overlap: far form at alpha plus calcHI's overlap correction at
-            // its own split parameter
-            double f1, f2, o1, o2, g1, g2;
-            real_kernel(alpha, rr, true, f1, f2);
-            real_kernel(alpha_ref, rr, false, o1, o2);
-            real_kernel(alpha_ref, rr, true, g1, g2);
-            t1 = f1 + (o1 - g1);
-            t2 = f2 + (o2 - g2);
-          }
-          R* o = T + ((size_t)i * rcap + n) * 6;
-          o[0] = (R)(t1 + t2 * dx * dx / rr);
-          o[1] = (R)(t2 * dx * dy / rr);
-          o[2] = (R)(t2 * dx * dz / rr);
-          o[3] = (R)(t1 + t2 * dy * dy / rr);
-          o[4] = (R)(t2 * dy * dz / rr);
-          o[5] = (R)(t1 + t2 * dz * dz / rr);
+          pair_terms(alpha, alpha_ref, rr, t1, t2);
           rows[(size_t)i * rcap + n] = j;
+          tt[2 * ((size_t)i * rcap + n)] = (R)t1;
+          tt[2 * ((size_t)i * rcap + n) + 1] = (R)(t2 / rr);
           n++;
         }
       }
   cnt[i] = n;
   if (over) atomicOr(err, ERRB_NBR_OVERFLOW);
 }
-
 
 namespace bd {
 
@@ -447,7 +476,8 @@ int pme_alloc(bd_ctx* c) {
   c->rl_cap = c->p.pme_max_pairs > 0 ? c->p.pme_max_pairs : 512;
   CU(cudaMalloc(&c->rl_cnt, 4 * (size_t)N));
   CU(cudaMalloc(&c->rl_rows, 4 * (size_t)N * c->rl_cap));
-  CU(cudaMalloc(&c->rl_T, es * 6 * (size_t)N * c->rl_cap));
+  CU(cudaMalloc(&c->rl_pos, 32 * (size_t)N));
+  CU(cudaMalloc(&c->rl_tt, 2 * es * (size_t)N * c->rl_cap));
   c->rl_ncell_cap = 4096;
   CU(cudaMalloc(&c->rl_cell_of, 4 * (size_t)N));
   CU(cudaMalloc(&c->rl_beads, 4 * (size_t)N));
@@ -456,7 +486,7 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_cursor, 4 * (size_t)c->rl_ncell_cap));
   CU(cudaMemsetAsync(c->rl_cell_count, 0, 4 * (size_t)c->rl_ncell_cap, c->stream));
   c->bytes += es * (3 * K3 + 6 * Ks + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
-              24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 6 * es) +
+              24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 2 * es) + 32 * (size_t)N +
               8 * (size_t)N + 12 * (size_t)c->rl_ncell_cap;
   int n[3] = {K, K, K};
   cufftHandle f, b;
@@ -481,7 +511,7 @@ void pme_free(bd_ctx* c) {
   if (c->pme_plan_f) cufftDestroy((cufftHandle)c->pme_plan_f);
   if (c->pme_plan_b) cufftDestroy((cufftHandle)c->pme_plan_b);
   void* ptrs[] = {c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
-                  c->rl_cnt, c->rl_rows, c->rl_T, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
+                  c->rl_cnt, c->rl_rows, c->rl_pos, c->rl_tt, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
                   c->rl_cell_start, c->rl_cursor};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -508,7 +538,8 @@ int pme_prepare(bd_ctx* c, const Lat& l) {
   double alpha_ref = 4.0 / rce;
   c->launches += 3;
   k_pme_weights<<<nblk(N, 256), 256, 0, c->stream>>>(cell, c->rx, c->ry, c->rz, cr, sr, N, K,
-                                                     c->pme_p, c->pme_base, c->pme_w, c->err);
+                                                     c->pme_p, c->pme_base, c->pme_w,
+                                                     (double4*)c->rl_pos, c->err);
   if (c->pme_f32)
     k_pme_influence<float><<<c->pme_nblk, 256, 0, c->stream>>>(
         cell, K, alpha, c->pme_bsq, (float*)c->pme_infl, c->pme_soff + 3);
@@ -545,15 +576,20 @@ int pme_prepare(bd_ctx* c, const Lat& l) {
   k_rl_scan<<<1, 1024, 0, c->stream>>>(ncell, c->rl_cell_count, c->rl_cell_start, c->rl_cursor);
   k_rl_fill<<<nblk(N, 256), 256, 0, c->stream>>>(c->rl_cell_of, c->rl_cell_start, c->rl_cursor,
                                                  c->rl_beads, N);
-#define PME_ROWS(R_)                                                                        \
-  k_rl_rows<R_><<<nblk(N, 128), 128, 0, c->stream>>>(                                      \
-      cell, g, c->rx, c->ry, c->rz, cr, sr, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha, \
-      alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (R_*)c->rl_T, c->err)
-  if (c->pme_f32)
-    PME_ROWS(float);
+if (c->pme_f32)
+    k_rl_rows<float><<<nblk(N, 128), 128, 0, c->stream>>>(
+        cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
+        alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (float*)c->rl_tt, c->err);
   else
-    PME_ROWS(double);
-#undef PME_ROWS
+    k_rl_rows<double><<<nblk(N, 128), 128, 0, c->stream>>>(
+        cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
+        alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (double*)c->rl_tt, c->err);
+  // the cell and calcHI's split parameter of this configuration, for the
+  // products until the next preparation
+  memcpy(c->pme_cellbuf, cell.H, sizeof(cell.H));
+  memcpy(c->pme_cellbuf + 9, cell.Hi, sizeof(cell.Hi));
+  c->pme_cellbuf[18] = cell.V;
+  c->pme_alpha_ref = alpha_ref;
   double a = alpha;
   c->pme_self = 1.0 - 6.0 / sqrt(M_PI) * a + 40.0 / (3.0 * sqrt(M_PI)) * a * a * a;
   c->Dtr[0] = c->Dtr[1] = c->Dtr[2] = c->pme_self;
@@ -593,11 +629,16 @@ static int pme_apply_t(bd_ctx* c, const VecIn& v, double* o0, double* o1, double
   else
     CF(cufftExecZ2D((cufftHandle)c->pme_plan_b, (cufftDoubleComplex*)spec,
                     (cufftDoubleReal*)grid));
-#define PME_GATHER(P_)                                                                        \
-  k_pme_gather<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, grid,           \
-                                                  c->pme_self, c->pme_soff, v, c->rl_cnt,       \
-                                                  c->rl_rows, (const R*)c->rl_T, c->rl_cap, o0, \
-                                                  o1, o2, ostride)
+  Cell cell;
+  memcpy(cell.H, c->pme_cellbuf, sizeof(cell.H));
+  memcpy(cell.Hi, c->pme_cellbuf + 9, sizeof(cell.Hi));
+  cell.V = c->pme_cellbuf[18];
+#define PME_GATHER(P_)                                                                         \
+  k_pme_gather<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, grid,            \
+                                                  c->pme_self, c->pme_soff, v, c->rl_cnt,        \
+                                                  c->rl_rows, (const double4*)c->rl_pos, cell,   \
+                                                  (const R*)c->rl_tt, c->rl_cap, o0, o1, o2,     \
+                                                  ostride)
   switch (p) {
     case 4: PME_GATHER(4); break;
     case 6: PME_GATHER(6); break;

@@ -120,37 +120,27 @@ __global__ void __launch_bounds__(128) k_seg_blocks(Lat l, const double* __restr
 }
 
 // y = op(B_b) x for every block; x, y in the Lanczos layout (component-major,
-// 3 x NTp).  One thread per output entry (block b, row i of op(B_b)); the
-// block's entries are read once per CTA from L1/L2.  trans = 1 reads a
-// column (coalesced across the threads of a block), trans = 0 a row.
-__global__ void __launch_bounds__(128) k_block_apply(const double* __restrict__ Bm, int S,
+// 3 x NTp).  One warp per output entry (block b, row i of op(B_b)): the lanes
+// split the 3S products of the row (trans = 0) or column (trans = 1) and a
+// butterfly adds them, which keeps enough loads in flight for blocks of a few
+// dozen rows.
+__global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ Bm, int S,
                                                      int nblk, int trans,
                                                      const double* __restrict__ x,
                                                      double* __restrict__ y, int NTp) {
-  int n = 3 * S;
-  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int n = 3 * S, lane = threadIdx.x & 31;
+  size_t e = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (e >= (size_t)nblk * n) return;
   int b = (int)(e / n), i = (int)(e % n);
   const double* Bb = Bm + (size_t)b * n * n;
-  const double* xb0 = x + (size_t)b * S;
-  double s0 = 0, s1 = 0, s2 = 0;
-  if (trans) {
-#pragma unroll 4
-    for (int a = 0; a < S; a++) {
-      s0 += Bb[(size_t)(3 * a) * n + i] * xb0[a];
-      s1 += Bb[(size_t)(3 * a + 1) * n + i] * xb0[NTp + a];
-      s2 += Bb[(size_t)(3 * a + 2) * n + i] * xb0[2 * (size_t)NTp + a];
-    }
-  } else {
-    const double* row = Bb + (size_t)i * n;
-#pragma unroll 4
-    for (int a = 0; a < S; a++) {
-      s0 += row[3 * a] * xb0[a];
-      s1 += row[3 * a + 1] * xb0[NTp + a];
-      s2 += row[3 * a + 2] * xb0[2 * (size_t)NTp + a];
-    }
+  const double* xb = x + (size_t)b * S;
+  double s = 0;
+  for (int k = lane; k < n; k += 32) {
+    double m = trans ? Bb[(size_t)k * n + i] : Bb[(size_t)i * n + k];
+    s += m * xb[(size_t)(k % 3) * NTp + k / 3];
   }
-  y[(size_t)(i % 3) * NTp + (size_t)b * S + i / 3] = (s0 + s1) + s2;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) y[(size_t)(i % 3) * NTp + (size_t)b * S + i / 3] = s;
 }
 
 // 3 x 3 bead blocks: one thread per bead.
@@ -305,8 +295,9 @@ int precond_apply(bd_ctx* c, int which, const double* x, double* y) {
   if (S == 1) {
     k_bead_apply<<<(c->N + 127) / 128, 128, 0, c->stream>>>(Bm, c->N, trans, x, y, NTp);
   } else {
-    int nb = c->N / S;
-    k_block_apply<<<(nb * 3 * S + 127) / 128, 128, 0, c->stream>>>(Bm, S, nb, trans, x, y, NTp);
+    long long nw = (long long)(c->N / S) * 3 * S;  // one warp per output entry
+    k_block_apply<<<(unsigned)((nw * 32 + 255) / 256), 256, 0, c->stream>>>(Bm, S, c->N / S,
+                                                                             trans, x, y, NTp);
   }
   return BD_OK;
 }
