@@ -355,20 +355,25 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def measure(w, path, K, W, rank, dist, e2e_steps):
+def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1):
     """Times K steps of one path after W warm-up steps; returns a dict."""
     import torch
     N = w["Nb"] * w["Nc"]
     pp = PATHS[path]
-    c = build_context(w, 1000 + rank, path)
+    nb = noise_block if pp["mobility"] == "pme" else 1
+    c = build_context(w, 1000 + rank, path, noise_block=nb)
     step = c.step_lanczos if pp["step"] == "lanczos" else c.step_reference
     step(0, W, True)
+    # noise blocks solved during the warm-up are dropped, so the timed steps
+    # pay for every block they use (and the e2e loop below likewise)
+    c.noise_block_release()
     c.sync()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     lan0 = c.lanczos_stats()
     pre0 = c.precond_stats()
+    blk0 = c.noise_block_stats()
     c.profile(True)
     n0 = c.launches()
     dev = int(os.environ.get("LOCAL_RANK", 0))
@@ -377,10 +382,11 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
         c.sync()
     launches = c.launches() - n0
     prof = {k: c.profile_read(getattr(c, "PROF_" + k)) for k in
-            ("STEP", "MATVEC", "HI_BUILD", "HOP", "FORCES")}
+            ("STEP", "MATVEC", "HI_BUILD", "HOP", "FORCES", "BLOCK")}
     c.profile(False)
     lan1 = c.lanczos_stats()
     pre1 = c.precond_stats()
+    blk1 = c.noise_block_stats()
     step_ms = prof["STEP"][0]
     t_max = step_ms
     if dist:
@@ -393,6 +399,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
     hb = [torch.empty(N, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
     for a, b in zip(hb, c.positions()):
         a[:] = b
+    c.noise_block_release()
     c.sync()
     t0 = time.perf_counter()
     for t in range(W + K, W + K + Ke):
@@ -419,11 +426,25 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
     avg_ms = mv_ms / max(mv_n, 1)
     iters = lan1["iterations"] - lan0["iterations"]
     calls = lan1["calls"] - lan0["calls"]
+    # noise blocks: the dominant kernel is the product of a whole block (its
+    # right-hand sides share the launches); its algorithmic bytes are those of
+    # one product times the mean right-hand sides per block iteration
+    bk = {k: blk1[k] - blk0[k] for k in blk1}
+    bl_ms, bl_n = prof["BLOCK"]
+    block = None
+    if bk["iterations"] > 0 and bl_n > 0:
+        rhs = bk["rhs_iterations"] / bk["iterations"]
+        b_avg = bl_ms / bl_n
+        block = dict(noise_block=nb, blocks=bk["blocks"], block_iterations=bk["iterations"],
+                     rhs_per_iteration=rhs, block_iterations_per_step=bk["iterations"] / K,
+                     product_ms=bl_ms, products=bl_n, avg_product_ms=b_avg,
+                     alg_bytes=alg_bytes * rhs,
+                     achieved_gbs=alg_bytes * rhs / (b_avg / 1e3) / 1e9)
     out = dict(path=path, t_max_ms=t_max, launches=launches, clocks=clk.summary(),
                e2e_s=e2e_s, e2e_steps=Ke, matvec_ms=mv_ms, matvec_launches=mv_n,
                matvec_avg_ms=avg_ms, alg_bytes=alg_bytes,
                achieved_gbs=alg_bytes / (avg_ms / 1e3) / 1e9 if mv_n else None,
-               lanczos_iters_per_step=(iters / calls) if calls else None,
+               lanczos_iters_per_step=(iters / calls) if calls else None, block=block,
                lanczos_maxed=lan1["maxed"] - lan0["maxed"],
                precond_fallbacks=pre1["fallbacks"] - pre0["fallbacks"],
                precond_calls=pre1["calls"] - pre0["calls"],
@@ -435,7 +456,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps):
     return out
 
 
-def measure_batch(path, K, W, e2e_steps):
+def measure_batch(path, K, W, e2e_steps, noise_block=1):
     """Times K steps of the c2 ensemble advanced as one batch (bd_batch_*)
     after W warm-up steps: device time bracketed by full synchronisation and
     CUDA events; per-replica grids from the autotuner."""
@@ -449,9 +470,13 @@ def measure_batch(path, K, W, e2e_steps):
         if pp["mobility"] == "pme":
             extra["pme_grid"] = B.autotune_pme_grid(w["L"], pp["precision"])
         grids.append(extra.get("pme_grid", B.pme_default_grid(w["L"])))
+        if pp["mobility"] == "pme":
+            extra["noise_block"] = noise_block
         ctxs.append(build_context(w, 5000 + k, path, **extra))
     batch = B.Batch(ctxs)
     batch.step_lanczos(0, W, True)
+    for c in ctxs:
+        c.noise_block_release()
     torch.cuda.synchronize()
     lan0 = [c.lanczos_stats() for c in ctxs]
     for c in ctxs:
@@ -486,6 +511,7 @@ def measure_batch(path, K, W, e2e_steps):
     for h, c in zip(hb, ctxs):
         for a, b in zip(h, c.positions()):
             a[:] = b
+        c.noise_block_release()
     Ke = max(1, min(K, e2e_steps))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -509,7 +535,7 @@ def measure_batch(path, K, W, e2e_steps):
 
 def run_batch(args, world):
     K, W = args.steps, args.warmup
-    m = measure_batch(args.path, K, W, args.e2e_steps)
+    m = measure_batch(args.path, K, W, args.e2e_steps, args.noise_block)
     peak, kind = peaks()
     value = world * m["nbeads"] * K / (m["t_ms"] / 1e3)
     line = {"metric": METRIC, "value": value, "unit": "bead-steps/s", "n_gpus": world,
@@ -543,7 +569,7 @@ def run_ours(args, rank, world, dist):
     K, W = args.steps, args.warmup
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps)
+    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps, args.noise_block)
     value = world * N * K / (main["t_max_ms"] / 1e3)
     peak, kind = peaks()
     pme = PATHS[args.path]["mobility"] == "pme"
@@ -554,6 +580,17 @@ def run_ours(args, rank, world, dist):
             "unit": "GB/s", "frac": (main["achieved_gbs"] or 0) / peak, "traffic": None,
             "alg_bytes_per_launch": main["alg_bytes"], "avg_launch_ms": main["matvec_avg_ms"],
             "launches": main["matvec_launches"]}
+    if main["block"]:
+        b = main["block"]
+        roof.update({"kernel": "particle-mesh product of a noise block (%.1f right-hand sides "
+                               "per launch: spread, R2C, influence, C2R, gather)"
+                               % b["rhs_per_iteration"],
+                     "achieved": b["achieved_gbs"], "frac": b["achieved_gbs"] / peak,
+                     "alg_bytes_per_launch": b["alg_bytes"], "avg_launch_ms": b["avg_product_ms"],
+                     "launches": b["products"],
+                     "single_product": {"achieved": main["achieved_gbs"],
+                                        "avg_launch_ms": main["matvec_avg_ms"],
+                                        "launches": main["matvec_launches"]}})
     e2e = {"value": world * N * main["e2e_steps"] / main["e2e_s"], "unit": "bead-steps/s",
            "h2d_bytes_per_step": 3 * 8 * N, "d2h_bytes_per_step": 3 * 8 * N,
            "steps": main["e2e_steps"]}
@@ -566,7 +603,10 @@ def run_ours(args, rank, world, dist):
                        "mobility": ("Ewald-summed RPY by smooth PME, grid %d^3, order 8, cutoff 10"
                                     % __import__("bd_b200").pme_default_grid(w["L"]) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
-                       "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation",
+                       "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation" +
+                                (", noise blocks of %d steps" % main["block"]["noise_block"]
+                                 if main["block"] else ""),
+                       "noise_block": main["block"],
                        "electrostatics": ("Ewald Coulomb, chains alternately -1 / +1 on half "
                                           "their beads" if PATHS[args.path].get("physics") ==
                                           "north" else "Debye-Hueckel, unsigned charges "
@@ -610,6 +650,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--path", choices=sorted(PATHS), default="pme32-learned")
+    ap.add_argument("--noise-block", type=int, default=16,
+                    help="steps whose Brownian displacements one multi-vector Lanczos run "
+                         "solves (particle-mesh paths; 1 = one solve per step)")
     ap.add_argument("--compare", type=int, default=1,
                     help="also time the plain FP64 Krylov path (reported as plain_fp64)")
     args = ap.parse_args()

@@ -71,6 +71,8 @@ typedef enum {
   BD_PRECOND_BLOCKS = 3
 } bd_precond_kind;
 #define BD_PRECOND_MAX_SEGMENT 25
+/* Largest noise block of bd_step_lanczos (bd_params.noise_block). */
+#define BD_MAX_NOISE_BLOCK 64
 /* Storage of the packed mobility tiles used by the products: FP64, or FP32
  * with FP64 accumulation. */
 typedef enum { BD_PREC_FP64 = 0, BD_PREC_FP32 = 1 } bd_precision;
@@ -136,6 +138,13 @@ typedef struct {
   int hop;                   /* bd_hop_kind */
   double hop_radius;         /* parallel sweep: minimum distance between cells that
                                 move at once; 0 -> 3 lambda_d */
+  /* bd_step_lanczos with BD_MOB_PME: number of steps whose Brownian
+   * displacements sqrt(M) z_t are solved together by one multi-vector Lanczos
+   * run (0 or 1 -> one per step, at most BD_MAX_NOISE_BLOCK).  The mobility
+   * is frozen between rebuilds and z_t does not depend on the state, so the
+   * block gives every step the displacement the per-step solve gives (to the
+   * Lanczos tolerance), with the same draws in the same order. */
+  int noise_block;
 } bd_params;
 
 typedef struct bd_ctx bd_ctx;
@@ -155,6 +164,9 @@ typedef struct {
 int bd_create(const bd_params *p, bd_ctx **out);
 int bd_destroy(bd_ctx *ctx);
 const char *bd_status_string(int status);
+/* Source line, message and code of the last CUDA or cuFFT failure reported
+ * as BD_ERR_CUDA on the calling thread ("" if none). */
+const char *bd_last_error_detail(void);
 int bd_sync(bd_ctx *ctx);
 /* Device bytes currently held by the context. */
 size_t bd_device_bytes(const bd_ctx *ctx);
@@ -232,6 +244,7 @@ enum {
   BD_PROF_HOP = 2,      /* charge-hop sweep kernel */
   BD_PROF_FORCES = 3,   /* bond + excluded-volume + electrostatic kernels */
   BD_PROF_STEP = 4,     /* one whole bd_step_reference call */
+  BD_PROF_BLOCK = 5,    /* particle-mesh product of a noise block (all its right-hand sides) */
   BD_PROF_SLOTS = 8
 };
 /* Replay each Lanczos iteration (product and orthogonalisation) as a CUDA
@@ -256,6 +269,14 @@ int bd_lanczos_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
 /* calls, total Krylov iterations, calls that hit lanczos_max, negative Ritz
  * values clamped (a hybrid mobility need not be positive definite) */
 int bd_lanczos_stats(bd_ctx *ctx, long *out4);
+/* Noise blocks of bd_step_lanczos: block solves run, block iterations
+ * launched (one iteration = one product of every right-hand side) and the
+ * sum over those iterations of their right-hand sides. */
+int bd_noise_block_stats(bd_ctx *ctx, long *out3);
+/* Drops the noise block solved ahead (if any): the generator is wound back to
+ * the draws the per-step order has made, and the next bd_step_lanczos solves
+ * a new block from its own step on. */
+int bd_noise_block_release(bd_ctx *ctx);
 /* No counterpart in the reference.  out = M v like bd_mobility_apply, for
  * callers that must not allocate device memory where they call it (a loop
  * running while another framework's pool owns the device, a fixed memory
@@ -274,7 +295,12 @@ int bd_mobility_apply_noalloc(bd_ctx *ctx, const double *v, double *out);
 /* One Brownian-dynamics step with the Krylov displacement
  * dr = dt M F + sqrt(2 dt) M^(1/2) z + dt u(r): the reference's step order
  * (lattice, PBC, neighbour check, forces, mobility rebuild every srpy steps,
- * charge hop every MStep steps) with Philox z; repeated nsteps times. */
+ * charge hop every MStep steps) with z from bd_get_noise; repeated nsteps
+ * times.  With noise_block B > 1 (particle-mesh mobility) the displacements
+ * M^(1/2) z_t of up to B consecutive steps are solved by one multi-vector
+ * Lanczos run when the first of them starts; a block never spans a mobility
+ * rebuild, the end of the call, or (ran1 noise with the sequential hop, which
+ * draw from one generator) a charge-hop sweep. */
 int bd_step_lanczos(bd_ctx *ctx, unsigned long t0, int nsteps, int with_hop);
 
 /* One reference-mode hydrodynamic step (the body of the step loop,

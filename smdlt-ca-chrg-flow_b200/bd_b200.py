@@ -53,6 +53,8 @@ class BDError(RuntimeError):
     def __init__(self, status: int, where: str):
         self.status = status
         msg = _lib().bd_status_string(status).decode() if _LIB else str(status)
+        if _LIB and status == 2:  # BD_ERR_CUDA: the failing call
+            msg += " at " + _lib().bd_last_error_detail().decode()
         super().__init__(f"{where}: {msg} (status {status})")
 
 
@@ -71,7 +73,7 @@ class Params(C.Structure):
         ("lanczos_max", C.c_int), ("pme_grid", C.c_int), ("pme_order", C.c_int),
         ("pme_rc", C.c_double), ("pme_alpha", C.c_double), ("pme_max_pairs", C.c_int),
         ("coulomb", C.c_int), ("coulomb_beta", C.c_double), ("coulomb_rc", C.c_double),
-        ("hop", C.c_int), ("hop_radius", C.c_double),
+        ("hop", C.c_int), ("hop_radius", C.c_double), ("noise_block", C.c_int),
     ]
 
 
@@ -97,6 +99,8 @@ def _lib() -> C.CDLL:
         vp = C.c_void_p
         L.bd_status_string.restype = C.c_char_p
         L.bd_status_string.argtypes = [C.c_int]
+        L.bd_last_error_detail.restype = C.c_char_p
+        L.bd_last_error_detail.argtypes = []
         L.bd_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
         L.bd_destroy.argtypes = [vp]
         L.bd_sync.argtypes = [vp]
@@ -133,6 +137,8 @@ def _lib() -> C.CDLL:
         L.bd_mobility_apply.argtypes = [vp, _dp, _dp]
         L.bd_lanczos_sqrt.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
         L.bd_lanczos_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        L.bd_noise_block_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        L.bd_noise_block_release.argtypes = [vp]
         L.bd_step_lanczos.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
         L.bd_profile_enable.argtypes = [vp, C.c_int]
         L.bd_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
@@ -321,7 +327,7 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
                 noise="ran1", philox_seed=20261203, mobility="hybrid", precision="fp64",
                 lanczos_tol=1e-6, lanczos_max=0, pme_grid=0, pme_order=0, pme_rc=0.0,
                 pme_alpha=0.0, pme_max_pairs=0, coulomb="dh", coulomb_beta=0.0,
-                coulomb_rc=0.0, hop="sequential", hop_radius=0.0) -> Params:
+                coulomb_rc=0.0, hop="sequential", hop_radius=0.0, noise_block=1) -> Params:
     p = Params()
     p.flow, p.Nb, p.Nc, p.L, p.edot, p.dt = int(flow), Nb, Nc, L, edot, dt
     p.box_volume = box_volume
@@ -344,6 +350,7 @@ def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3
     p.coulomb_beta, p.coulomb_rc = coulomb_beta, coulomb_rc
     p.hop = {"sequential": 0, "parallel": 1}[hop]
     p.hop_radius = hop_radius
+    p.noise_block = noise_block
     return p
 
 
@@ -500,6 +507,18 @@ class Context:
         self._call("bd_lanczos_stats", o)
         return dict(calls=int(o[0]), iterations=int(o[1]), maxed=int(o[2]), negative=int(o[3]))
 
+    def noise_block_stats(self):
+        """Noise blocks of step_lanczos: block solves, block iterations run and
+        the sum over those iterations of their right-hand sides."""
+        o = np.zeros(3, np.int64)
+        self._call("bd_noise_block_stats", o)
+        return dict(blocks=int(o[0]), iterations=int(o[1]), rhs_iterations=int(o[2]))
+
+    def noise_block_release(self):
+        """Drops the noise block solved ahead; the generator rewinds to the
+        per-step order."""
+        self._call("bd_noise_block_release")
+
     def step_lanczos(self, t0, nsteps, with_hop=True):
         self._call("bd_step_lanczos", int(t0), int(nsteps), int(bool(with_hop)))
 
@@ -509,7 +528,7 @@ class Context:
     def sync(self):
         self._call("bd_sync")
 
-    PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP = 0, 1, 2, 3, 4
+    PROF_MATVEC, PROF_HI_BUILD, PROF_HOP, PROF_FORCES, PROF_STEP, PROF_BLOCK = 0, 1, 2, 3, 4, 5
 
     def chain_props(self):
         Nc = self.p.Nc

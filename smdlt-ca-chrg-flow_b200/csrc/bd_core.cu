@@ -12,11 +12,7 @@
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 namespace bd {
 
@@ -29,10 +25,33 @@ int set_error_from_bits(int bits) {
   return BD_OK;
 }
 
-int launch_ok(bd_ctx* c) {
-  (void)c;
+static thread_local char g_detail[320];
+
+int cuda_fail(int code, const char* msg, const char* file, int line) {
+  const char* base = file;
+  for (const char* q = file; *q; q++)
+    if (*q == '/') base = q + 1;
+  snprintf(g_detail, sizeof(g_detail), "%s:%d: %s (code %d)", base, line, msg ? msg : "", code);
+  return BD_ERR_CUDA;
+}
+
+// BD_DEBUG_SYNC=1 in the environment: every launch check also waits for the
+// context's stream, so an asynchronous fault is reported at the launches
+// that caused it (slow; for diagnosis only).
+static bool debug_sync() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("BD_DEBUG_SYNC");
+    on = (e && e[0] == '1') ? 1 : 0;
+  }
+  return on == 1;
+}
+
+int launch_ok_at(bd_ctx* c, const char* file, int line) {
   cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? BD_OK : BD_ERR_CUDA;
+  if (e == cudaSuccess && c && !c->capturing && debug_sync()) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) return BD_OK;
+  return cuda_fail((int)e, cudaGetErrorString(e), file, line);
 }
 
 int check(bd_ctx* c) {
@@ -505,6 +524,8 @@ static int dalloc(bd_ctx* c, void** p, size_t bytes) {
 
 extern "C" {
 
+const char* bd_last_error_detail(void) { return g_detail; }
+
 const char* bd_status_string(int s) {
   switch (s) {
     case BD_OK: return "ok";
@@ -568,8 +589,10 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   c->strain_ss = p->strain_ss > 0 ? p->strain_ss : 10.0;
   c->strain_interval = c->strain_ss / c->sbins;
   c->maxnb = p->max_neighbors > 0 ? p->max_neighbors : 256;
+  // noise blocks need the particle-mesh product (any number of right-hand sides)
+  c->nbk = (p->mobility == BD_MOB_PME && p->noise_block > 1) ? p->noise_block : 1;
   if (p->lanczos_max > kMaxKrylov || p->mobility < 0 || p->mobility > 2 || p->precision < 0 ||
-      p->precision > 1) {
+      p->precision > 1 || p->noise_block < 0 || p->noise_block > BD_MAX_NOISE_BLOCK) {
     bd_destroy(c);
     return BD_ERR_ARG;
   }
@@ -719,6 +742,7 @@ int bd_destroy(bd_ctx* c) {
   if (c->Lvcur) cudaFree(c->Lvcur);
   if (c->Ljd) cudaFree(c->Ljd);
   lanczos_graphs_reset(c);
+  lanczos_blocks_free(c);
   prof_clear(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -866,6 +890,7 @@ int bd_download_charges(bd_ctx* c, int* track, int* old, int* flags) {
 
 int bd_set_rng(bd_ctx* c, const bd_ran1_state* s) {
   if (!c || !s) return BD_ERR_ARG;
+  noise_blocks_release(c);
   Ran1 g;
   g.idum = s->idum;
   g.idum2 = s->idum2;
@@ -880,6 +905,7 @@ int bd_set_rng(bd_ctx* c, const bd_ran1_state* s) {
 
 int bd_get_rng(bd_ctx* c, bd_ran1_state* s) {
   if (!c || !s) return BD_ERR_ARG;
+  noise_blocks_release(c);
   Ran1 g;
   CU(cudaMemcpyAsync(&g, c->rng, sizeof(g), cudaMemcpyDeviceToHost, c->stream));
   int st = check(c);
@@ -1024,15 +1050,8 @@ int bd_coulomb_force(bd_ctx* c) {
 
 int bd_get_noise(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
-  c->launches++;
-  if (c->p.noise == BD_NOISE_PHILOX) {
-    int n = 3 * c->N, pairs = (n + 1) / 2;
-    k_noise_philox<<<nblk(pairs, 256), 256, 0, c->stream>>>(c->R, n, c->p.philox_seed,
-                                                            c->noise_draws++);
-  } else {
-    k_gasdev_seq<<<1, 32, 0, c->stream>>>(c->rng, c->R, 3 * c->N);
-  }
-  return launch_ok(c);
+  noise_blocks_release(c);
+  return draw_noise(c, c->R);
 }
 
 int bd_update_fd(bd_ctx* c) {
@@ -1072,6 +1091,7 @@ int bd_download_mobility(bd_ctx* c, double* M9) {
 
 int bd_charge_hop(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
+  noise_blocks_release(c);
   return charge_hop(c);
 }
 
@@ -1088,6 +1108,7 @@ int bd_download_hop_log(bd_ctx* c, int* log3) {
 // the reference's periods (t % srpy, t % MStep).
 int bd_step_reference(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
   if (!c || nsteps < 0) return BD_ERR_ARG;
+  noise_blocks_release(c);
   int s;
   bool ext = c->p.flow == BD_FLOW_EXT;
   prof_begin(c, BD_PROF_STEP);
@@ -1126,6 +1147,20 @@ int bd_step_reference(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
 }  // extern "C"
 
 namespace bd {
+// One draw of the Brownian noise into dst: Philox keyed by the draw count, or
+// the reference's sequential ran1/gasdev stream.
+int draw_noise(bd_ctx* c, double* dst) {
+  c->launches++;
+  if (c->p.noise == BD_NOISE_PHILOX) {
+    int n = 3 * c->N, pairs = (n + 1) / 2;
+    k_noise_philox<<<nblk(pairs, 256), 256, 0, c->stream>>>(dst, n, c->p.philox_seed,
+                                                            c->noise_draws++);
+  } else {
+    k_gasdev_seq<<<1, 32, 0, c->stream>>>(c->rng, dst, 3 * c->N);
+  }
+  return launch_ok(c);
+}
+
 void rotate_coords(bd_ctx* c, int inverse) {
   c->launches++;
   k_rotate<<<nblk(c->N, 256), 256, 0, c->stream>>>(c->lat, c->rx, c->ry, c->N, inverse);

@@ -25,15 +25,8 @@
 #include "bd_ctx.cuh"
 #include "bd_cell.cuh"
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
-#define CF(call)                                      \
-  do {                                                \
-    if ((call) != CUFFT_SUCCESS) return BD_ERR_CUDA;  \
-  } while (0)
+#define CU(call) BD_CU(call)
+#define CF(call) BD_CF(call)
 
 namespace {
 

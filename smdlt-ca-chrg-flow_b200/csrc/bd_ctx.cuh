@@ -100,6 +100,38 @@ struct bd_ctx {
   long long lan_calls, lan_iters, lan_maxed, lan_negative;
   int lan_last, pre_last;
 
+  // multi-vector Lanczos over a block of steps' noise (bd_step_lanczos with
+  // noise_block > 1); vector (j, r) of the basis at BV + (j * nbk + r) * 3 NTp
+  int nbk;             // block capacity (1: per-step solves)
+  double *BV;          // (lmax+1) x nbk basis vectors
+  double *Bw, *Bvcur, *Bt1, *Bt2, *BY;  // nbk x 3 NTp each
+  double *BR;          // nbk x 3N noise draws (bead-interleaved)
+  double *Bpart;       // 3 x nbk x (lmax+1) x kDotBlocks partial dots
+  double *Bh;          // nbk x (lmax+1) first-pass coefficients
+  double *Bab;         // alpha, beta: 2 x (lmax+1) x nbk, [j * nbk + r]
+  double *Bsc;         // nbk x 2: |z_r|, 1/|z_r|
+  double *Bc;          // nbk x (lmax+1) combination coefficients
+  int *Bm;             // nbk Krylov dimensions
+  int *Bjd;
+  double *Bhost;       // pinned host copy of alpha, beta
+  void *blk_ev;        // cudaEvent_t of the pending convergence check
+  void *blk_graph[4][2];  // captured block iterations (product, orthogonalisation),
+  int blk_graph_key[4];   // keyed by (preconditioned, right-hand sides)
+  long long blk_graph_launches[4][2];
+  int blk_last;        // smallest Krylov dimension of the previous block
+  long long blk_runs, blk_products;  // block solves, block iterations run
+  long long blk_rhs_products;        // sum over block iterations of their right-hand sides
+  // the current block: steps blk_t0 .. blk_t0 + blk_n - 1, of which blk_next
+  // are taken; valid while the mobility version and the hop flag it was made
+  // with hold.  The generator ran ahead by the untaken draws: Philox counter
+  // blk_draw0 at the first draw, ran1 states before each draw in Brng.
+  unsigned long blk_t0;
+  int blk_n, blk_next, blk_hop;
+  long long blk_hiv;
+  unsigned long long blk_draw0;
+  void *Brng;          // (nbk + 1) bd::Ran1 states
+  long long hi_version;  // bumped whenever the mobility or the preconditioner changes
+
   // CA-TEA sampling (bd_catea.cu)
   double *cb_part;
   int *cb_tileI;
@@ -146,6 +178,7 @@ struct bd_ctx {
   int *pme_base;     // per bead base grid index, 3 x N
   double *pme_w;     // per bead spline weights, 3 x N x 8
   int pme_plan_f, pme_plan_b;
+  int pme_mplan_k[4], pme_mplan_f[4], pme_mplan_b[4];  // batched plans for k right-hand sides
   int rl_cap, rl_ncell_cap;  // real-space pair rows
   int *rl_cnt, *rl_rows, *rl_cell_of, *rl_beads, *rl_cell_count, *rl_cell_start, *rl_cursor;
   void *rl_pos;      // lab-frame positions of the last preparation (double4)
@@ -169,7 +202,10 @@ void prof_clear(bd_ctx* c);
 
 int set_error_from_bits(int bits);
 int check(bd_ctx* c);                 // synchronise and fold device error bits
-int launch_ok(bd_ctx* c);             // report an asynchronous launch error
+// report a launch error (or an earlier asynchronous one), recording the call
+// site for bd_last_error_detail
+int launch_ok_at(bd_ctx* c, const char* file, int line);
+#define launch_ok(c) ::bd::launch_ok_at((c), __FILE__, __LINE__)
 void host_lattice(bd_ctx* c, unsigned long t, Lat* out);
 void host_lattice_at(bd_ctx* c, unsigned long t, double dt, int tp, Lat* out);
 void rotate_coords(bd_ctx* c, int inverse);  // transformCoords (0) / inverseCoords (1)
@@ -196,6 +232,9 @@ int charge_hop(bd_ctx* c);
 // smooth-PME mobility
 int pme_prepare(bd_ctx* c, const Lat& l);
 int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride);
+// Y_r = M X_r for k vectors in Lanczos layout (3 x NTp), RHS strides xs, ys
+int pme_apply_multi(bd_ctx* c, int k, const double* X, size_t xs, double* Y, size_t ys);
+int pme_multi_plan(bd_ctx* c, int k);  // creates the batched transforms for k
 void pme_free(bd_ctx* c);
 
 // CA-TEA sampling
@@ -208,6 +247,8 @@ void coulomb_free(bd_ctx* c);
 // block preconditioner
 int precond_build(bd_ctx* c, const Lat& l);
 int precond_apply(bd_ctx* c, int which, const double* x, double* y);
+int precond_apply_k(bd_ctx* c, int which, int k, const double* x, size_t xs, double* y,
+                    size_t ys);
 void precond_free(bd_ctx* c);
 int mpnn_blocks(bd_ctx* c, const Lat& l, double* G9);
 void mpnn_free(bd_ctx* c);
@@ -216,5 +257,13 @@ void mpnn_free(bd_ctx* c);
 void lanczos_graphs_reset(bd_ctx* c);
 int alloc_lanczos(bd_ctx* c);
 int lanczos_sqrt(bd_ctx* c, const double* zdev_interleaved, bool with_force, int* iters);
+void lanczos_blocks_free(bd_ctx* c);
+// drops the current noise block and winds the generator back to the draws the
+// per-step order has made; every use of the generator outside
+// bd_step_lanczos calls it first
+void noise_blocks_release(bd_ctx* c);
+
+// noise draw of bd_get_noise into dst (3N, bead-interleaved)
+int draw_noise(bd_ctx* c, double* dst);
 
 }  // namespace bd

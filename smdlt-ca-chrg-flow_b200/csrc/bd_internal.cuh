@@ -15,6 +15,10 @@
 
 namespace bd {
 
+// Records the failing CUDA or cuFFT call (code, message, source line) for
+// bd_last_error_detail and returns BD_ERR_CUDA.
+int cuda_fail(int code, const char* msg, const char* file, int line);
+
 // Lattice of the deforming cell at one step (updateLattice,
 // shear/src/main26.c:1382-1408, extensional/src/main14.c:1426-1450).  Built
 // on the host with the C library's transcendental functions and passed to
@@ -175,3 +179,16 @@ __device__ __forceinline__ float ran1_dev(Ran1& g) {
 }
 
 }  // namespace bd
+
+// Checked CUDA runtime and cuFFT calls inside functions returning a status.
+#define BD_CU(call)                                                                   \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return bd::cuda_fail((int)e_, cudaGetErrorString(e_), __FILE__, __LINE__);      \
+  } while (0)
+#define BD_CF(call)                                                                   \
+  do {                                                                                \
+    int r_ = (int)(call);                                                             \
+    if (r_ != 0) return bd::cuda_fail(r_, "cuFFT call failed", __FILE__, __LINE__);   \
+  } while (0)

@@ -17,17 +17,14 @@
 #include <string.h>
 
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "bd_ctx.cuh"
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 static const int kDotBlocks = 148;  // one CTA per SM for the vector reductions
 
@@ -42,8 +39,11 @@ __device__ __forceinline__ double warp_sum_parts(const double* __restrict__ part
   return s;
 }
 
-// sc[0] = sqrt(sum of part) = |w|, sc[1] = 1/|w| (one warp)
+// sc[0] = sqrt(sum of part) = |w|, sc[1] = 1/|w| (one warp per right-hand
+// side blockIdx.x: partials nblk further on, scalars 2 further on)
 __global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc) {
+  part += (size_t)blockIdx.x * nblk;
+  sc += 2 * blockIdx.x;
   double s = warp_sum_parts(part, nblk, 1);
   if (threadIdx.x == 0) {
     sc[0] = sqrt(s);
@@ -51,13 +51,36 @@ __global__ void k_norm_fin(const double* __restrict__ part, int nblk, double* sc
   }
 }
 
-// v (SoA, padded) = z (bead-interleaved) / |z|; padding entries are zero
-__global__ void k_interleaved_to_soa(const double* __restrict__ z, const double* __restrict__ sc,
-                                     double* v, int N, int NTp) {
+// v (SoA, padded) = z (bead-interleaved) / |z|; padding entries are zero.
+// Right-hand side blockIdx.y: z zs, v vs entries further on, scalars 2.
+__global__ void k_interleaved_to_soa(const double* __restrict__ z, size_t zs,
+                                     const double* __restrict__ sc, double* v, size_t vs, int N,
+                                     int NTp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= NTp) return;
+  z += (size_t)blockIdx.y * zs;
+  sc += 2 * blockIdx.y;
+  v += (size_t)blockIdx.y * vs;
   double f = sc[1];
   for (int a = 0; a < 3; a++) v[(size_t)a * NTp + i] = i < N ? z[3 * i + a] * f : 0.0;
+}
+
+// y_r = |z_r| sum_k c_r[k] V_r,k for the right-hand sides of a block
+// (blockIdx.y = r): Krylov dimension m[r], coefficients c + r * cst, basis
+// vector k at V + k * bs + r * n, norm sc[2 r], output y + r * n.
+__global__ void k_combo_m(const double* __restrict__ V, size_t bs, const double* __restrict__ c,
+                          int cst, const int* __restrict__ m, const double* __restrict__ sc,
+                          double* y, int n) {
+  int r = blockIdx.y, nv = m[r];
+  const double* Vr = V + (size_t)r * n;
+  const double* cr = c + (size_t)r * cst;
+  double scale = sc[2 * r];
+  double* yr = y + (size_t)r * n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int k = 0; k < nv; k++) s += cr[k] * Vr[(size_t)k * bs + i];
+    yr[i] = scale * s;
+  }
 }
 
 // y = scale * sum_k c[k] V_k
@@ -149,46 +172,61 @@ __device__ __forceinline__ void sum_parts(const double* __restrict__ part, int n
   __syncthreads();
 }
 
+// Buffers of a Lanczos run over one or several right-hand sides (a block of
+// steps' noise); right-hand side r = blockIdx.y.  Vectors have n entries;
+// basis vector j of r is at V + j * bs + r * n, the work vector at w + r * n,
+// the next product input at vcur + r * n; partial dots at part1/part2 +
+// r * pst and part3 + r * gridDim.x, first-pass coefficients at hsave +
+// r * hst, alpha_j and beta_j at [j * kst + r].
+struct Kry {
+  double* V;
+  size_t bs;
+  double *w, *vcur;
+  double *part1, *part2, *part3;
+  size_t pst;
+  double* hsave;
+  int hst;
+  double *alpha, *beta;
+  int kst;
+  const int* jd;
+  int n;
+};
+
 // The iteration index j lives on the device (*jd) so that one iteration's
 // launches are the same every iteration and can be replayed as a CUDA graph;
 // k_next_j advances it at the end of the iteration.
-__global__ void __launch_bounds__(256) k_orth0(const double* __restrict__ V, size_t vs,
-                                               const int* __restrict__ jd,
-                                               const double* __restrict__ w, int n,
-                                               double* part1) {
-  int nv = *jd + 1, lo, hi;
-  chunk_range(n, lo, hi);
-  chunk_dots(V, vs, nv, w, lo, hi, part1);
+__global__ void __launch_bounds__(256) k_orth0(Kry q) {
+  int r = blockIdx.y, nv = *q.jd + 1, lo, hi;
+  chunk_range(q.n, lo, hi);
+  chunk_dots(q.V + (size_t)r * q.n, q.bs, nv, q.w + (size_t)r * q.n, lo, hi,
+             q.part1 + r * q.pst);
 }
 
-__global__ void __launch_bounds__(256) k_orth1(const double* __restrict__ V, size_t vs,
-                                               const int* __restrict__ jd, double* w, int n,
-                                               const double* __restrict__ part1,
-                                               double* part2, double* hsave) {
+__global__ void __launch_bounds__(256) k_orth1(Kry q) {
   __shared__ double h[kMaxKrylov + 1];
-  int nv = *jd + 1, lo, hi;
-  chunk_range(n, lo, hi);
-  sum_parts(part1, nv, h);
+  int r = blockIdx.y, nv = *q.jd + 1, lo, hi;
+  const double* V = q.V + (size_t)r * q.n;
+  double* w = q.w + (size_t)r * q.n;
+  chunk_range(q.n, lo, hi);
+  sum_parts(q.part1 + r * q.pst, nv, h);
   if (blockIdx.x == 0)
-    for (int k = threadIdx.x; k < nv; k += blockDim.x) hsave[k] = h[k];
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) w[i] -= combo_row(V, vs, h, nv, i);
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) q.hsave[(size_t)r * q.hst + k] = h[k];
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) w[i] -= combo_row(V, q.bs, h, nv, i);
   __syncthreads();
-  chunk_dots(V, vs, nv, w, lo, hi, part2);
+  chunk_dots(V, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
 }
 
-__global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, size_t vs,
-                                               const int* __restrict__ jd, double* w, int n,
-                                               const double* __restrict__ part2,
-                                               double* part3, const double* __restrict__ hsave,
-                                               double* alpha) {
+__global__ void __launch_bounds__(256) k_orth2(Kry q) {
   __shared__ double h[kMaxKrylov + 1];
   __shared__ double red[8];
-  int j = *jd, nv = j + 1, lo, hi;
-  chunk_range(n, lo, hi);
-  sum_parts(part2, nv, h);
+  int r = blockIdx.y, j = *q.jd, nv = j + 1, lo, hi;
+  const double* V = q.V + (size_t)r * q.n;
+  double* w = q.w + (size_t)r * q.n;
+  chunk_range(q.n, lo, hi);
+  sum_parts(q.part2 + r * q.pst, nv, h);
   double s2 = 0;
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double x = w[i] - combo_row(V, vs, h, nv, i);
+    double x = w[i] - combo_row(V, q.bs, h, nv, i);
     w[i] = x;
     s2 += x * x;
   }
@@ -197,32 +235,31 @@ __global__ void __launch_bounds__(256) k_orth2(const double* __restrict__ V, siz
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
-    part3[blockIdx.x] = t;
-    if (blockIdx.x == 0) alpha[j] = hsave[j] + h[j];
+    for (int p = 0; p < (int)(blockDim.x >> 5); p++) t += red[p];
+    q.part3[(size_t)r * gridDim.x + blockIdx.x] = t;
+    if (blockIdx.x == 0) q.alpha[(size_t)j * q.kst + r] = q.hsave[(size_t)r * q.hst + j] + h[j];
   }
 }
 
 // beta_j = |w|; v_{j+1} = w / beta_j into the basis and into vcur (the
 // fixed input of the next iteration's product)
-__global__ void __launch_bounds__(256) k_orth3(const double* __restrict__ w, int n,
-                                               const double* __restrict__ part3, double* beta,
-                                               const int* __restrict__ jd, double* V, size_t vs,
-                                               double* vcur) {
+__global__ void __launch_bounds__(256) k_orth3(Kry q) {
   __shared__ double b;
-  int j = *jd;
+  int r = blockIdx.y, j = *q.jd;
   if (threadIdx.x < 32) {
-    double s = warp_sum_parts(part3, gridDim.x, 1);
+    double s = warp_sum_parts(q.part3 + (size_t)r * gridDim.x, gridDim.x, 1);
     if (threadIdx.x == 0) {
       b = sqrt(s);
-      if (blockIdx.x == 0) beta[j] = b;
+      if (blockIdx.x == 0) q.beta[(size_t)j * q.kst + r] = b;
     }
   }
   __syncthreads();
   double f = b > 0 ? 1.0 / b : 0.0;
-  double* vnext = V + (size_t)(j + 1) * vs;
+  const double* w = q.w + (size_t)r * q.n;
+  double* vnext = q.V + (size_t)(j + 1) * q.bs + (size_t)r * q.n;
+  double* vcur = q.vcur + (size_t)r * q.n;
   int lo, hi;
-  chunk_range(n, lo, hi);
+  chunk_range(q.n, lo, hi);
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     double x = w[i] * f;
     vnext[i] = x;
@@ -234,8 +271,12 @@ __global__ void k_next_j(int* jd) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *jd += 1;
 }
 
-// |z|^2 partials over the bead-interleaved noise
-__global__ void __launch_bounds__(256) k_sumsq(const double* __restrict__ z, int n, double* part) {
+// |z|^2 partials over the bead-interleaved noise (right-hand side blockIdx.y:
+// z zs entries further on, partials gridDim.x further on)
+__global__ void __launch_bounds__(256) k_sumsq(const double* __restrict__ z, size_t zs, int n,
+                                               double* part) {
+  z += (size_t)blockIdx.y * zs;
+  part += (size_t)blockIdx.y * gridDim.x;
   double s = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     s += z[i] * z[i];
@@ -281,12 +322,19 @@ __global__ void k_krylov_update(int flow, double* rx, double* ry, double* rz, do
 
 // Implicit symmetric QR with Wilkinson shifts on T = tridiag(e, d, e)
 // (Golub & Van Loan, Alg. 8.3.2/8.3.3).  d[n] diagonal, e[n-1] off-diagonal;
-// on return d holds the eigenvalues and Z (n x n, Z[i*n+k] = component i of
-// eigenvector k) the orthonormal eigenvectors.
+// on return d holds the eigenvalues.  The eigenvector matrix is the product
+// Z = R_1 R_2 ... R_T of the Givens rotations of the sweeps (R_t acting on
+// columns k, k+1 as [[cs, sn], [-sn, cs]]); they are returned in order instead
+// of accumulated, so that f(T) e_1 = Z f(Lambda) Z^T e_1 costs O(T) = O(n^2)
+// rather than the O(n^3) of forming Z.
+struct Givens {
+  int k;
+  double cs, sn;
+};
+
 static void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e,
-                        std::vector<double>& Z) {
-  Z.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; i++) Z[(size_t)i * n + i] = 1.0;
+                        std::vector<Givens>& rot) {
+  rot.clear();
   if (n == 1) return;
   e.resize(n, 0.0);
   int hi = n - 1, guard = 0;
@@ -319,36 +367,49 @@ static void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e,
         x = e[k];
         z = bulge;
       }
-      for (int i = 0; i < n; i++) {
-        double zk = Z[(size_t)i * n + k], zk1 = Z[(size_t)i * n + k + 1];
-        Z[(size_t)i * n + k] = cs * zk - sn * zk1;
-        Z[(size_t)i * n + k + 1] = sn * zk + cs * zk1;
-      }
+      rot.push_back({k, cs, sn});
     }
   }
 }
 
 // c = T^q e_1 for T = tridiag(beta, alpha, beta) of size m, q = +1/2 or
 // -1/2; non-positive Ritz values are clamped (to zero for q > 0, to 1e-12 of
-// the largest for q < 0) and counted.
+// the largest for q < 0) and counted.  y = Z^T e_1 applies R_1^T .. R_T^T to
+// e_1; c = Z f(Lambda) y applies R_T .. R_1.
 static int sqrt_e1(const std::vector<double>& alpha, const std::vector<double>& beta, int m,
                    std::vector<double>& c, double q = 0.5) {
+  if (m <= 0) {
+    c.clear();
+    return 0;
+  }
   std::vector<double> d(alpha.begin(), alpha.begin() + m), e(beta.begin(), beta.begin() + (m - 1));
-  std::vector<double> Z;
-  tridiag_eig(m, d, e, Z);
+  std::vector<Givens> rot;
+  tridiag_eig(m, d, e, rot);
+  std::vector<double> y(m, 0.0);
+  y[0] = 1.0;
+  for (const Givens& g : rot) {
+    double a = y[g.k], b = y[g.k + 1];
+    y[g.k] = g.cs * a - g.sn * b;
+    y[g.k + 1] = g.sn * a + g.cs * b;
+  }
   int neg = 0;
   double lmax = 0;
   for (int k = 0; k < m; k++) lmax = std::max(lmax, d[k]);
-  c.assign(m, 0.0);
   for (int k = 0; k < m; k++) {
     double lam = d[k];
     if (lam <= 0) {
       neg++;
       lam = q > 0 ? 0.0 : 1e-12 * lmax;
     }
-    double w = (q > 0 ? sqrt(lam) : 1.0 / sqrt(lam)) * Z[(size_t)0 * m + k];
-    for (int i = 0; i < m; i++) c[i] += Z[(size_t)i * m + k] * w;
+    y[k] *= q > 0 ? sqrt(lam) : 1.0 / sqrt(lam);
   }
+  for (size_t t = rot.size(); t-- > 0;) {
+    const Givens& g = rot[t];
+    double a = y[g.k], b = y[g.k + 1];
+    y[g.k] = g.cs * a + g.sn * b;
+    y[g.k + 1] = -g.sn * a + g.cs * b;
+  }
+  c.swap(y);
   return neg;
 }
 
@@ -409,14 +470,27 @@ static int lanczos_iteration(bd_ctx* c, bool pre, bool force) {
     }
     precond_apply(c, 0, c->Lt2, c->Lw);
   }
-  double* part1 = c->Lpart;
-  double* part2 = c->Lpart + (size_t)(c->lmax + 1) * blk;
-  double* part3 = c->Lpart + (size_t)2 * (c->lmax + 1) * blk;
+  Kry q;
+  q.V = c->LV;
+  q.bs = vs;
+  q.w = c->Lw;
+  q.vcur = vc;
+  q.part1 = c->Lpart;
+  q.part2 = c->Lpart + (size_t)(c->lmax + 1) * blk;
+  q.part3 = c->Lpart + (size_t)2 * (c->lmax + 1) * blk;
+  q.pst = 0;
+  q.hsave = c->Lc;
+  q.hst = 0;
+  q.alpha = c->Lh;
+  q.beta = c->Lsc + 8;
+  q.kst = 1;
+  q.jd = c->Ljd;
+  q.n = n;
   c->launches += 5;
-  k_orth0<<<blk, 256, 0, st>>>(c->LV, vs, c->Ljd, c->Lw, n, part1);
-  k_orth1<<<blk, 256, 0, st>>>(c->LV, vs, c->Ljd, c->Lw, n, part1, part2, c->Lc);
-  k_orth2<<<blk, 256, 0, st>>>(c->LV, vs, c->Ljd, c->Lw, n, part2, part3, c->Lc, c->Lh);
-  k_orth3<<<blk, 256, 0, st>>>(c->Lw, n, part3, c->Lsc + 8, c->Ljd, c->LV, vs, vc);
+  k_orth0<<<blk, 256, 0, st>>>(q);
+  k_orth1<<<blk, 256, 0, st>>>(q);
+  k_orth2<<<blk, 256, 0, st>>>(q);
+  k_orth3<<<blk, 256, 0, st>>>(q);
   k_next_j<<<1, 32, 0, st>>>(c->Ljd);
   return launch_ok(c);
 }
@@ -445,7 +519,7 @@ static int lanczos_iteration_graph(bd_ctx* c, bool pre) {
   }
   CU(cudaGraphLaunch((cudaGraphExec_t)c->lan_graph[v], c->stream));
   c->launches += c->lan_graph_launches[v];
-  return BD_OK;
+  return launch_ok(c);
 }
 
 // Lanczos for f(A) z, f(x) = x^q (q = +-1/2), z bead-interleaved on the
@@ -462,9 +536,10 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
   cudaStream_t st = c->stream;
   // |z|, v_0 (into the basis and the product input), j = 0
   c->launches += 3;
-  k_sumsq<<<blk, 256, 0, st>>>(z, 3 * N, c->Lpart);
+  k_sumsq<<<blk, 256, 0, st>>>(z, 0, 3 * N, c->Lpart);
   k_norm_fin<<<1, 32, 0, st>>>(c->Lpart, blk, c->Lsc);
-  k_interleaved_to_soa<<<(NTp + 255) / 256, 256, 0, st>>>(z, c->Lsc, c->LV, N, NTp);
+  k_interleaved_to_soa<<<(NTp + 255) / 256, 256, 0, st>>>(z, 0, c->Lsc, c->LV, 0, N, NTp);
+  if ((s = launch_ok(c)) != BD_OK) return s;
   CU(cudaMemcpyAsync(c->Lvcur, c->LV, 8 * vs, cudaMemcpyDeviceToDevice, st));
   CU(cudaMemsetAsync(c->Ljd, 0, sizeof(int), st));
   double zn = 0;
@@ -528,6 +603,343 @@ void lanczos_graphs_reset(bd_ctx* c) {
       cudaGraphExecDestroy((cudaGraphExec_t)c->lan_graph[v]);
       c->lan_graph[v] = nullptr;
     }
+  for (int v = 0; v < 4; v++)
+    for (int h = 0; h < 2; h++)
+      if (c->blk_graph[v][h]) {
+        cudaGraphExecDestroy((cudaGraphExec_t)c->blk_graph[v][h]);
+        c->blk_graph[v][h] = nullptr;
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Noise blocks: sqrt(A) z_r for the noise draws z_0..z_{k-1} of k consecutive
+// steps by one Lanczos run over k right-hand sides.  Each right-hand side has
+// its own basis, coefficients and stopping point; they share the launches
+// (the particle-mesh product of 3 k grids, the preconditioner blocks and the
+// CGS2 kernels with blockIdx.y = r), which turns k latency-bound iterations
+// into one.  The host checks convergence for all right-hand sides at once,
+// one iteration behind the device (the next iteration is already queued
+// while the tridiagonal problems are solved, on several host threads).
+
+static int alloc_blocks(bd_ctx* c) {
+  if (c->BV) return BD_OK;
+  int k = c->nbk, L1 = c->lmax + 1, blk = kDotBlocks;
+  size_t n = 3 * (size_t)c->NT * 32;
+  CU(cudaMalloc(&c->BV, 8 * n * k * L1));
+  for (double** q : {&c->Bw, &c->Bvcur, &c->Bt1, &c->Bt2, &c->BY}) {
+    CU(cudaMalloc(q, 8 * n * k));
+    CU(cudaMemsetAsync(*q, 0, 8 * n * k, c->stream));  // padding entries stay zero
+  }
+  CU(cudaMalloc(&c->BR, 8 * 3 * (size_t)c->N * k));
+  CU(cudaMalloc(&c->Bpart, 8 * (size_t)3 * k * L1 * blk));
+  CU(cudaMalloc(&c->Bh, 8 * (size_t)k * L1));
+  CU(cudaMalloc(&c->Bab, 8 * (size_t)2 * k * L1));
+  CU(cudaMalloc(&c->Bsc, 8 * (size_t)2 * k));
+  CU(cudaMalloc(&c->Bc, 8 * (size_t)k * L1));
+  CU(cudaMalloc(&c->Bm, 4 * (size_t)k));
+  CU(cudaMalloc(&c->Bjd, 16));
+  CU(cudaMallocHost(&c->Bhost, 8 * (size_t)2 * k * L1));
+  CU(cudaMalloc(&c->Brng, sizeof(Ran1) * (size_t)(k + 1)));
+  cudaEvent_t ev;
+  CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  c->blk_ev = (void*)ev;
+  c->bytes += 8 * n * k * (L1 + 5) + 24 * (size_t)c->N * k + 8 * (size_t)k * L1 * (3 * blk + 4) +
+              24 * (size_t)k;
+  return BD_OK;
+}
+
+void lanczos_blocks_free(bd_ctx* c) {
+  for (double* q : {c->BV, c->Bw, c->Bvcur, c->Bt1, c->Bt2, c->BY, c->BR, c->Bpart, c->Bh, c->Bab,
+                    c->Bsc, c->Bc})
+    if (q) cudaFree(q);
+  if (c->Bm) cudaFree(c->Bm);
+  if (c->Bjd) cudaFree(c->Bjd);
+  if (c->Bhost) cudaFreeHost(c->Bhost);
+  if (c->Brng) cudaFree(c->Brng);
+  c->Brng = nullptr;
+  if (c->blk_ev) cudaEventDestroy((cudaEvent_t)c->blk_ev);
+  c->BV = nullptr;
+  c->Bhost = nullptr;
+  c->blk_ev = nullptr;
+}
+
+void noise_blocks_release(bd_ctx* c) {
+  if (c->blk_n > 0 && c->blk_next < c->blk_n) {
+    if (c->p.noise == BD_NOISE_PHILOX)
+      c->noise_draws = c->blk_draw0 + (unsigned long long)c->blk_next;
+    else
+      cudaMemcpyAsync(c->rng, (const Ran1*)c->Brng + c->blk_next, sizeof(Ran1),
+                      cudaMemcpyDeviceToDevice, c->stream);
+  }
+  c->blk_n = 0;
+  c->blk_next = 0;
+}
+
+// Layout of a block of k right-hand sides: basis vector j of r at
+// BV + (j k + r) n, alpha_j and beta_j at [j k + r].
+static Kry block_kry(bd_ctx* c, int k) {
+  int L1 = c->lmax + 1, blk = kDotBlocks;
+  size_t n = 3 * (size_t)c->NT * 32;
+  Kry q;
+  q.V = c->BV;
+  q.bs = n * k;
+  q.w = c->Bw;
+  q.vcur = c->Bvcur;
+  q.part1 = c->Bpart;
+  q.part2 = c->Bpart + (size_t)k * L1 * blk;
+  q.part3 = c->Bpart + (size_t)2 * k * L1 * blk;
+  q.pst = (size_t)L1 * blk;
+  q.hsave = c->Bh;
+  q.hst = L1;
+  q.alpha = c->Bab;
+  q.beta = c->Bab + (size_t)L1 * k;
+  q.kst = k;
+  q.jd = c->Bjd;
+  q.n = (int)n;
+  return q;
+}
+
+// One iteration of the block, in two parts: the product W = A V_cur for the
+// k inputs (part 0), then CGS2 of each against its own basis, beta, next
+// vectors, j += 1 (part 1).  The same launches every iteration (j is read on
+// the device), so each part can be captured as a graph; the product is timed
+// on its own (BD_PROF_BLOCK) between the two.
+static int block_part(bd_ctx* c, int k, bool pre, int part) {
+  int s;
+  size_t n = 3 * (size_t)c->NT * 32;
+  cudaStream_t st = c->stream;
+  if (part == 0) {
+    if (!pre) {
+      if ((s = pme_apply_multi(c, k, c->Bvcur, n, c->Bw, n)) != BD_OK) return s;
+    } else {
+      precond_apply_k(c, 1, k, c->Bvcur, n, c->Bt1, n);
+      if ((s = pme_apply_multi(c, k, c->Bt1, n, c->Bt2, n)) != BD_OK) return s;
+      precond_apply_k(c, 0, k, c->Bt2, n, c->Bw, n);
+    }
+    return launch_ok(c);
+  }
+  Kry q = block_kry(c, k);
+  dim3 g(kDotBlocks, k);
+  c->launches += 5;
+  k_orth0<<<g, 256, 0, st>>>(q);
+  k_orth1<<<g, 256, 0, st>>>(q);
+  k_orth2<<<g, 256, 0, st>>>(q);
+  k_orth3<<<g, 256, 0, st>>>(q);
+  k_next_j<<<1, 32, 0, st>>>(c->Bjd);
+  return launch_ok(c);
+}
+
+static int block_iteration(bd_ctx* c, int k, bool pre) {
+  int s;
+  if (!c->use_graphs) {
+    prof_begin(c, BD_PROF_BLOCK);
+    if ((s = block_part(c, k, pre, 0)) != BD_OK) return s;
+    prof_end(c, BD_PROF_BLOCK);
+    return block_part(c, k, pre, 1);
+  }
+  int key = 2 * k + (pre ? 1 : 0), slot = -1;
+  for (int q = 0; q < 4 && slot < 0; q++)
+    if (c->blk_graph[q][0] && c->blk_graph_key[q] == key) slot = q;
+  if (slot < 0) {
+    for (int q = 0; q < 4 && slot < 0; q++)
+      if (!c->blk_graph[q][0]) slot = q;
+    if (slot < 0) {
+      slot = 3;
+      for (int h = 0; h < 2; h++) {
+        cudaGraphExecDestroy((cudaGraphExec_t)c->blk_graph[slot][h]);
+        c->blk_graph[slot][h] = nullptr;
+      }
+    }
+    for (int h = 0; h < 2; h++) {
+      cudaGraph_t g;
+      long long l0 = c->launches;
+      c->capturing = true;
+      CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int s2 = block_part(c, k, pre, h);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      c->capturing = false;
+      if (s2 != BD_OK) return s2;
+      if (e != cudaSuccess) return BD_ERR_CUDA;
+      cudaGraphExec_t ex;
+      e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return BD_ERR_CUDA;
+      c->blk_graph[slot][h] = (void*)ex;
+      c->blk_graph_launches[slot][h] = c->launches - l0;
+      c->launches = l0;
+    }
+    c->blk_graph_key[slot] = key;
+  }
+  prof_begin(c, BD_PROF_BLOCK);
+  CU(cudaGraphLaunch((cudaGraphExec_t)c->blk_graph[slot][0], c->stream));
+  prof_end(c, BD_PROF_BLOCK);
+  CU(cudaGraphLaunch((cudaGraphExec_t)c->blk_graph[slot][1], c->stream));
+  c->launches += c->blk_graph_launches[slot][0] + c->blk_graph_launches[slot][1];
+  return BD_OK;
+}
+
+// f(i) for i < n on up to 16 host threads.
+template <class F>
+static void parallel_for(int n, F f) {
+  int nt = std::min(n, (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  if (nt <= 1) {
+    for (int i = 0; i < n; i++) f(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; t++)
+    th.emplace_back([&f, t, nt, n] {
+      for (int i = t; i < n; i += nt) f(i);
+    });
+  for (int i = 0; i < n; i += nt) f(i);
+  for (auto& x : th) x.join();
+}
+
+// Lanczos for sqrt(A) z_r, r < k, z_r = BR + 3 N r; the results
+// |z_r| V_r,m f(T_r,m) e_1 go to out + r n.  mr[r] is the Krylov dimension of
+// right-hand side r, conv[r] whether it met the tolerance within the cap.
+static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vector<int>& mr,
+                             std::vector<char>& conv, int* iters_run) {
+  int s, N = c->N, NTp = c->NT * 32, blk = kDotBlocks, L1 = c->lmax + 1;
+  size_t n = 3 * (size_t)NTp;
+  cudaStream_t st = c->stream;
+  cudaEvent_t ev = (cudaEvent_t)c->blk_ev;
+  c->launches += 3;
+  k_sumsq<<<dim3(blk, k), 256, 0, st>>>(c->BR, 3 * (size_t)N, 3 * N, c->Bpart);
+  k_norm_fin<<<k, 32, 0, st>>>(c->Bpart, blk, c->Bsc);
+  k_interleaved_to_soa<<<dim3((NTp + 255) / 256, k), 256, 0, st>>>(c->BR, 3 * (size_t)N, c->Bsc,
+                                                                   c->BV, n, N, NTp);
+  CU(cudaMemcpyAsync(c->Bvcur, c->BV, 8 * n * k, cudaMemcpyDeviceToDevice, st));
+  CU(cudaMemsetAsync(c->Bjd, 0, sizeof(int), st));
+  std::vector<std::vector<double>> cc(k);
+  std::vector<char> done(k, 0);
+  std::vector<int> negs(k, 0);
+  mr.assign(k, 0);
+  conv.assign(k, 0);
+  int ndone = 0, pending = 0, m = 0;
+  int next_check = std::max(4, c->blk_last - 2);
+  const double* ha = c->Bhost;
+  const double* hb = c->Bhost + (size_t)L1 * k;
+  // convergence of every open right-hand side at Krylov dimension mm, from the
+  // alpha and beta copied after iteration mm
+  auto evaluate = [&](int mm) -> int {
+    CU(cudaEventSynchronize(ev));
+    std::vector<int> open;
+    for (int r = 0; r < k; r++)
+      if (!done[r]) open.push_back(r);
+    parallel_for((int)open.size(), [&](int q) {
+      int r = open[q];
+      std::vector<double> alpha(mm), beta(mm), cprev;
+      for (int i = 0; i < mm; i++) {
+        alpha[i] = ha[(size_t)i * k + r];
+        beta[i] = hb[(size_t)i * k + r];
+      }
+      std::vector<double> cm;
+      int neg = sqrt_e1(alpha, beta, mm, cm, 0.5);
+      sqrt_e1(alpha, beta, mm - 1, cprev, 0.5);
+      double dn = 0, cn = 0;
+      for (int i = 0; i < mm; i++) {
+        double prev = i < mm - 1 ? cprev[i] : 0.0;
+        dn += (cm[i] - prev) * (cm[i] - prev);
+        cn += cm[i] * cm[i];
+      }
+      bool ok = sqrt(dn) <= c->ltol * sqrt(cn) || beta[mm - 1] <= 1e-300;
+      if (ok || mm >= c->lmax) {
+        done[r] = 1;
+        conv[r] = ok;
+        mr[r] = mm;
+        negs[r] = neg;
+        cc[r].swap(cm);
+      }
+    });
+    ndone = 0;
+    for (int r = 0; r < k; r++) ndone += done[r];
+    return BD_OK;
+  };
+  int j = 0;
+  for (; j < c->lmax; j++) {
+    s = block_iteration(c, k, pre);
+    if (s != BD_OK) return s;
+    m = j + 1;
+    if (pending) {
+      if ((s = evaluate(pending)) != BD_OK) return s;
+      pending = 0;
+      if (ndone == k) {
+        j++;
+        break;
+      }
+    }
+    if (m >= next_check || m == c->lmax) {
+      CU(cudaMemcpyAsync(c->Bhost, c->Bab, 8 * (size_t)m * k, cudaMemcpyDeviceToHost, st));
+      CU(cudaMemcpyAsync(c->Bhost + (size_t)L1 * k, c->Bab + (size_t)L1 * k, 8 * (size_t)m * k,
+                         cudaMemcpyDeviceToHost, st));
+      CU(cudaEventRecord(ev, st));
+      pending = m;
+      next_check = m + 2;
+    }
+  }
+  if (pending && (s = evaluate(pending)) != BD_OK) return s;
+  std::vector<double> hc((size_t)k * L1, 0.0);
+  int mmin = c->lmax;
+  for (int r = 0; r < k; r++) {
+    std::copy(cc[r].begin(), cc[r].end(), hc.begin() + (size_t)r * L1);
+    mmin = std::min(mmin, mr[r]);
+    c->lan_negative += negs[r];
+  }
+  CU(cudaMemcpyAsync(c->Bc, hc.data(), 8 * hc.size(), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(c->Bm, mr.data(), 4 * (size_t)k, cudaMemcpyHostToDevice, st));
+  c->launches++;
+  k_combo_m<<<dim3(blk, k), 256, 0, st>>>(c->BV, n * k, c->Bc, L1, c->Bm, c->Bsc, out, (int)n);
+  c->blk_last = mmin;
+  c->blk_runs++;
+  c->blk_products += j;
+  c->blk_rhs_products += (long long)j * k;
+  if (iters_run) *iters_run = j;
+  CU(cudaStreamSynchronize(st));  // hc and mr are read by the copies above
+  return launch_ok(c);
+}
+
+// sqrt(M) z_r for the k noise draws at BR into BY (Lanczos layout, stride
+// 3 NTp): the preconditioned solve G^-1 sqrt(G M G^T) z_r when a block
+// preconditioner is set, with the plain single-vector solve for a right-hand
+// side that misses the tolerance (a fallback, counted).
+static int lanczos_sqrt_block(bd_ctx* c, int k) {
+  int s;
+  if (!c->hi_built) return BD_ERR_STATE;
+  if ((s = alloc_lanczos(c)) != BD_OK) return s;
+  if ((s = alloc_blocks(c)) != BD_OK) return s;
+  if (k < 1 || k > c->nbk) return BD_ERR_ARG;
+  if (k > 1 && (s = pme_multi_plan(c, k)) != BD_OK) return s;
+  size_t n = 3 * (size_t)c->NT * 32;
+  bool pre = c->pre_kind != BD_PRECOND_NONE && c->pre_ready;
+  std::vector<int> mr;
+  std::vector<char> conv;
+  if ((s = lanczos_run_multi(c, k, pre, pre ? c->Bt1 : c->BY, mr, conv, nullptr)) != BD_OK)
+    return s;
+  if (pre) precond_apply_k(c, 2, k, c->Bt1, n, c->BY, n);
+  for (int r = 0; r < k; r++) {
+    c->lan_calls++;
+    if (pre) {
+      c->pre_calls++;
+      c->pre_iters += mr[r];
+      if (conv[r]) {
+        c->lan_iters += mr[r];
+        continue;
+      }
+      c->pre_fallbacks++;
+      int m = 0;
+      bool cv = false;
+      if ((s = lanczos_run(c, c->BR + 3 * (size_t)c->N * r, false, false, 0.5, c->BY + n * r, &m,
+                           &cv)) != BD_OK)
+        return s;
+      c->lan_iters += m;
+      if (!cv) c->lan_maxed++;
+    } else {
+      c->lan_iters += mr[r];
+      if (!conv[r]) c->lan_maxed++;
+    }
+  }
+  return launch_ok(c);
 }
 
 // sqrt(M) z for the bead-interleaved z on the device (c->R): result in c->Yz.
@@ -633,6 +1045,20 @@ int bd_lanczos_inv_sqrt(bd_ctx* c, const double* z, double* out, int* iters) {
   return conv ? BD_OK : BD_ERR_LANCZOS;
 }
 
+int bd_noise_block_release(bd_ctx* c) {
+  if (!c) return BD_ERR_ARG;
+  noise_blocks_release(c);
+  return launch_ok(c);
+}
+
+int bd_noise_block_stats(bd_ctx* c, long* o) {
+  if (!c || !o) return BD_ERR_ARG;
+  o[0] = (long)c->blk_runs;
+  o[1] = (long)c->blk_products;
+  o[2] = (long)c->blk_rhs_products;
+  return BD_OK;
+}
+
 int bd_lanczos_stats(bd_ctx* c, long* o) {
   if (!c || !o) return BD_ERR_ARG;
   o[0] = (long)c->lan_calls;
@@ -642,10 +1068,31 @@ int bd_lanczos_stats(bd_ctx* c, long* o) {
   return BD_OK;
 }
 
+// Steps from t covered by one noise block: at most the block capacity, none
+// past the next mobility rebuild, and with the reference's ran1 noise and
+// sequential hop (one generator) none past the next charge-hop sweep, so that
+// every draw happens in the per-step order.  A block may outlive the call that
+// made it (a caller stepping one step at a time still gets blocks).
+static int block_len(bd_ctx* c, unsigned long t, int with_hop) {
+  unsigned long kb = (unsigned long)c->nbk;
+  unsigned long sr = (unsigned long)c->srpy;
+  kb = std::min(kb, (t / sr + 1) * sr - t);
+  if (c->tstart > t) kb = std::min(kb, c->tstart - t);
+  if (with_hop && c->nch > 0 && c->p.noise == BD_NOISE_RAN1 && c->p.hop == BD_HOP_SEQUENTIAL) {
+    unsigned long ms = (unsigned long)c->p.MStep;
+    unsigned long th = (t + ms - 1) / ms * ms;  // next sweep at or after t
+    kb = std::min(kb, th - t + 1);
+  }
+  return (int)std::max(1ul, kb);
+}
+
 int bd_step_lanczos(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
   if (!c || nsteps < 0) return BD_ERR_ARG;
   int s;
+  with_hop = with_hop != 0;
   bool ext = c->p.flow == BD_FLOW_EXT;
+  bool blocks = c->nbk > 1;
+  size_t nl = 3 * (size_t)c->NT * 32;
   prof_begin(c, BD_PROF_STEP);
   for (int n = 0; n < nsteps; n++) {
     unsigned long t = t0 + (unsigned long)n;
@@ -661,15 +1108,58 @@ int bd_step_lanczos(bd_ctx* c, unsigned long t0, int nsteps, int with_hop) {
     if ((s = bd_ev_force(c))) return s;
     if ((s = bd_coulomb_force(c))) return s;
     prof_end(c, BD_PROF_FORCES);
-    if ((s = bd_get_noise(c))) return s;
-    if (t % (unsigned long)c->srpy == 0 || t == c->tstart || !c->hi_built)
-      if ((s = calc_hi(c))) return s;
-    if (ext) rotate_coords(c, 1);
-    if ((s = lanczos_sqrt(c, c->R, true, nullptr))) return s;
+    const double* Y = nullptr;  // this step's sqrt(M) z (the solve allocates its buffers)
+    if (!blocks) {
+      noise_blocks_release(c);
+      if ((s = draw_noise(c, c->R))) return s;
+      if (t % (unsigned long)c->srpy == 0 || t == c->tstart || !c->hi_built)
+        if ((s = calc_hi(c))) return s;
+      if (ext) rotate_coords(c, 1);
+      if ((s = lanczos_sqrt(c, c->R, true, nullptr))) return s;
+      Y = c->Yz;
+    } else {
+      if (t % (unsigned long)c->srpy == 0 || t == c->tstart || !c->hi_built)
+        if ((s = calc_hi(c))) return s;
+      bool have = c->blk_n > 0 && c->blk_next < c->blk_n &&
+                  t == c->blk_t0 + (unsigned long)c->blk_next && c->blk_hiv == c->hi_version &&
+                  c->blk_hop == with_hop;
+      if (!have) {
+        // the draws of the block's steps, in step order, and their displacements
+        noise_blocks_release(c);
+        if ((s = alloc_lanczos(c)) != BD_OK || (s = alloc_blocks(c)) != BD_OK) return s;
+        int kb = block_len(c, t, with_hop);
+        c->blk_draw0 = c->noise_draws;
+        for (int r = 0; r < kb; r++) {
+          if (c->p.noise != BD_NOISE_PHILOX)
+            CU(cudaMemcpyAsync((Ran1*)c->Brng + r, c->rng, sizeof(Ran1),
+                               cudaMemcpyDeviceToDevice, c->stream));
+          if ((s = draw_noise(c, c->BR + 3 * (size_t)c->N * r))) return s;
+        }
+        c->blk_t0 = t;
+        c->blk_n = kb;
+        c->blk_next = 0;
+        c->blk_hiv = c->hi_version;
+        c->blk_hop = with_hop;
+        if ((s = lanczos_sqrt_block(c, kb))) {
+          c->blk_n = 0;
+          return s;
+        }
+      }
+      int r = c->blk_next++;
+      // this step's draw stays readable as the context's noise vector
+      CU(cudaMemcpyAsync(c->R, c->BR + 3 * (size_t)c->N * r, 24 * (size_t)c->N,
+                         cudaMemcpyDeviceToDevice, c->stream));
+      if (ext) rotate_coords(c, 1);
+      VecIn vf = {{c->fx, c->fy, c->fz}, 1};
+      if ((s = sym_matvec(c, 1, vf, vf, c->MF, c->MF, true)) != BD_OK) return s;
+      Y = c->BY + nl * r;
+    }
+    if (!Y || !c->MF) return BD_ERR_STATE;
     c->launches++;
     k_krylov_update<<<(c->N + 255) / 256, 256, 0, c->stream>>>(
-        c->p.flow, c->rx, c->ry, c->rz, c->dxv, c->dyv, c->dzv, c->MF, c->Yz, c->NT * 32, c->N,
+        c->p.flow, c->rx, c->ry, c->rz, c->dxv, c->dyv, c->dzv, c->MF, Y, c->NT * 32, c->N,
         c->p.dt, c->p.edot, sqrt(2.0 * c->p.dt));
+    if ((s = launch_ok(c)) != BD_OK) return s;
     if (with_hop && c->nch > 0 && t % (unsigned long)c->p.MStep == 0) {
       if (ext && (s = bd_transform_coords(c))) return s;
       if ((s = charge_hop(c))) return s;

@@ -21,11 +21,7 @@
 #include "bd_ctx.cuh"
 #include "bd_cell.cuh"
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 static const int kHopThreads = 1024;
 

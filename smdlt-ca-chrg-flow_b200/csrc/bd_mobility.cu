@@ -31,11 +31,7 @@
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 static const int kRedSplit = 16;  // column-range splits of the matvec reduction
 
@@ -746,6 +742,7 @@ static Lat step_lat(bd_ctx* c) {
 int calc_hi(bd_ctx* c) {
   int s;
   lanczos_graphs_reset(c);  // captured products hold the diagonal by value
+  c->hi_version++;          // noise blocks solved with the old mobility are void
   if (c->p.mobility == BD_MOB_PME) {
     prof_begin(c, BD_PROF_HI_BUILD);
     s = pme_prepare(c, step_lat(c));

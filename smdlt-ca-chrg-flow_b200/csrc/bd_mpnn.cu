@@ -29,11 +29,7 @@
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 namespace {
 

@@ -19,11 +19,7 @@
 
 #include "bd_ctx.cuh"
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 __global__ void __launch_bounds__(256) k_msd_lag(const double* __restrict__ P, int Tmax, int wmax,
                                                  int nq, int MSDstart, double* out) {

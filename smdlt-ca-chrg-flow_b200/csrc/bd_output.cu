@@ -23,11 +23,7 @@
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 // One thread per chain: unwrapped coordinates, x extension, centre of mass
 // and gyration tensor (xx xy xz yy yz zz) of the unwrapped chain.

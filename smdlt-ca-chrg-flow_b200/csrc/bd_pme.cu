@@ -29,7 +29,8 @@
 //  * calcHI stores only the diagonal entries of the self blocks
 //    (shear/src/main26.c:1663-1700); the off-diagonal entries of the k-space
 //    self sum, which a sheared or stretched cell makes non-zero, are removed.
-// cuFFT is used for the transforms only.  Spreading uses FP64 atomics; the
+// cuFFT is used for the transforms only.  Spreading uses atomics in the grid
+// precision; several right-hand sides share each launch (blockIdx.y).  The
 // spline weights and pair tensors are computed once per step because the
 // positions do not change during a Krylov solve.
 #include <cufft.h>
@@ -44,15 +45,8 @@
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
-#define CF(call)                                  \
-  do {                                            \
-    if ((call) != CUFFT_SUCCESS) return BD_ERR_CUDA; \
-  } while (0)
+#define CU(call) BD_CU(call)
+#define CF(call) BD_CF(call)
 
 // Per bead: base grid index floor(u) and the p weights in each lattice
 // direction (u = K s, s wrapped into [0,1)).  Positions held in the rotated
@@ -87,16 +81,19 @@ __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
 // Q[c][g] += v_c(i) W_i(g): one warp per bead, the P^3 stencil points
 // spread over the lanes with the fastest index along the contiguous grid
 // direction, so each atomic instruction of a warp covers runs of P adjacent
-// grid values.  FP64 atomics into the grid.
+// grid values.  Atomics into the grid.  Right-hand side blockIdx.y reads its
+// vector vr entries further on and owns the grids 3 K^3 entries further on.
 template <int P, typename R>
 __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base,
                                                     const double* __restrict__ w, int N, int K,
-                                                    VecIn v, R* grid) {
+                                                    VecIn v, size_t vr, R* grid) {
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
-  double f0 = v.p[0][(size_t)i * v.stride];
-  double f1 = v.p[1][(size_t)i * v.stride];
-  double f2 = v.p[2][(size_t)i * v.stride];
+  size_t ro = (size_t)blockIdx.y * vr;
+  grid += (size_t)blockIdx.y * 3 * ((size_t)K * K * K);
+  double f0 = v.p[0][ro + (size_t)i * v.stride];
+  double f1 = v.p[1][ro + (size_t)i * v.stride];
+  double f2 = v.p[2][ro + (size_t)i * v.stride];
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
@@ -197,10 +194,12 @@ __global__ void k_pme_soff_fin(const double* __restrict__ part, int nb, double* 
   if (threadIdx.x < 3) soff[threadIdx.x] = red[threadIdx.x][0];
 }
 
+// Right-hand side blockIdx.y owns the spectra 3 n entries further on.
 template <typename R, typename Cx>
 __global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size_t n) {
   size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
+  spec += (size_t)blockIdx.y * 3 * n;
   const R* t = infl + 6 * e;
   Cx x = spec[e], y = spec[n + e], z = spec[2 * n + e];
   Cx u, v, w;
@@ -266,16 +265,27 @@ __device__ __forceinline__ void pair_terms(double alpha, double alpha_ref, doubl
 // out_c(i) = sum_g W_i(g) grid_c(g) + self * v_c(i) - S_off v(i)
 //            + sum_j T_ij v_j (row list)
 // One warp per bead: lanes share the stencil points and the pair row, then a
-// butterfly reduction.
+// butterfly reduction.  Right-hand side blockIdx.y: input vr, output orr
+// entries further on, grids 3 K^3 further on.
 template <int P, typename R>
 __global__ void __launch_bounds__(256) k_pme_gather(
     const int* __restrict__ base, const double* __restrict__ w, int N, int K,
-    const R* __restrict__ grid, double self, const double* __restrict__ soff, VecIn v,
+    const R* __restrict__ grid, double self, const double* __restrict__ soff, VecIn v, size_t vr,
     const int* __restrict__ rcnt, const int* __restrict__ rrows,
     const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
-    double* o0, double* o1, double* o2, int ostride) {
+    double* o0, double* o1, double* o2, int ostride, size_t orr) {
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
+  {
+    size_t ro = (size_t)blockIdx.y * vr, oo = (size_t)blockIdx.y * orr;
+    v.p[0] += ro;
+    v.p[1] += ro;
+    v.p[2] += ro;
+    o0 += oo;
+    o1 += oo;
+    o2 += oo;
+    grid += (size_t)blockIdx.y * 3 * ((size_t)K * K * K);
+  }
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
@@ -465,8 +475,10 @@ int pme_alloc(bd_ctx* c) {
   size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
   c->pme_f32 = c->p.precision == BD_PREC_FP32;
   size_t es = c->pme_f32 ? 4 : 8;  // grid, spectrum, influence and pair tensors
-  CU(cudaMalloc(&c->pme_grid, es * 3 * K3));
-  CU(cudaMalloc(&c->pme_spec, 2 * es * 3 * Ks));
+  // grids and spectra for the largest number of right-hand sides of a product
+  size_t nr = (size_t)std::max(1, c->nbk);
+  CU(cudaMalloc(&c->pme_grid, es * 3 * K3 * nr));
+  CU(cudaMalloc(&c->pme_spec, 2 * es * 3 * Ks * nr));
   CU(cudaMalloc(&c->pme_infl, es * 6 * Ks));
   CU(cudaMalloc(&c->pme_bsq, 8 * 3 * (size_t)K));
   c->pme_nblk = (int)((Ks + 255) / 256);
@@ -485,7 +497,7 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_cell_start, 4 * (size_t)(c->rl_ncell_cap + 1)));
   CU(cudaMalloc(&c->rl_cursor, 4 * (size_t)c->rl_ncell_cap));
   CU(cudaMemsetAsync(c->rl_cell_count, 0, 4 * (size_t)c->rl_ncell_cap, c->stream));
-  c->bytes += es * (3 * K3 + 6 * Ks + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
+  c->bytes += es * (3 * K3 * nr + 6 * Ks * nr + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
               24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 2 * es) + 32 * (size_t)N +
               8 * (size_t)N + 12 * (size_t)c->rl_ncell_cap;
   int n[3] = {K, K, K};
@@ -507,9 +519,50 @@ int pme_alloc(bd_ctx* c) {
   return BD_OK;
 }
 
+// Batched transforms of 3 k grids, created outside any stream capture and
+// kept for up to four values of k (replacing one drops the captured
+// iterations that use it).
+int pme_multi_plan(bd_ctx* c, int k) {
+  int slot = -1;
+  for (int q = 0; q < 4; q++)
+    if (c->pme_mplan_k[q] == k) return BD_OK;
+  for (int q = 0; q < 4 && slot < 0; q++)
+    if (c->pme_mplan_k[q] == 0) slot = q;
+  if (slot < 0) {
+    slot = 3;
+    lanczos_graphs_reset(c);
+    cufftDestroy((cufftHandle)c->pme_mplan_f[slot]);
+    cufftDestroy((cufftHandle)c->pme_mplan_b[slot]);
+    c->pme_mplan_k[slot] = 0;
+  }
+  int K = c->pmeK;
+  size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
+  int n[3] = {K, K, K};
+  cufftHandle f, b;
+  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
+                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3 * k));
+  if (cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
+                    c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3 * k) != CUFFT_SUCCESS) {
+    cufftDestroy(f);
+    return BD_ERR_CUDA;
+  }
+  CF(cufftSetStream(f, c->stream));
+  CF(cufftSetStream(b, c->stream));
+  c->pme_mplan_f[slot] = (int)f;
+  c->pme_mplan_b[slot] = (int)b;
+  c->pme_mplan_k[slot] = k;
+  return BD_OK;
+}
+
 void pme_free(bd_ctx* c) {
   if (c->pme_plan_f) cufftDestroy((cufftHandle)c->pme_plan_f);
   if (c->pme_plan_b) cufftDestroy((cufftHandle)c->pme_plan_b);
+  for (int q = 0; q < 4; q++)
+    if (c->pme_mplan_k[q]) {
+      cufftDestroy((cufftHandle)c->pme_mplan_f[q]);
+      cufftDestroy((cufftHandle)c->pme_mplan_b[q]);
+      c->pme_mplan_k[q] = 0;
+    }
   void* ptrs[] = {c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
                   c->rl_cnt, c->rl_rows, c->rl_pos, c->rl_tt, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
                   c->rl_cell_start, c->rl_cursor};
@@ -547,6 +600,7 @@ int pme_prepare(bd_ctx* c, const Lat& l) {
     k_pme_influence<double><<<c->pme_nblk, 256, 0, c->stream>>>(
         cell, K, alpha, c->pme_bsq, (double*)c->pme_infl, c->pme_soff + 3);
   k_pme_soff_fin<<<1, 256, 0, c->stream>>>(c->pme_soff + 3, c->pme_nblk, c->pme_soff);
+  if ((s = launch_ok(c)) != BD_OK) return s;
   // real-space cells: perpendicular widths V/|a_j x a_k|
   double w[3];
   {
@@ -576,6 +630,7 @@ int pme_prepare(bd_ctx* c, const Lat& l) {
   k_rl_scan<<<1, 1024, 0, c->stream>>>(ncell, c->rl_cell_count, c->rl_cell_start, c->rl_cursor);
   k_rl_fill<<<nblk(N, 256), 256, 0, c->stream>>>(c->rl_cell_of, c->rl_cell_start, c->rl_cursor,
                                                  c->rl_beads, N);
+  if ((s = launch_ok(c)) != BD_OK) return s;
 if (c->pme_f32)
     k_rl_rows<float><<<nblk(N, 128), 128, 0, c->stream>>>(
         cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
@@ -598,19 +653,30 @@ if (c->pme_f32)
   return launch_ok(c);
 }
 
-// out = M v by PME for one vector given by component pointers (VecIn).
+// out_r = M v_r by PME for k right-hand sides given by component pointers
+// (VecIn) and RHS strides vr (input) and orr (output); k = 1 is the
+// single-vector product with the context's own transforms.
 template <typename R, typename Cx>
-static int pme_apply_t(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2,
-                       int ostride) {
+static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, double* o1,
+                       double* o2, int ostride, size_t orr) {
   int K = c->pmeK, N = c->N, p = c->pme_p;
   size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
+  if (k < 1 || k > std::max(1, c->nbk)) return BD_ERR_ARG;
+  int pf = c->pme_plan_f, pb = c->pme_plan_b;
+  if (k > 1) {
+    int q = 0;
+    while (q < 4 && c->pme_mplan_k[q] != k) q++;
+    if (q == 4) return BD_ERR_STATE;  // pme_multi_plan(c, k) first
+    pf = c->pme_mplan_f[q];
+    pb = c->pme_mplan_b[q];
+  }
   R* grid = (R*)c->pme_grid;
   Cx* spec = (Cx*)c->pme_spec;
-  CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3, c->stream));
+  CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3 * k, c->stream));
   c->launches += 3;  // spread, influence, gather (the transforms are cuFFT's)
-  int nb8 = nblk(N, 8);
+  dim3 g8(nblk(N, 8), k);
 #define PME_SPREAD(P_) \
-  k_pme_spread<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, grid)
+  k_pme_spread<P_, R><<<g8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, grid)
   switch (p) {
     case 4: PME_SPREAD(4); break;
     case 6: PME_SPREAD(6); break;
@@ -618,27 +684,25 @@ static int pme_apply_t(bd_ctx* c, const VecIn& v, double* o0, double* o1, double
   }
 #undef PME_SPREAD
   if constexpr (sizeof(R) == 4)
-    CF(cufftExecR2C((cufftHandle)c->pme_plan_f, (cufftReal*)grid, (cufftComplex*)spec));
+    CF(cufftExecR2C((cufftHandle)pf, (cufftReal*)grid, (cufftComplex*)spec));
   else
-    CF(cufftExecD2Z((cufftHandle)c->pme_plan_f, (cufftDoubleReal*)grid,
-                    (cufftDoubleComplex*)spec));
-  k_pme_apply_influence<R, Cx><<<nblk((long long)Ks, 256), 256, 0, c->stream>>>(
+    CF(cufftExecD2Z((cufftHandle)pf, (cufftDoubleReal*)grid, (cufftDoubleComplex*)spec));
+  k_pme_apply_influence<R, Cx><<<dim3(nblk((long long)Ks, 256), k), 256, 0, c->stream>>>(
       (const R*)c->pme_infl, spec, Ks);
   if constexpr (sizeof(R) == 4)
-    CF(cufftExecC2R((cufftHandle)c->pme_plan_b, (cufftComplex*)spec, (cufftReal*)grid));
+    CF(cufftExecC2R((cufftHandle)pb, (cufftComplex*)spec, (cufftReal*)grid));
   else
-    CF(cufftExecZ2D((cufftHandle)c->pme_plan_b, (cufftDoubleComplex*)spec,
-                    (cufftDoubleReal*)grid));
+    CF(cufftExecZ2D((cufftHandle)pb, (cufftDoubleComplex*)spec, (cufftDoubleReal*)grid));
   Cell cell;
   memcpy(cell.H, c->pme_cellbuf, sizeof(cell.H));
   memcpy(cell.Hi, c->pme_cellbuf + 9, sizeof(cell.Hi));
   cell.V = c->pme_cellbuf[18];
 #define PME_GATHER(P_)                                                                         \
-  k_pme_gather<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, grid,            \
-                                                  c->pme_self, c->pme_soff, v, c->rl_cnt,        \
-                                                  c->rl_rows, (const double4*)c->rl_pos, cell,   \
-                                                  (const R*)c->rl_tt, c->rl_cap, o0, o1, o2,     \
-                                                  ostride)
+  k_pme_gather<P_, R><<<g8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, grid,             \
+                                                 c->pme_self, c->pme_soff, v, vr, c->rl_cnt,     \
+                                                 c->rl_rows, (const double4*)c->rl_pos, cell,    \
+                                                 (const R*)c->rl_tt, c->rl_cap, o0, o1, o2,      \
+                                                 ostride, orr)
   switch (p) {
     case 4: PME_GATHER(4); break;
     case 6: PME_GATHER(6); break;
@@ -648,14 +712,26 @@ static int pme_apply_t(bd_ctx* c, const VecIn& v, double* o0, double* o1, double
   return BD_OK;
 }
 
-int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride) {
+static int pme_apply_k(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, double* o1,
+                       double* o2, int ostride, size_t orr) {
   if (!c->pme_ready) return BD_ERR_STATE;
   prof_begin(c, BD_PROF_MATVEC);
-  int s = c->pme_f32 ? pme_apply_t<float, cufftComplex>(c, v, o0, o1, o2, ostride)
-                     : pme_apply_t<double, cufftDoubleComplex>(c, v, o0, o1, o2, ostride);
+  int s = c->pme_f32
+              ? pme_apply_t<float, cufftComplex>(c, k, v, vr, o0, o1, o2, ostride, orr)
+              : pme_apply_t<double, cufftDoubleComplex>(c, k, v, vr, o0, o1, o2, ostride, orr);
   prof_end(c, BD_PROF_MATVEC);
   if (s != BD_OK) return s;
   return launch_ok(c);
+}
+
+int pme_apply(bd_ctx* c, const VecIn& v, double* o0, double* o1, double* o2, int ostride) {
+  return pme_apply_k(c, 1, v, 0, o0, o1, o2, ostride, 0);
+}
+
+int pme_apply_multi(bd_ctx* c, int k, const double* X, size_t xs, double* Y, size_t ys) {
+  int NTp = c->NT * 32;
+  VecIn v = {{X, X + NTp, X + 2 * (size_t)NTp}, 1};
+  return pme_apply_k(c, k, v, xs, Y, Y + NTp, Y + 2 * (size_t)NTp, 1, ys);
 }
 
 }  // namespace bd

@@ -24,11 +24,7 @@
 
 using namespace bd;
 
-#define CU(call)                                  \
-  do {                                            \
-    cudaError_t e_ = (call);                      \
-    if (e_ != cudaSuccess) return BD_ERR_CUDA;    \
-  } while (0)
+#define CU(call) BD_CU(call)
 
 // Free-space RPY block for the pair vector d (unit bead radius):
 // (3/4r + 1/2r^3) I + (3/4r - 3/2r^3) d d^T/r^2 for r >= 2,
@@ -126,11 +122,13 @@ __global__ void __launch_bounds__(128) k_seg_blocks(Lat l, const double* __restr
 // dozen rows.
 __global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ Bm, int S,
                                                      int nblk, int trans,
-                                                     const double* __restrict__ x,
-                                                     double* __restrict__ y, int NTp) {
+                                                     const double* __restrict__ x, size_t xs,
+                                                     double* __restrict__ y, size_t ys, int NTp) {
   int n = 3 * S, lane = threadIdx.x & 31;
   size_t e = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (e >= (size_t)nblk * n) return;
+  x += (size_t)blockIdx.y * xs;  // right-hand side blockIdx.y
+  y += (size_t)blockIdx.y * ys;
   int b = (int)(e / n), i = (int)(e % n);
   const double* Bb = Bm + (size_t)b * n * n;
   const double* xb = x + (size_t)b * S;
@@ -145,9 +143,12 @@ __global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ 
 
 // 3 x 3 bead blocks: one thread per bead.
 __global__ void k_bead_apply(const double* __restrict__ Bm, int N, int trans,
-                             const double* __restrict__ x, double* __restrict__ y, int NTp) {
+                             const double* __restrict__ x, size_t xs, double* __restrict__ y,
+                             size_t ys, int NTp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  x += (size_t)blockIdx.y * xs;  // right-hand side blockIdx.y
+  y += (size_t)blockIdx.y * ys;
   const double* B = Bm + 9 * (size_t)i;
   double v0 = x[i], v1 = x[NTp + i], v2 = x[2 * (size_t)NTp + i];
   for (int p = 0; p < 3; p++) {
@@ -287,19 +288,27 @@ int precond_build(bd_ctx* c, const Lat& l) {
 }
 
 // y = op(G) x (which = 0: G, 1: G^T, 2: G^(-1)) in the Lanczos layout.
-int precond_apply(bd_ctx* c, int which, const double* x, double* y) {
+// y_r = B x_r for k right-hand sides (RHS strides xs, ys); B = G (which 0),
+// G^T (1) or G^-1 (2).
+int precond_apply_k(bd_ctx* c, int which, int k, const double* x, size_t xs, double* y,
+                    size_t ys) {
   int S = c->pre_S, NTp = c->NT * 32;
   const double* Bm = which == 2 ? c->pre_Gi : c->pre_G;
   int trans = which == 1;
   c->launches++;
   if (S == 1) {
-    k_bead_apply<<<(c->N + 127) / 128, 128, 0, c->stream>>>(Bm, c->N, trans, x, y, NTp);
+    k_bead_apply<<<dim3((c->N + 127) / 128, k), 128, 0, c->stream>>>(Bm, c->N, trans, x, xs, y,
+                                                                       ys, NTp);
   } else {
     long long nw = (long long)(c->N / S) * 3 * S;  // one warp per output entry
-    k_block_apply<<<(unsigned)((nw * 32 + 255) / 256), 256, 0, c->stream>>>(Bm, S, c->N / S,
-                                                                             trans, x, y, NTp);
+    k_block_apply<<<dim3((unsigned)((nw * 32 + 255) / 256), k), 256, 0, c->stream>>>(
+        Bm, S, c->N / S, trans, x, xs, y, ys, NTp);
   }
   return BD_OK;
+}
+
+int precond_apply(bd_ctx* c, int which, const double* x, double* y) {
+  return precond_apply_k(c, which, 1, x, 0, y, 0);
 }
 
 void precond_free(bd_ctx* c) {
@@ -337,6 +346,7 @@ int bd_set_preconditioner(bd_ctx* c, int kind, int segment) {
   if (kind == BD_PRECOND_LEARNED && !c->mpnn_ready) return BD_ERR_STATE;
   CU(cudaStreamSynchronize(c->stream));
   lanczos_graphs_reset(c);
+  c->hi_version++;
   c->pre_kind = kind;
   c->pre_S = S;
   c->pre_ready = false;
@@ -363,6 +373,7 @@ int bd_set_precond_blocks(bd_ctx* c, const double* G9) {
   k_bead_invert<<<(c->N + 127) / 128, 128, 0, c->stream>>>(c->pre_G, c->pre_Gi, c->N,
                                                            c->pre_bad);
   lanczos_graphs_reset(c);
+  c->hi_version++;
   c->pre_kind = BD_PRECOND_BLOCKS;
   c->pre_S = 1;
   c->pre_ready = true;
