@@ -355,13 +355,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1):
+def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0):
     """Times K steps of one path after W warm-up steps; returns a dict."""
     import torch
     N = w["Nb"] * w["Nc"]
     pp = PATHS[path]
     nb = noise_block if pp["mobility"] == "pme" else 1
-    c = build_context(w, 1000 + rank, path, noise_block=nb)
+    extra = dict(noise_block=nb, pme_rc=pme_rc) if pp["mobility"] == "pme" else {}
+    c = build_context(w, 1000 + rank, path, **extra)
     step = c.step_lanczos if pp["step"] == "lanczos" else c.step_reference
     step(0, W, True)
     # noise blocks solved during the warm-up are dropped, so the timed steps
@@ -418,7 +419,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1):
         # bead vectors and weights 48 N (s/4) plus 8 passes over 3 grids
         # 96 K^3 (s/4)
         import bd_b200 as B
-        Kg = B.pme_default_grid(w["L"])
+        Kg = B.pme_default_grid(w["L"], pme_rc)
         sb = 8 if pp["precision"] == "fp64" else 4
         alg_bytes = (48 * N + 96 * Kg ** 3) * sb / 4
     else:
@@ -569,7 +570,7 @@ def run_ours(args, rank, world, dist):
     K, W = args.steps, args.warmup
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps, args.noise_block)
+    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps, args.noise_block, args.pme_rc)
     value = world * N * K / (main["t_max_ms"] / 1e3)
     peak, kind = peaks()
     pme = PATHS[args.path]["mobility"] == "pme"
@@ -600,8 +601,9 @@ def run_ours(args, rank, world, dist):
             "dtype": "f32" if PATHS[args.path]["precision"] == "fp32" else "f64",
             "data": "synthetic",
             "config": {"workload": w["name"], "beads": N, "path": args.path,
-                       "mobility": ("Ewald-summed RPY by smooth PME, grid %d^3, order 8, cutoff 10"
-                                    % __import__("bd_b200").pme_default_grid(w["L"]) if pme else
+                       "mobility": ("Ewald-summed RPY by smooth PME, grid %d^3, order 8, cutoff %g"
+                                    % (__import__("bd_b200").pme_default_grid(w["L"], args.pme_rc),
+                                       args.pme_rc) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
                        "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation" +
                                 (", noise blocks of %d steps" % main["block"]["noise_block"]
@@ -653,6 +655,9 @@ def main():
     ap.add_argument("--noise-block", type=int, default=16,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
+    ap.add_argument("--pme-rc", type=float, default=10.0,
+                    help="particle-mesh real-space cutoff; the grid follows it (14.5 L / rc "
+                         "points, constant interpolation accuracy)")
     ap.add_argument("--compare", type=int, default=1,
                     help="also time the plain FP64 Krylov path (reported as plain_fp64)")
     args = ap.parse_args()

@@ -123,7 +123,8 @@ typedef struct {
   double lanczos_tol;        /* relative change of sqrt(M) z between iterations; 0 -> 1e-6 */
   int lanczos_max;           /* Krylov dimension cap, at most 400; 0 -> 200 */
   /* BD_MOB_PME discretisation (no reference counterpart): grid points per
-   * reduced lattice direction (0 -> smallest 2^a 3^b 5^c >= 1.45 L),
+   * reduced lattice direction (0 -> smallest 2^a 3^b 5^c >= 14.5 L / rc,
+   * i.e. 1.45 L at the default cutoff 10: spacing proportional to the cutoff),
    * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> the smaller
    * of 10 and 0.43 L; at most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
    * real-space pairs per bead (0 -> 512). */

@@ -30,7 +30,8 @@
 //    (shear/src/main26.c:1663-1700); the off-diagonal entries of the k-space
 //    self sum, which a sheared or stretched cell makes non-zero, are removed.
 // cuFFT is used for the transforms only.  Spreading uses atomics in the grid
-// precision; several right-hand sides share each launch (blockIdx.y).  The
+// precision (float4 atomics on the interleaved layout); several right-hand
+// sides share each launch.  The
 // spline weights and pair tensors are computed once per step because the
 // positions do not change during a Krylov solve.
 #include <cufft.h>
@@ -78,27 +79,39 @@ __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
   }
 }
 
-// Q[c][g] += v_c(i) W_i(g): one warp per bead, the P^3 stencil points
+// Grid layout of a product of k right-hand sides: the values of one grid
+// point are contiguous, ncp per point, column j = 3 r + c holding component c
+// of right-hand side r (ncp = 3k rounded up to a multiple of 4 in FP32, so a
+// point's row is a whole number of float4; the padding columns stay zero and
+// are not transformed).  The transforms are strided batches (istride = ncp,
+// idist = 1), the spectrum has the same layout.
+__host__ __device__ __forceinline__ int pme_ncp(bool f32, int k) {
+  return f32 ? (3 * k + 3) / 4 * 4 : 3 * k;
+}
+
+constexpr int kMaxNcp = 3 * BD_MAX_NOISE_BLOCK;
+
+// Q[g][3 r + c] += v_r,c(i) W_i(g): one warp per bead, the P^3 stencil points
 // spread over the lanes with the fastest index along the contiguous grid
-// direction, so each atomic instruction of a warp covers runs of P adjacent
-// grid values.  Atomics into the grid.  Right-hand side blockIdx.y reads its
-// vector vr entries further on and owns the grids 3 K^3 entries further on.
+// direction.  The bead's ncp values are staged in shared memory; each grid
+// point takes ncp / 4 float4 atomics (FP32) or 3k scalar atomics (FP64).
 template <int P, typename R>
 __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base,
                                                     const double* __restrict__ w, int N, int K,
-                                                    VecIn v, size_t vr, R* grid) {
-  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+                                                    VecIn v, size_t vr, int k, int ncp, R* grid) {
+  __shared__ __align__(16) R sf[8][kMaxNcp];
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   if (i >= N) return;
-  size_t ro = (size_t)blockIdx.y * vr;
-  grid += (size_t)blockIdx.y * 3 * ((size_t)K * K * K);
-  double f0 = v.p[0][ro + (size_t)i * v.stride];
-  double f1 = v.p[1][ro + (size_t)i * v.stride];
-  double f2 = v.p[2][ro + (size_t)i * v.stride];
+  for (int j = lane; j < ncp; j += 32) {
+    int c3 = j % 3;
+    const double* pc = c3 == 0 ? v.p[0] : (c3 == 1 ? v.p[1] : v.p[2]);
+    sf[wp][j] = j < 3 * k ? (R)pc[(size_t)(j / 3) * vr + (size_t)i * v.stride] : (R)0;
+  }
+  __syncwarp();
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
   int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
-  size_t K3 = (size_t)K * K * K;
   // fully unrolled: the stencil index of each lane is a compile-time
   // function of the iteration, so the weights stay in registers
 #pragma unroll
@@ -112,9 +125,18 @@ __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base
     g2 += g2 < 0 ? K : 0;
     double wt = w0[a] * w1[b] * w2[c];
     size_t g = ((size_t)g0 * K + g1) * K + g2;
-    atomicAdd(grid + g, (R)(wt * f0));
-    atomicAdd(grid + K3 + g, (R)(wt * f1));
-    atomicAdd(grid + 2 * K3 + g, (R)(wt * f2));
+    if constexpr (sizeof(R) == 4) {
+      float wf = (float)wt;
+      float4* dst = (float4*)(grid + g * ncp);
+      const float4* src = (const float4*)sf[wp];
+      for (int e = 0; e < ncp / 4; e++) {
+        float4 f = src[e];
+        atomicAdd(dst + e, make_float4(wf * f.x, wf * f.y, wf * f.z, wf * f.w));
+      }
+    } else {
+      R* dst = grid + g * ncp;
+      for (int e = 0; e < ncp; e++) atomicAdd(dst + e, wt * sf[wp][e]);
+    }
   }
 }
 
@@ -194,14 +216,18 @@ __global__ void k_pme_soff_fin(const double* __restrict__ part, int nb, double* 
   if (threadIdx.x < 3) soff[threadIdx.x] = red[threadIdx.x][0];
 }
 
-// Right-hand side blockIdx.y owns the spectra 3 n entries further on.
+// One thread per (spectrum point m, right-hand side r), r fastest: the three
+// components of r at m are columns 3 r .. 3 r + 2 of row m (ncp per row).
 template <typename R, typename Cx>
-__global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size_t n) {
+__global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size_t n, int k,
+                                      int ncp) {
   size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  spec += (size_t)blockIdx.y * 3 * n;
-  const R* t = infl + 6 * e;
-  Cx x = spec[e], y = spec[n + e], z = spec[2 * n + e];
+  if (e >= n * k) return;
+  size_t m = e / k;
+  int r = (int)(e % k);
+  const R* t = infl + 6 * m;
+  Cx* sp = spec + m * ncp + 3 * r;
+  Cx x = sp[0], y = sp[1], z = sp[2];
   Cx u, v, w;
   u.x = t[0] * x.x + t[1] * y.x + t[2] * z.x;
   u.y = t[0] * x.y + t[1] * y.y + t[2] * z.y;
@@ -209,9 +235,9 @@ __global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size
   v.y = t[1] * x.y + t[3] * y.y + t[4] * z.y;
   w.x = t[2] * x.x + t[4] * y.x + t[5] * z.x;
   w.y = t[2] * x.y + t[4] * y.y + t[5] * z.y;
-  spec[e] = u;
-  spec[n + e] = v;
-  spec[2 * n + e] = w;
+  sp[0] = u;
+  sp[1] = v;
+  sp[2] = w;
 }
 
 // Real-space Beenakker kernel t1 I + t2 r r^T/r^2 (shear/src/main26.c:
@@ -262,36 +288,34 @@ __device__ __forceinline__ void pair_terms(double alpha, double alpha_ref, doubl
   }
 }
 
-// out_c(i) = sum_g W_i(g) grid_c(g) + self * v_c(i) - S_off v(i)
-//            + sum_j T_ij v_j (row list)
-// One warp per bead: lanes share the stencil points and the pair row, then a
-// butterfly reduction.  Right-hand side blockIdx.y: input vr, output orr
-// entries further on, grids 3 K^3 further on.
-template <int P, typename R>
+// out_r,c(i) = sum_g W_i(g) Q[g][3 r + c] + self v_r,c(i) - (S_off v_r(i))_c
+//              + sum_j (T_ij v_r,j)_c (row list)
+// for the right-hand sides r0 .. r0 + kc - 1 of chunk blockIdx.y (r0 =
+// KG blockIdx.y, KG = 1 for single products, kGatherRhs otherwise).  One warp
+// per bead: the lanes share the stencil points (float4 reads of the chunk's
+// columns in FP32) and the pair row (the pair data read once for every
+// right-hand side of the chunk), then a butterfly reduction and lane e writes
+// column e.
+constexpr int kGatherRhs = 8;
+
+template <int P, typename R, int KG>
 __global__ void __launch_bounds__(256) k_pme_gather(
     const int* __restrict__ base, const double* __restrict__ w, int N, int K,
-    const R* __restrict__ grid, double self, const double* __restrict__ soff, VecIn v, size_t vr,
-    const int* __restrict__ rcnt, const int* __restrict__ rrows,
+    const R* __restrict__ grid, int k, int ncp, double self, const double* __restrict__ soff,
+    VecIn v, size_t vr, const int* __restrict__ rcnt, const int* __restrict__ rrows,
     const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
     double* o0, double* o1, double* o2, int ostride, size_t orr) {
+  constexpr int NA = 3 * KG, NA4 = (NA + 3) / 4 * 4;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
-  {
-    size_t ro = (size_t)blockIdx.y * vr, oo = (size_t)blockIdx.y * orr;
-    v.p[0] += ro;
-    v.p[1] += ro;
-    v.p[2] += ro;
-    o0 += oo;
-    o1 += oo;
-    o2 += oo;
-    grid += (size_t)blockIdx.y * 3 * ((size_t)K * K * K);
-  }
+  int r0 = KG * blockIdx.y, kc = min(KG, k - r0), nj = 3 * kc;
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
   int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
-  size_t K3 = (size_t)K * K * K;
-  double u0 = 0, u1 = 0, u2 = 0;
+  double u[NA4];
+#pragma unroll
+  for (int e = 0; e < NA4; e++) u[e] = 0.0;
 #pragma unroll
   for (int it = 0; it < (P * P * P + 31) / 32; it++) {
     int q = lane + 32 * it;
@@ -302,23 +326,40 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     g1 += g1 < 0 ? K : 0;
     g2 += g2 < 0 ? K : 0;
     double wt = w0[a] * w1[b] * w2[c];
-    size_t g = ((size_t)g0 * K + g1) * K + g2;
-    u0 += wt * (double)grid[g];
-    u1 += wt * (double)grid[K3 + g];
-    u2 += wt * (double)grid[2 * K3 + g];
+    const R* row = grid + (((size_t)g0 * K + g1) * K + g2) * ncp + 3 * r0;
+    if constexpr (sizeof(R) == 4) {
+      // 3 r0 is a multiple of 4 (r0 a multiple of 8, or 0); the chunk's
+      // columns round up to whole float4 within the row (padding reads zeros
+      // or the next chunk's columns, which are not written out)
+#pragma unroll
+      for (int e = 0; e < NA4 / 4; e++) {
+        if (4 * e >= nj) break;
+        float4 x = ((const float4*)row)[e];
+        u[4 * e] += wt * x.x;
+        u[4 * e + 1] += wt * x.y;
+        u[4 * e + 2] += wt * x.z;
+        u[4 * e + 3] += wt * x.w;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < NA; e++) {
+        if (e >= nj) break;
+        u[e] += wt * row[e];
+      }
+    }
   }
   // real-space pairs: the tensor t1 I + t2 d d^T/r^2 of the minimum-image
   // displacement d; t1 and t2/r^2 are stored per pair (8 or 16 bytes), d is
   // recomputed from the frozen lab-frame positions (L2-resident)
   int n = rcnt[i];
-  const int* row = rrows + (size_t)i * rcap;
+  const int* prow = rrows + (size_t)i * rcap;
   // the cell is (b1, b2) in the xy plane and L e_z: a 2 x 2 block and L
   double4 pi = pos[i];
   const double h00 = cell.H[0], h01 = cell.H[1], h10 = cell.H[3], h11 = cell.H[4];
   const double g00 = cell.Hi[0], g01 = cell.Hi[1], g10 = cell.Hi[3], g11 = cell.Hi[4];
   const double Lz = cell.H[8], iLz = cell.Hi[8];
-  for (int k = lane; k < n; k += 32) {
-    int j = row[k];
+  for (int kk = lane; kk < n; kk += 32) {
+    int j = prow[kk];
     double4 pj = pos[j];
     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
     double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
@@ -328,28 +369,44 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     dx = h00 * s0 + h01 * s1;
     dy = h10 * s0 + h11 * s1;
     dz = Lz * s2;
-    const R* tk = tt + 2 * ((size_t)i * rcap + k);
+    const R* tk = tt + 2 * ((size_t)i * rcap + kk);
     double t1 = tk[0], t2r = tk[1];  // t1 and t2 / r^2 of the pair
-    double x0 = v.p[0][(size_t)j * v.stride], x1 = v.p[1][(size_t)j * v.stride];
-    double x2 = v.p[2][(size_t)j * v.stride];
-    double q = t2r * (dx * x0 + dy * x1 + dz * x2);
-    u0 += t1 * x0 + q * dx;
-    u1 += t1 * x1 + q * dy;
-    u2 += t1 * x2 + q * dz;
+#pragma unroll
+    for (int r = 0; r < KG; r++) {
+      if (r >= kc) break;
+      size_t o = (size_t)(r0 + r) * vr + (size_t)j * v.stride;
+      double x0 = v.p[0][o], x1 = v.p[1][o], x2 = v.p[2][o];
+      double qq = t2r * (dx * x0 + dy * x1 + dz * x2);
+      u[3 * r] += t1 * x0 + qq * dx;
+      u[3 * r + 1] += t1 * x1 + qq * dy;
+      u[3 * r + 2] += t1 * x2 + qq * dz;
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    u0 += __shfl_xor_sync(0xffffffffu, u0, o);
-    u1 += __shfl_xor_sync(0xffffffffu, u1, o);
-    u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+  for (int e = 0; e < NA; e++) {
+    if (e >= nj) break;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) u[e] += __shfl_xor_sync(0xffffffffu, u[e], o);
   }
-  if (lane == 0) {
-    double vi0 = v.p[0][(size_t)i * v.stride], vi1 = v.p[1][(size_t)i * v.stride];
-    double vi2 = v.p[2][(size_t)i * v.stride];
+  // lane e < 3 kc writes column e: component c of right-hand side r0 + r
+  double mine = 0.0;
+#pragma unroll
+  for (int e = 0; e < NA; e++)
+    if (e == lane) mine = u[e];
+  if (lane < nj) {
+    int r = lane / 3, c = lane % 3;
+    size_t o = (size_t)(r0 + r) * vr + (size_t)i * v.stride;
+    double vi0 = v.p[0][o], vi1 = v.p[1][o], vi2 = v.p[2][o];
     double sxy = soff[0], sxz = soff[1], syz = soff[2];
-    o0[(size_t)i * ostride] = u0 + self * vi0 - sxy * vi1 - sxz * vi2;
-    o1[(size_t)i * ostride] = u1 + self * vi1 - sxy * vi0 - syz * vi2;
-    o2[(size_t)i * ostride] = u2 + self * vi2 - sxz * vi0 - syz * vi1;
+    double out;
+    if (c == 0)
+      out = mine + self * vi0 - sxy * vi1 - sxz * vi2;
+    else if (c == 1)
+      out = mine + self * vi1 - sxy * vi0 - syz * vi2;
+    else
+      out = mine + self * vi2 - sxz * vi0 - syz * vi1;
+    double* dst = c == 0 ? o0 : (c == 1 ? o1 : o2);
+    dst[(size_t)(r0 + r) * orr + (size_t)i * ostride] = out;
   }
 }
 
@@ -469,6 +526,8 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, i
 
 namespace bd {
 
+static int pme_plans(bd_ctx* c, int k, int* bk);
+
 int pme_alloc(bd_ctx* c) {
   if (c->pme_grid) return BD_OK;
   int K = c->pmeK, N = c->N;
@@ -476,9 +535,9 @@ int pme_alloc(bd_ctx* c) {
   c->pme_f32 = c->p.precision == BD_PREC_FP32;
   size_t es = c->pme_f32 ? 4 : 8;  // grid, spectrum, influence and pair tensors
   // grids and spectra for the largest number of right-hand sides of a product
-  size_t nr = (size_t)std::max(1, c->nbk);
-  CU(cudaMalloc(&c->pme_grid, es * 3 * K3 * nr));
-  CU(cudaMalloc(&c->pme_spec, 2 * es * 3 * Ks * nr));
+  size_t nr = (size_t)pme_ncp(c->pme_f32, std::max(1, c->nbk));
+  CU(cudaMalloc(&c->pme_grid, es * K3 * nr));
+  CU(cudaMalloc(&c->pme_spec, 2 * es * Ks * nr));
   CU(cudaMalloc(&c->pme_infl, es * 6 * Ks));
   CU(cudaMalloc(&c->pme_bsq, 8 * 3 * (size_t)K));
   c->pme_nblk = (int)((Ks + 255) / 256);
@@ -497,19 +556,13 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_cell_start, 4 * (size_t)(c->rl_ncell_cap + 1)));
   CU(cudaMalloc(&c->rl_cursor, 4 * (size_t)c->rl_ncell_cap));
   CU(cudaMemsetAsync(c->rl_cell_count, 0, 4 * (size_t)c->rl_ncell_cap, c->stream));
-  c->bytes += es * (3 * K3 * nr + 6 * Ks * nr + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
+  c->bytes += es * (K3 * nr + 2 * Ks * nr + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
               24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 2 * es) + 32 * (size_t)N +
               8 * (size_t)N + 12 * (size_t)c->rl_ncell_cap;
-  int n[3] = {K, K, K};
-  cufftHandle f, b;
-  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
-                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3));
-  CF(cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
-                   c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3));
-  CF(cufftSetStream(f, c->stream));
-  CF(cufftSetStream(b, c->stream));
-  c->pme_plan_f = (int)f;
-  c->pme_plan_b = (int)b;
+  int f, b;
+  if ((f = pme_plans(c, 1, &b)) < 0) return BD_ERR_CUDA;
+  c->pme_plan_f = f;
+  c->pme_plan_b = b;
   std::vector<double> bs(3 * (size_t)K);
   bspline_moduli(K, c->pme_p, bs.data());
   for (int d = 1; d < 3; d++)
@@ -519,8 +572,33 @@ int pme_alloc(bd_ctx* c) {
   return BD_OK;
 }
 
-// Batched transforms of 3 k grids, created outside any stream capture and
-// kept for up to four values of k (replacing one drops the captured
+// Forward and inverse transforms of the 3 k columns of a k-right-hand-side
+// grid (strided batches: istride = ncp, idist = 1); returns the forward plan
+// (the inverse in *bk) or -1.
+static int pme_plans(bd_ctx* c, int k, int* bk) {
+  int K = c->pmeK, Kh = K / 2 + 1, ncp = pme_ncp(c->pme_f32, k);
+  int n[3] = {K, K, K}, re[3] = {K, K, K}, cx[3] = {K, K, Kh};
+  cufftHandle f, b;
+  if (cufftPlanMany(&f, 3, n, re, ncp, 1, cx, ncp, 1, c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z,
+                    3 * k) != CUFFT_SUCCESS)
+    return -1;
+  if (cufftPlanMany(&b, 3, n, cx, ncp, 1, re, ncp, 1, c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D,
+                    3 * k) != CUFFT_SUCCESS) {
+    cufftDestroy(f);
+    return -1;
+  }
+  if (cufftSetStream(f, c->stream) != CUFFT_SUCCESS ||
+      cufftSetStream(b, c->stream) != CUFFT_SUCCESS) {
+    cufftDestroy(f);
+    cufftDestroy(b);
+    return -1;
+  }
+  *bk = (int)b;
+  return (int)f;
+}
+
+// Batched transforms of the 3 k columns, created outside any stream capture
+// and kept for up to four values of k (replacing one drops the captured
 // iterations that use it).
 int pme_multi_plan(bd_ctx* c, int k) {
   int slot = -1;
@@ -535,21 +613,10 @@ int pme_multi_plan(bd_ctx* c, int k) {
     cufftDestroy((cufftHandle)c->pme_mplan_b[slot]);
     c->pme_mplan_k[slot] = 0;
   }
-  int K = c->pmeK;
-  size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
-  int n[3] = {K, K, K};
-  cufftHandle f, b;
-  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
-                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3 * k));
-  if (cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
-                    c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3 * k) != CUFFT_SUCCESS) {
-    cufftDestroy(f);
-    return BD_ERR_CUDA;
-  }
-  CF(cufftSetStream(f, c->stream));
-  CF(cufftSetStream(b, c->stream));
-  c->pme_mplan_f[slot] = (int)f;
-  c->pme_mplan_b[slot] = (int)b;
+  int f, b;
+  if ((f = pme_plans(c, k, &b)) < 0) return BD_ERR_CUDA;
+  c->pme_mplan_f[slot] = f;
+  c->pme_mplan_b[slot] = b;
   c->pme_mplan_k[slot] = k;
   return BD_OK;
 }
@@ -672,11 +739,13 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   }
   R* grid = (R*)c->pme_grid;
   Cx* spec = (Cx*)c->pme_spec;
-  CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3 * k, c->stream));
+  int ncp = pme_ncp(sizeof(R) == 4, k);
+  CU(cudaMemsetAsync(grid, 0, sizeof(R) * K3 * ncp, c->stream));
   c->launches += 3;  // spread, influence, gather (the transforms are cuFFT's)
-  dim3 g8(nblk(N, 8), k);
-#define PME_SPREAD(P_) \
-  k_pme_spread<P_, R><<<g8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, grid)
+  int nb8 = nblk(N, 8);
+#define PME_SPREAD(P_)                                                                  \
+  k_pme_spread<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, ncp, \
+                                                  grid)
   switch (p) {
     case 4: PME_SPREAD(4); break;
     case 6: PME_SPREAD(6); break;
@@ -687,8 +756,8 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
     CF(cufftExecR2C((cufftHandle)pf, (cufftReal*)grid, (cufftComplex*)spec));
   else
     CF(cufftExecD2Z((cufftHandle)pf, (cufftDoubleReal*)grid, (cufftDoubleComplex*)spec));
-  k_pme_apply_influence<R, Cx><<<dim3(nblk((long long)Ks, 256), k), 256, 0, c->stream>>>(
-      (const R*)c->pme_infl, spec, Ks);
+  k_pme_apply_influence<R, Cx><<<nblk((long long)Ks * k, 256), 256, 0, c->stream>>>(
+      (const R*)c->pme_infl, spec, Ks, k, ncp);
   if constexpr (sizeof(R) == 4)
     CF(cufftExecC2R((cufftHandle)pb, (cufftComplex*)spec, (cufftReal*)grid));
   else
@@ -697,12 +766,18 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   memcpy(cell.H, c->pme_cellbuf, sizeof(cell.H));
   memcpy(cell.Hi, c->pme_cellbuf + 9, sizeof(cell.Hi));
   cell.V = c->pme_cellbuf[18];
-#define PME_GATHER(P_)                                                                         \
-  k_pme_gather<P_, R><<<g8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, grid,             \
-                                                 c->pme_self, c->pme_soff, v, vr, c->rl_cnt,     \
-                                                 c->rl_rows, (const double4*)c->rl_pos, cell,    \
-                                                 (const R*)c->rl_tt, c->rl_cap, o0, o1, o2,      \
-                                                 ostride, orr)
+  dim3 gg(nb8, (k + kGatherRhs - 1) / kGatherRhs);
+#define PME_GATHER(P_)                                                                          \
+  if (k == 1)                                                                                   \
+    k_pme_gather<P_, R, 1><<<nb8, 256, 0, c->stream>>>(                                         \
+        c->pme_base, c->pme_w, N, K, grid, k, ncp, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,  \
+        c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
+        ostride, orr);                                                                          \
+  else                                                                                          \
+    k_pme_gather<P_, R, kGatherRhs><<<gg, 256, 0, c->stream>>>(                                 \
+        c->pme_base, c->pme_w, N, K, grid, k, ncp, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,  \
+        c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
+        ostride, orr)
   switch (p) {
     case 4: PME_GATHER(4); break;
     case 6: PME_GATHER(6); break;

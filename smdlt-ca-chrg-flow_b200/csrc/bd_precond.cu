@@ -115,30 +115,36 @@ __global__ void __launch_bounds__(128) k_seg_blocks(Lat l, const double* __restr
   if (t == 0 && fail) atomicAdd(bad, 1);
 }
 
-// y = op(B_b) x for every block; x, y in the Lanczos layout (component-major,
-// 3 x NTp).  One warp per output entry (block b, row i of op(B_b)): the lanes
-// split the 3S products of the row (trans = 0) or column (trans = 1) and a
-// butterfly adds them, which keeps enough loads in flight for blocks of a few
-// dozen rows.
-__global__ void __launch_bounds__(256) k_block_apply(const double* __restrict__ Bm, int S,
-                                                     int nblk, int trans,
+// y_r = op(B_b) x_r for every block b and right-hand side r < k; x, y in the
+// Lanczos layout (component-major, 3 x NTp, right-hand sides xs / ys apart).
+// One CTA per block: B_b (stored transposed for op = B, as is for op = B^T,
+// so that the threads of consecutive rows read consecutive words) and the
+// block's slices of the k inputs are staged in shared memory once, so each
+// block matrix is read from memory once for all right-hand sides.  Each output
+// sums its row in a fixed order.
+__global__ void __launch_bounds__(128) k_block_apply(const double* __restrict__ Bm, int S,
+                                                     int trans, int k,
                                                      const double* __restrict__ x, size_t xs,
                                                      double* __restrict__ y, size_t ys, int NTp) {
-  int n = 3 * S, lane = threadIdx.x & 31;
-  size_t e = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (e >= (size_t)nblk * n) return;
-  x += (size_t)blockIdx.y * xs;  // right-hand side blockIdx.y
-  y += (size_t)blockIdx.y * ys;
-  int b = (int)(e / n), i = (int)(e % n);
+  extern __shared__ double sm[];
+  int n = 3 * S, b = blockIdx.x;
+  double* Bs = sm;          // Bs[q * n + i] = op(B_b)[i][q]
+  double* xv = sm + n * n;  // k x n inputs
   const double* Bb = Bm + (size_t)b * n * n;
-  const double* xb = x + (size_t)b * S;
-  double s = 0;
-  for (int k = lane; k < n; k += 32) {
-    double m = trans ? Bb[(size_t)k * n + i] : Bb[(size_t)i * n + k];
-    s += m * xb[(size_t)(k % 3) * NTp + k / 3];
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x)
+    Bs[trans ? e : (e % n) * n + e / n] = Bb[e];
+  for (int e = threadIdx.x; e < k * n; e += blockDim.x) {
+    int r = e / n, q = e % n;
+    xv[e] = x[(size_t)r * xs + (size_t)(q % 3) * NTp + (size_t)b * S + q / 3];
   }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) y[(size_t)(i % 3) * NTp + (size_t)b * S + i / 3] = s;
+  __syncthreads();
+  for (int e = threadIdx.x; e < k * n; e += blockDim.x) {
+    int r = e / n, i = e % n;
+    const double* xr = xv + r * n;
+    double s = 0;
+    for (int q = 0; q < n; q++) s += Bs[q * n + i] * xr[q];
+    y[(size_t)r * ys + (size_t)(i % 3) * NTp + (size_t)b * S + i / 3] = s;
+  }
 }
 
 // 3 x 3 bead blocks: one thread per bead.
@@ -300,9 +306,10 @@ int precond_apply_k(bd_ctx* c, int which, int k, const double* x, size_t xs, dou
     k_bead_apply<<<dim3((c->N + 127) / 128, k), 128, 0, c->stream>>>(Bm, c->N, trans, x, xs, y,
                                                                        ys, NTp);
   } else {
-    long long nw = (long long)(c->N / S) * 3 * S;  // one warp per output entry
-    k_block_apply<<<dim3((unsigned)((nw * 32 + 255) / 256), k), 256, 0, c->stream>>>(
-        Bm, S, c->N / S, trans, x, xs, y, ys, NTp);
+    size_t smem = 8 * (size_t)(3 * S) * (3 * S + k);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_block_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_block_apply<<<c->N / S, 128, smem, c->stream>>>(Bm, S, trans, k, x, xs, y, ys, NTp);
   }
   return BD_OK;
 }
