@@ -633,7 +633,7 @@ def run_ours(args, rank, world, dist):
     plain = "pme64" if pme else "lanczos64"
     if args.compare and args.path != plain:
         # the plain method: same mobility in FP64, no preconditioner
-        ref64 = measure(w, plain, K, W, rank, dist, 1)
+        ref64 = measure(w, plain, K, W, rank, dist, 1, 1, args.pme_rc)
         line["plain_fp64"] = {"path": plain, "value": world * N * K / (ref64["t_max_ms"] / 1e3),
                               "ms_per_step": ref64["t_max_ms"] / K,
                               "lanczos_iters_per_step": ref64["lanczos_iters_per_step"],
@@ -652,10 +652,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--path", choices=sorted(PATHS), default="pme32-learned")
-    ap.add_argument("--noise-block", type=int, default=16,
+    ap.add_argument("--noise-block", type=int, default=8,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
-    ap.add_argument("--pme-rc", type=float, default=10.0,
+    ap.add_argument("--pme-rc", type=float, default=11.0,
                     help="particle-mesh real-space cutoff; the grid follows it (14.5 L / rc "
                          "points, constant interpolation accuracy)")
     ap.add_argument("--compare", type=int, default=1,

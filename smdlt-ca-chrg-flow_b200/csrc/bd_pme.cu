@@ -30,8 +30,7 @@
 //    (shear/src/main26.c:1663-1700); the off-diagonal entries of the k-space
 //    self sum, which a sheared or stretched cell makes non-zero, are removed.
 // cuFFT is used for the transforms only.  Spreading uses atomics in the grid
-// precision (float4 atomics on the interleaved layout); several right-hand
-// sides share each launch.  The
+// precision; several right-hand sides share each launch (blockIdx.y).  The
 // spline weights and pair tensors are computed once per step because the
 // positions do not change during a Krylov solve.
 #include <cufft.h>
@@ -79,35 +78,33 @@ __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
   }
 }
 
-// Grid layout of a product of k right-hand sides: the values of one grid
-// point are contiguous, ncp per point, column j = 3 r + c holding component c
-// of right-hand side r (ncp = 3k rounded up to a multiple of 4 in FP32, so a
-// point's row is a whole number of float4; the padding columns stay zero and
-// are not transformed).  The transforms are strided batches (istride = ncp,
-// idist = 1), the spectrum has the same layout.
-__host__ __device__ __forceinline__ int pme_ncp(bool f32, int k) {
-  return f32 ? (3 * k + 3) / 4 * 4 : 3 * k;
-}
+// Q_r[c][g] += v_r,c(i) W_i(g) for the right-hand sides r0 .. r0 + kc - 1
+// of chunk blockIdx.y (r0 = KS blockIdx.y; KS = 1 for single products): one
+// warp per bead, the P^3 stencil points spread over the lanes with the
+// fastest index along the contiguous grid direction, so each atomic
+// instruction of a warp covers runs of P adjacent grid values; the weights
+// and the bead's values are loaded once for the chunk.  Right-hand side r
+// reads its vector vr entries further on and owns the grids 3 K^3 entries
+// further on.
+constexpr int kGatherChunk = 2;  // right-hand sides per interpolating warp
 
-constexpr int kMaxNcp = 3 * BD_MAX_NOISE_BLOCK;
-
-// Q[g][3 r + c] += v_r,c(i) W_i(g): one warp per bead, the P^3 stencil points
-// spread over the lanes with the fastest index along the contiguous grid
-// direction.  The bead's ncp values are staged in shared memory; each grid
-// point takes ncp / 4 float4 atomics (FP32) or 3k scalar atomics (FP64).
-template <int P, typename R>
+template <int P, typename R, int KS>
 __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base,
                                                     const double* __restrict__ w, int N, int K,
-                                                    VecIn v, size_t vr, int k, int ncp, R* grid) {
-  __shared__ __align__(16) R sf[8][kMaxNcp];
-  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+                                                    VecIn v, size_t vr, int k, R* grid) {
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
-  for (int j = lane; j < ncp; j += 32) {
-    int c3 = j % 3;
-    const double* pc = c3 == 0 ? v.p[0] : (c3 == 1 ? v.p[1] : v.p[2]);
-    sf[wp][j] = j < 3 * k ? (R)pc[(size_t)(j / 3) * vr + (size_t)i * v.stride] : (R)0;
+  int r0 = KS * blockIdx.y, kc = min(KS, k - r0);
+  size_t K3 = (size_t)K * K * K;
+  R f[3 * KS];
+#pragma unroll
+  for (int r = 0; r < KS; r++) {
+    size_t o = (size_t)(r0 + (r < kc ? r : 0)) * vr + (size_t)i * v.stride;
+    f[3 * r] = (R)v.p[0][o];
+    f[3 * r + 1] = (R)v.p[1][o];
+    f[3 * r + 2] = (R)v.p[2][o];
   }
-  __syncwarp();
+  R* g0p = grid + (size_t)r0 * 3 * K3;
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
@@ -124,18 +121,21 @@ __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base
     g1 += g1 < 0 ? K : 0;
     g2 += g2 < 0 ? K : 0;
     double wt = w0[a] * w1[b] * w2[c];
+    R wr = (R)wt;
     size_t g = ((size_t)g0 * K + g1) * K + g2;
-    if constexpr (sizeof(R) == 4) {
-      float wf = (float)wt;
-      float4* dst = (float4*)(grid + g * ncp);
-      const float4* src = (const float4*)sf[wp];
-      for (int e = 0; e < ncp / 4; e++) {
-        float4 f = src[e];
-        atomicAdd(dst + e, make_float4(wf * f.x, wf * f.y, wf * f.z, wf * f.w));
+#pragma unroll
+    for (int r = 0; r < KS; r++) {
+      if (r >= kc) break;
+      R* gr = g0p + (size_t)r * 3 * K3 + g;
+      if constexpr (sizeof(R) == 8) {
+        atomicAdd(gr, wt * f[3 * r]);
+        atomicAdd(gr + K3, wt * f[3 * r + 1]);
+        atomicAdd(gr + 2 * K3, wt * f[3 * r + 2]);
+      } else {
+        atomicAdd(gr, wr * f[3 * r]);
+        atomicAdd(gr + K3, wr * f[3 * r + 1]);
+        atomicAdd(gr + 2 * K3, wr * f[3 * r + 2]);
       }
-    } else {
-      R* dst = grid + g * ncp;
-      for (int e = 0; e < ncp; e++) atomicAdd(dst + e, wt * sf[wp][e]);
     }
   }
 }
@@ -216,18 +216,14 @@ __global__ void k_pme_soff_fin(const double* __restrict__ part, int nb, double* 
   if (threadIdx.x < 3) soff[threadIdx.x] = red[threadIdx.x][0];
 }
 
-// One thread per (spectrum point m, right-hand side r), r fastest: the three
-// components of r at m are columns 3 r .. 3 r + 2 of row m (ncp per row).
+// Right-hand side blockIdx.y owns the spectra 3 n entries further on.
 template <typename R, typename Cx>
-__global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size_t n, int k,
-                                      int ncp) {
+__global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size_t n) {
   size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * k) return;
-  size_t m = e / k;
-  int r = (int)(e % k);
-  const R* t = infl + 6 * m;
-  Cx* sp = spec + m * ncp + 3 * r;
-  Cx x = sp[0], y = sp[1], z = sp[2];
+  if (e >= n) return;
+  spec += (size_t)blockIdx.y * 3 * n;
+  const R* t = infl + 6 * e;
+  Cx x = spec[e], y = spec[n + e], z = spec[2 * n + e];
   Cx u, v, w;
   u.x = t[0] * x.x + t[1] * y.x + t[2] * z.x;
   u.y = t[0] * x.y + t[1] * y.y + t[2] * z.y;
@@ -235,9 +231,9 @@ __global__ void k_pme_apply_influence(const R* __restrict__ infl, Cx* spec, size
   v.y = t[1] * x.y + t[3] * y.y + t[4] * z.y;
   w.x = t[2] * x.x + t[4] * y.x + t[5] * z.x;
   w.y = t[2] * x.y + t[4] * y.y + t[5] * z.y;
-  sp[0] = u;
-  sp[1] = v;
-  sp[2] = w;
+  spec[e] = u;
+  spec[n + e] = v;
+  spec[2 * n + e] = w;
 }
 
 // Real-space Beenakker kernel t1 I + t2 r r^T/r^2 (shear/src/main26.c:
@@ -288,34 +284,34 @@ __device__ __forceinline__ void pair_terms(double alpha, double alpha_ref, doubl
   }
 }
 
-// out_r,c(i) = sum_g W_i(g) Q[g][3 r + c] + self v_r,c(i) - (S_off v_r(i))_c
+// out_r,c(i) = sum_g W_i(g) grid_r,c(g) + self v_r,c(i) - (S_off v_r(i))_c
 //              + sum_j (T_ij v_r,j)_c (row list)
 // for the right-hand sides r0 .. r0 + kc - 1 of chunk blockIdx.y (r0 =
-// KG blockIdx.y, KG = 1 for single products, kGatherRhs otherwise).  One warp
-// per bead: the lanes share the stencil points (float4 reads of the chunk's
-// columns in FP32) and the pair row (the pair data read once for every
-// right-hand side of the chunk), then a butterfly reduction and lane e writes
-// column e.
-constexpr int kGatherRhs = 8;
-
+// KG blockIdx.y; KG = 1 for single products).  One warp per bead: the lanes
+// share the stencil points (weights computed once for the chunk) and the pair
+// row (pair terms, positions and minimum image once for the chunk), then a
+// butterfly reduction; lane e < 3 kc writes component e % 3 of right-hand
+// side r0 + e / 3.
 template <int P, typename R, int KG>
 __global__ void __launch_bounds__(256) k_pme_gather(
     const int* __restrict__ base, const double* __restrict__ w, int N, int K,
-    const R* __restrict__ grid, int k, int ncp, double self, const double* __restrict__ soff,
-    VecIn v, size_t vr, const int* __restrict__ rcnt, const int* __restrict__ rrows,
+    const R* __restrict__ grid, int k, double self, const double* __restrict__ soff, VecIn v,
+    size_t vr, const int* __restrict__ rcnt, const int* __restrict__ rrows,
     const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
     double* o0, double* o1, double* o2, int ostride, size_t orr) {
-  constexpr int NA = 3 * KG, NA4 = (NA + 3) / 4 * 4;
+  constexpr int NA = 3 * KG;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
   int r0 = KG * blockIdx.y, kc = min(KG, k - r0), nj = 3 * kc;
+  size_t K3 = (size_t)K * K * K;
+  const R* gbase = grid + (size_t)r0 * 3 * K3;
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
   const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
   int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
-  double u[NA4];
+  double u[NA];
 #pragma unroll
-  for (int e = 0; e < NA4; e++) u[e] = 0.0;
+  for (int e = 0; e < NA; e++) u[e] = 0.0;
 #pragma unroll
   for (int it = 0; it < (P * P * P + 31) / 32; it++) {
     int q = lane + 32 * it;
@@ -326,26 +322,14 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     g1 += g1 < 0 ? K : 0;
     g2 += g2 < 0 ? K : 0;
     double wt = w0[a] * w1[b] * w2[c];
-    const R* row = grid + (((size_t)g0 * K + g1) * K + g2) * ncp + 3 * r0;
-    if constexpr (sizeof(R) == 4) {
-      // 3 r0 is a multiple of 4 (r0 a multiple of 8, or 0); the chunk's
-      // columns round up to whole float4 within the row (padding reads zeros
-      // or the next chunk's columns, which are not written out)
+    const R* gp = gbase + ((size_t)g0 * K + g1) * K + g2;
 #pragma unroll
-      for (int e = 0; e < NA4 / 4; e++) {
-        if (4 * e >= nj) break;
-        float4 x = ((const float4*)row)[e];
-        u[4 * e] += wt * x.x;
-        u[4 * e + 1] += wt * x.y;
-        u[4 * e + 2] += wt * x.z;
-        u[4 * e + 3] += wt * x.w;
-      }
-    } else {
-#pragma unroll
-      for (int e = 0; e < NA; e++) {
-        if (e >= nj) break;
-        u[e] += wt * row[e];
-      }
+    for (int r = 0; r < KG; r++) {
+      if (r >= kc) break;
+      const R* gr = gp + (size_t)r * 3 * K3;
+      u[3 * r] += wt * (double)gr[0];
+      u[3 * r + 1] += wt * (double)gr[K3];
+      u[3 * r + 2] += wt * (double)gr[2 * K3];
     }
   }
   // real-space pairs: the tensor t1 I + t2 d d^T/r^2 of the minimum-image
@@ -388,7 +372,6 @@ __global__ void __launch_bounds__(256) k_pme_gather(
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) u[e] += __shfl_xor_sync(0xffffffffu, u[e], o);
   }
-  // lane e < 3 kc writes column e: component c of right-hand side r0 + r
   double mine = 0.0;
 #pragma unroll
   for (int e = 0; e < NA; e++)
@@ -526,8 +509,6 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, i
 
 namespace bd {
 
-static int pme_plans(bd_ctx* c, int k, int* bk);
-
 int pme_alloc(bd_ctx* c) {
   if (c->pme_grid) return BD_OK;
   int K = c->pmeK, N = c->N;
@@ -535,9 +516,9 @@ int pme_alloc(bd_ctx* c) {
   c->pme_f32 = c->p.precision == BD_PREC_FP32;
   size_t es = c->pme_f32 ? 4 : 8;  // grid, spectrum, influence and pair tensors
   // grids and spectra for the largest number of right-hand sides of a product
-  size_t nr = (size_t)pme_ncp(c->pme_f32, std::max(1, c->nbk));
-  CU(cudaMalloc(&c->pme_grid, es * K3 * nr));
-  CU(cudaMalloc(&c->pme_spec, 2 * es * Ks * nr));
+  size_t nr = (size_t)std::max(1, c->nbk);
+  CU(cudaMalloc(&c->pme_grid, es * 3 * K3 * nr));
+  CU(cudaMalloc(&c->pme_spec, 2 * es * 3 * Ks * nr));
   CU(cudaMalloc(&c->pme_infl, es * 6 * Ks));
   CU(cudaMalloc(&c->pme_bsq, 8 * 3 * (size_t)K));
   c->pme_nblk = (int)((Ks + 255) / 256);
@@ -556,13 +537,19 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_cell_start, 4 * (size_t)(c->rl_ncell_cap + 1)));
   CU(cudaMalloc(&c->rl_cursor, 4 * (size_t)c->rl_ncell_cap));
   CU(cudaMemsetAsync(c->rl_cell_count, 0, 4 * (size_t)c->rl_ncell_cap, c->stream));
-  c->bytes += es * (K3 * nr + 2 * Ks * nr + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
+  c->bytes += es * (3 * K3 * nr + 6 * Ks * nr + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
               24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 2 * es) + 32 * (size_t)N +
               8 * (size_t)N + 12 * (size_t)c->rl_ncell_cap;
-  int f, b;
-  if ((f = pme_plans(c, 1, &b)) < 0) return BD_ERR_CUDA;
-  c->pme_plan_f = f;
-  c->pme_plan_b = b;
+  int n[3] = {K, K, K};
+  cufftHandle f, b;
+  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
+                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3));
+  CF(cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
+                   c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3));
+  CF(cufftSetStream(f, c->stream));
+  CF(cufftSetStream(b, c->stream));
+  c->pme_plan_f = (int)f;
+  c->pme_plan_b = (int)b;
   std::vector<double> bs(3 * (size_t)K);
   bspline_moduli(K, c->pme_p, bs.data());
   for (int d = 1; d < 3; d++)
@@ -572,33 +559,8 @@ int pme_alloc(bd_ctx* c) {
   return BD_OK;
 }
 
-// Forward and inverse transforms of the 3 k columns of a k-right-hand-side
-// grid (strided batches: istride = ncp, idist = 1); returns the forward plan
-// (the inverse in *bk) or -1.
-static int pme_plans(bd_ctx* c, int k, int* bk) {
-  int K = c->pmeK, Kh = K / 2 + 1, ncp = pme_ncp(c->pme_f32, k);
-  int n[3] = {K, K, K}, re[3] = {K, K, K}, cx[3] = {K, K, Kh};
-  cufftHandle f, b;
-  if (cufftPlanMany(&f, 3, n, re, ncp, 1, cx, ncp, 1, c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z,
-                    3 * k) != CUFFT_SUCCESS)
-    return -1;
-  if (cufftPlanMany(&b, 3, n, cx, ncp, 1, re, ncp, 1, c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D,
-                    3 * k) != CUFFT_SUCCESS) {
-    cufftDestroy(f);
-    return -1;
-  }
-  if (cufftSetStream(f, c->stream) != CUFFT_SUCCESS ||
-      cufftSetStream(b, c->stream) != CUFFT_SUCCESS) {
-    cufftDestroy(f);
-    cufftDestroy(b);
-    return -1;
-  }
-  *bk = (int)b;
-  return (int)f;
-}
-
-// Batched transforms of the 3 k columns, created outside any stream capture
-// and kept for up to four values of k (replacing one drops the captured
+// Batched transforms of 3 k grids, created outside any stream capture and
+// kept for up to four values of k (replacing one drops the captured
 // iterations that use it).
 int pme_multi_plan(bd_ctx* c, int k) {
   int slot = -1;
@@ -613,10 +575,21 @@ int pme_multi_plan(bd_ctx* c, int k) {
     cufftDestroy((cufftHandle)c->pme_mplan_b[slot]);
     c->pme_mplan_k[slot] = 0;
   }
-  int f, b;
-  if ((f = pme_plans(c, k, &b)) < 0) return BD_ERR_CUDA;
-  c->pme_mplan_f[slot] = f;
-  c->pme_mplan_b[slot] = b;
+  int K = c->pmeK;
+  size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
+  int n[3] = {K, K, K};
+  cufftHandle f, b;
+  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
+                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3 * k));
+  if (cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
+                    c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3 * k) != CUFFT_SUCCESS) {
+    cufftDestroy(f);
+    return BD_ERR_CUDA;
+  }
+  CF(cufftSetStream(f, c->stream));
+  CF(cufftSetStream(b, c->stream));
+  c->pme_mplan_f[slot] = (int)f;
+  c->pme_mplan_b[slot] = (int)b;
   c->pme_mplan_k[slot] = k;
   return BD_OK;
 }
@@ -739,13 +712,16 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   }
   R* grid = (R*)c->pme_grid;
   Cx* spec = (Cx*)c->pme_spec;
-  int ncp = pme_ncp(sizeof(R) == 4, k);
-  CU(cudaMemsetAsync(grid, 0, sizeof(R) * K3 * ncp, c->stream));
+  CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3 * k, c->stream));
   c->launches += 3;  // spread, influence, gather (the transforms are cuFFT's)
   int nb8 = nblk(N, 8);
-#define PME_SPREAD(P_)                                                                  \
-  k_pme_spread<P_, R><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, ncp, \
-                                                  grid)
+  // measured on the 8000-bead workload with blocks of 8: spreading one
+  // right-hand side per warp and interpolating two per warp is fastest (more
+  // resident warps beat fewer reloads of the weights and pair terms)
+  int cg = k == 1 ? 1 : kGatherChunk;
+  dim3 gs(nb8, k), ggr(nb8, (k + cg - 1) / cg);
+#define PME_SPREAD(P_)                                                                          \
+  k_pme_spread<P_, R, 1><<<gs, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, grid)
   switch (p) {
     case 4: PME_SPREAD(4); break;
     case 6: PME_SPREAD(6); break;
@@ -756,8 +732,8 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
     CF(cufftExecR2C((cufftHandle)pf, (cufftReal*)grid, (cufftComplex*)spec));
   else
     CF(cufftExecD2Z((cufftHandle)pf, (cufftDoubleReal*)grid, (cufftDoubleComplex*)spec));
-  k_pme_apply_influence<R, Cx><<<nblk((long long)Ks * k, 256), 256, 0, c->stream>>>(
-      (const R*)c->pme_infl, spec, Ks, k, ncp);
+  k_pme_apply_influence<R, Cx><<<dim3(nblk((long long)Ks, 256), k), 256, 0, c->stream>>>(
+      (const R*)c->pme_infl, spec, Ks);
   if constexpr (sizeof(R) == 4)
     CF(cufftExecC2R((cufftHandle)pb, (cufftComplex*)spec, (cufftReal*)grid));
   else
@@ -766,24 +742,23 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   memcpy(cell.H, c->pme_cellbuf, sizeof(cell.H));
   memcpy(cell.Hi, c->pme_cellbuf + 9, sizeof(cell.Hi));
   cell.V = c->pme_cellbuf[18];
-  dim3 gg(nb8, (k + kGatherRhs - 1) / kGatherRhs);
-#define PME_GATHER(P_)                                                                          \
-  if (k == 1)                                                                                   \
-    k_pme_gather<P_, R, 1><<<nb8, 256, 0, c->stream>>>(                                         \
-        c->pme_base, c->pme_w, N, K, grid, k, ncp, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,  \
-        c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
-        ostride, orr);                                                                          \
-  else                                                                                          \
-    k_pme_gather<P_, R, kGatherRhs><<<gg, 256, 0, c->stream>>>(                                 \
-        c->pme_base, c->pme_w, N, K, grid, k, ncp, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,  \
-        c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
-        ostride, orr)
+#define PME_GATHER_K(P_, C_)                                                                    \
+  k_pme_gather<P_, R, C_><<<ggr, 256, 0, c->stream>>>(                                          \
+      c->pme_base, c->pme_w, N, K, grid, k, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,         \
+      c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2,   \
+      ostride, orr)
+#define PME_GATHER(P_)               \
+  if (cg == 1)                       \
+    PME_GATHER_K(P_, 1);             \
+  else                               \
+    PME_GATHER_K(P_, kGatherChunk)
   switch (p) {
     case 4: PME_GATHER(4); break;
     case 6: PME_GATHER(6); break;
     default: PME_GATHER(8);
   }
 #undef PME_GATHER
+#undef PME_GATHER_K
   return BD_OK;
 }
 
