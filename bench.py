@@ -312,6 +312,9 @@ def c2_replicas(seed=20261203, n=64):
     return out
 
 
+SEGMENT = [10]  # beads per preconditioner segment (--segment)
+
+
 def build_context(w, seed, path="lanczos32", device_noise="philox", **extra):
     import bd_b200 as B
     edot = edot_of(w)
@@ -340,10 +343,10 @@ def build_context(w, seed, path="lanczos32", device_noise="philox", **extra):
     c.build_neighbors()
     c.inverse_coords()
     if pp.get("precond") == "segment":
-        c.set_preconditioner("segment", 10 if w["Nb"] % 10 == 0 else 5)
+        c.set_preconditioner("segment", SEGMENT[0] if w["Nb"] % SEGMENT[0] == 0 else 5)
     elif pp.get("precond") == "learned":
         c.mpnn_set_params(np.load(os.path.join(PKG, "mpnn_params.npy")))
-        c.set_preconditioner("learned", 10 if w["Nb"] % 10 == 0 else 5)
+        c.set_preconditioner("learned", SEGMENT[0] if w["Nb"] % SEGMENT[0] == 0 else 5)
     return c
 
 
@@ -655,12 +658,15 @@ def main():
     ap.add_argument("--noise-block", type=int, default=8,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
-    ap.add_argument("--pme-rc", type=float, default=11.0,
+    ap.add_argument("--pme-rc", type=float, default=12.1,
                     help="particle-mesh real-space cutoff; the grid follows it (14.5 L / rc "
                          "points, constant interpolation accuracy)")
+    ap.add_argument("--segment", type=int, default=10,
+                    help="beads per segment block of the preconditioned paths")
     ap.add_argument("--compare", type=int, default=1,
                     help="also time the plain FP64 Krylov path (reported as plain_fp64)")
     args = ap.parse_args()
+    SEGMENT[0] = args.segment
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

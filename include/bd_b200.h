@@ -127,7 +127,8 @@ typedef struct {
    * i.e. 1.45 L at the default cutoff 10: spacing proportional to the cutoff),
    * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> the smaller
    * of 10 and 0.43 L; at most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
-   * real-space pairs per bead (0 -> 512). */
+   * real-space pairs per bead (0 -> 2.5 times the mean number of beads within
+   * the cutoff, at least 512). */
   int pme_grid;
   int pme_order;
   double pme_rc;

@@ -178,7 +178,7 @@ struct bd_ctx {
   int *pme_base;     // per bead base grid index, 3 x N
   double *pme_w;     // per bead spline weights, 3 x N x 8
   int pme_plan_f, pme_plan_b;
-  int pme_mplan_k[4], pme_mplan_f[4], pme_mplan_b[4];  // batched plans for k right-hand sides
+  int pme_mplan_k[4], pme_mplan_f[4];  // packed-pair transforms for k right-hand sides
   int rl_cap, rl_ncell_cap;  // real-space pair rows
   int *rl_cnt, *rl_rows, *rl_cell_of, *rl_beads, *rl_cell_count, *rl_cell_start, *rl_cursor;
   void *rl_pos;      // lab-frame positions of the last preparation (double4)

@@ -86,7 +86,6 @@ __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
 // and the bead's values are loaded once for the chunk.  Right-hand side r
 // reads its vector vr entries further on and owns the grids 3 K^3 entries
 // further on.
-constexpr int kGatherChunk = 2;  // right-hand sides per interpolating warp
 
 template <int P, typename R, int KS>
 __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base,
@@ -138,6 +137,105 @@ __global__ void __launch_bounds__(256) k_pme_spread(const int* __restrict__ base
       }
     }
   }
+}
+
+// Products of k >= 2 right-hand sides pack them in pairs: right-hand sides
+// 2p and 2p + 1 are the real and imaginary parts of one complex grid per
+// component (pair p, component c at (3 p + c) K^3).  The influence tensor is
+// real and even in k, so one complex transform, the multiplication and the
+// inverse transform give both products, with no unpacking: spreading takes
+// one float2 atomic per pair and grid point, interpolation one float2 load,
+// and the transforms are contiguous C2C batches.
+template <typename R>
+struct Pair;
+template <>
+struct Pair<float> {
+  using T = float2;
+};
+template <>
+struct Pair<double> {
+  using T = double2;
+};
+
+template <int P, typename R>
+__global__ void __launch_bounds__(256) k_pme_spread_pairs(const int* __restrict__ base,
+                                                          const double* __restrict__ w, int N,
+                                                          int K, VecIn v, size_t vr, int k,
+                                                          typename Pair<R>::T* cgrid) {
+  using C2 = typename Pair<R>::T;
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= N) return;
+  int pr = blockIdx.y, ra = 2 * pr, rb = 2 * pr + 1;
+  size_t K3 = (size_t)K * K * K;
+  size_t oa = (size_t)ra * vr + (size_t)i * v.stride;
+  size_t ob = (size_t)(rb < k ? rb : ra) * vr + (size_t)i * v.stride;
+  R fb_on = rb < k ? (R)1 : (R)0;
+  R fa0 = (R)v.p[0][oa], fa1 = (R)v.p[1][oa], fa2 = (R)v.p[2][oa];
+  R fb0 = fb_on * (R)v.p[0][ob], fb1 = fb_on * (R)v.p[1][ob], fb2 = fb_on * (R)v.p[2][ob];
+  C2* gp = cgrid + (size_t)pr * 3 * K3;
+  const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
+  const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
+  const double* w2 = w + ((size_t)3 * i + 2) * kMaxOrder;
+  int b0 = base[3 * i], b1 = base[3 * i + 1], b2 = base[3 * i + 2];
+#pragma unroll
+  for (int it = 0; it < (P * P * P + 31) / 32; it++) {
+    int q = lane + 32 * it;
+    if (q >= P * P * P) break;
+    int c = q % P, b = (q / P) % P, a = q / (P * P);
+    int g0 = b0 - a, g1 = b1 - b, g2 = b2 - c;
+    g0 += g0 < 0 ? K : 0;
+    g1 += g1 < 0 ? K : 0;
+    g2 += g2 < 0 ? K : 0;
+    double wt = w0[a] * w1[b] * w2[c];
+    size_t g = ((size_t)g0 * K + g1) * K + g2;
+    if constexpr (sizeof(R) == 4) {
+      float wr = (float)wt;
+      atomicAdd(gp + g, make_float2(wr * fa0, wr * fb0));
+      atomicAdd(gp + K3 + g, make_float2(wr * fa1, wr * fb1));
+      atomicAdd(gp + 2 * K3 + g, make_float2(wr * fa2, wr * fb2));
+    } else {
+      atomicAdd(&gp[g].x, wt * fa0);
+      atomicAdd(&gp[g].y, wt * fb0);
+      atomicAdd(&gp[K3 + g].x, wt * fa1);
+      atomicAdd(&gp[K3 + g].y, wt * fb1);
+      atomicAdd(&gp[2 * K3 + g].x, wt * fa2);
+      atomicAdd(&gp[2 * K3 + g].y, wt * fb2);
+    }
+  }
+}
+
+// The influence tensor on the full spectrum of the packed pairs (thread per
+// point and pair): points with m2 > K/2 take the tensor of their mirror -m,
+// stored in the half spectrum (the tensor is even in k; on the Nyquist planes
+// of an even K the stored pairs differ in the sign of off-diagonal entries,
+// where the influence is below 1e-14 of its peak).
+template <typename R, typename Cx>
+__global__ void k_pme_apply_influence_full(const R* __restrict__ infl, Cx* cgrid, int K,
+                                           size_t np3) {
+  size_t K3 = (size_t)K * K * K;
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= K3 * np3) return;
+  size_t m = e % K3, pc = e / K3;  // pair index (components 3 apart)
+  int Kh = K / 2 + 1;
+  int m0 = (int)(m / ((size_t)K * K)), m1 = (int)((m / K) % K), m2 = (int)(m % K);
+  if (m2 > K / 2) {
+    m0 = (K - m0) % K;
+    m1 = (K - m1) % K;
+    m2 = K - m2;
+  }
+  const R* t = infl + 6 * (((size_t)m0 * K + m1) * Kh + m2);
+  Cx* b = cgrid + pc * 3 * K3 + m;
+  Cx x = b[0], y = b[K3], z = b[2 * K3];
+  Cx u, v, ww;
+  u.x = t[0] * x.x + t[1] * y.x + t[2] * z.x;
+  u.y = t[0] * x.y + t[1] * y.y + t[2] * z.y;
+  v.x = t[1] * x.x + t[3] * y.x + t[4] * z.x;
+  v.y = t[1] * x.y + t[3] * y.y + t[4] * z.y;
+  ww.x = t[2] * x.x + t[4] * y.x + t[5] * z.x;
+  ww.y = t[2] * x.y + t[4] * y.y + t[5] * z.y;
+  b[0] = u;
+  b[K3] = v;
+  b[2 * K3] = ww;
 }
 
 // Influence tensor on the half spectrum: (phi(k)/V)(I - k k^T/k^2) |b|^2,
@@ -292,7 +390,7 @@ __device__ __forceinline__ void pair_terms(double alpha, double alpha_ref, doubl
 // row (pair terms, positions and minimum image once for the chunk), then a
 // butterfly reduction; lane e < 3 kc writes component e % 3 of right-hand
 // side r0 + e / 3.
-template <int P, typename R, int KG>
+template <int P, typename R, int KG, bool PK>
 __global__ void __launch_bounds__(256) k_pme_gather(
     const int* __restrict__ base, const double* __restrict__ w, int N, int K,
     const R* __restrict__ grid, int k, double self, const double* __restrict__ soff, VecIn v,
@@ -323,13 +421,28 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     g2 += g2 < 0 ? K : 0;
     double wt = w0[a] * w1[b] * w2[c];
     const R* gp = gbase + ((size_t)g0 * K + g1) * K + g2;
+    if constexpr (PK) {
+      // packed pair blockIdx.y: right-hand sides r0, r0 + 1 as real and
+      // imaginary parts (the grid argument is the pairs' complex grid)
+      using C2 = typename Pair<R>::T;
+      const C2* gq = (const C2*)grid + (size_t)blockIdx.y * 3 * K3 +
+                     (((size_t)g0 * K + g1) * K + g2);
+      C2 x0 = gq[0], x1 = gq[K3], x2 = gq[2 * K3];
+      u[0] += wt * (double)x0.x;
+      u[1] += wt * (double)x1.x;
+      u[2] += wt * (double)x2.x;
+      u[3] += wt * (double)x0.y;
+      u[4] += wt * (double)x1.y;
+      u[5] += wt * (double)x2.y;
+    } else {
 #pragma unroll
-    for (int r = 0; r < KG; r++) {
-      if (r >= kc) break;
-      const R* gr = gp + (size_t)r * 3 * K3;
-      u[3 * r] += wt * (double)gr[0];
-      u[3 * r + 1] += wt * (double)gr[K3];
-      u[3 * r + 2] += wt * (double)gr[2 * K3];
+      for (int r = 0; r < KG; r++) {
+        if (r >= kc) break;
+        const R* gr = gp + (size_t)r * 3 * K3;
+        u[3 * r] += wt * (double)gr[0];
+        u[3 * r + 1] += wt * (double)gr[K3];
+        u[3 * r + 2] += wt * (double)gr[2 * K3];
+      }
     }
   }
   // real-space pairs: the tensor t1 I + t2 d d^T/r^2 of the minimum-image
@@ -518,14 +631,24 @@ int pme_alloc(bd_ctx* c) {
   // grids and spectra for the largest number of right-hand sides of a product
   size_t nr = (size_t)std::max(1, c->nbk);
   CU(cudaMalloc(&c->pme_grid, es * 3 * K3 * nr));
-  CU(cudaMalloc(&c->pme_spec, 2 * es * 3 * Ks * nr));
+  // the spectra; for products of several right-hand sides the same buffer
+  // holds the packed pairs' complex grids (3 ceil(k/2) K^3 complex values)
+  size_t spec_bytes = std::max(2 * es * 3 * Ks * nr, nr > 1 ? 2 * es * 3 * K3 * ((nr + 1) / 2) : 0);
+  CU(cudaMalloc(&c->pme_spec, spec_bytes));
   CU(cudaMalloc(&c->pme_infl, es * 6 * Ks));
   CU(cudaMalloc(&c->pme_bsq, 8 * 3 * (size_t)K));
   c->pme_nblk = (int)((Ks + 255) / 256);
   CU(cudaMalloc(&c->pme_soff, 8 * (3 * (size_t)c->pme_nblk + 3)));
   CU(cudaMalloc(&c->pme_base, 4 * 3 * (size_t)N));
   CU(cudaMalloc(&c->pme_w, 8 * 3 * (size_t)N * kMaxOrder));
-  c->rl_cap = c->p.pme_max_pairs > 0 ? c->p.pme_max_pairs : 512;
+  // default row cap: 2.5 times the mean number of beads within the cutoff at
+  // the system's density, at least 512, a multiple of 32
+  if (c->p.pme_max_pairs > 0) {
+    c->rl_cap = c->p.pme_max_pairs;
+  } else {
+    double mean = 4.0 / 3.0 * M_PI * c->pme_rc * c->pme_rc * c->pme_rc * N / c->boxvol;
+    c->rl_cap = std::max(512, ((int)ceil(2.5 * mean) + 31) / 32 * 32);
+  }
   CU(cudaMalloc(&c->rl_cnt, 4 * (size_t)N));
   CU(cudaMalloc(&c->rl_rows, 4 * (size_t)N * c->rl_cap));
   CU(cudaMalloc(&c->rl_pos, 32 * (size_t)N));
@@ -537,7 +660,7 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_cell_start, 4 * (size_t)(c->rl_ncell_cap + 1)));
   CU(cudaMalloc(&c->rl_cursor, 4 * (size_t)c->rl_ncell_cap));
   CU(cudaMemsetAsync(c->rl_cell_count, 0, 4 * (size_t)c->rl_ncell_cap, c->stream));
-  c->bytes += es * (3 * K3 * nr + 6 * Ks * nr + 6 * Ks) + 24 * (size_t)K + 12 * (size_t)N +
+  c->bytes += es * (3 * K3 * nr + 6 * Ks) + spec_bytes + 24 * (size_t)K + 12 * (size_t)N +
               24 * (size_t)N * kMaxOrder + 4 * (size_t)N + (size_t)N * c->rl_cap * (4 + 2 * es) + 32 * (size_t)N +
               8 * (size_t)N + 12 * (size_t)c->rl_ncell_cap;
   int n[3] = {K, K, K};
@@ -559,9 +682,10 @@ int pme_alloc(bd_ctx* c) {
   return BD_OK;
 }
 
-// Batched transforms of 3 k grids, created outside any stream capture and
-// kept for up to four values of k (replacing one drops the captured
-// iterations that use it).
+// In-place complex transforms of the 3 ceil(k/2) packed-pair grids of a
+// k-right-hand-side product (one plan, used forward and inverse), created
+// outside any stream capture and kept for up to four values of k (replacing
+// one drops the captured iterations that use it).
 int pme_multi_plan(bd_ctx* c, int k) {
   int slot = -1;
   for (int q = 0; q < 4; q++)
@@ -572,24 +696,19 @@ int pme_multi_plan(bd_ctx* c, int k) {
     slot = 3;
     lanczos_graphs_reset(c);
     cufftDestroy((cufftHandle)c->pme_mplan_f[slot]);
-    cufftDestroy((cufftHandle)c->pme_mplan_b[slot]);
     c->pme_mplan_k[slot] = 0;
   }
   int K = c->pmeK;
-  size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
+  size_t K3 = (size_t)K * K * K;
   int n[3] = {K, K, K};
-  cufftHandle f, b;
-  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)Ks,
-                   c->pme_f32 ? CUFFT_R2C : CUFFT_D2Z, 3 * k));
-  if (cufftPlanMany(&b, 3, n, nullptr, 1, (int)Ks, nullptr, 1, (int)K3,
-                    c->pme_f32 ? CUFFT_C2R : CUFFT_Z2D, 3 * k) != CUFFT_SUCCESS) {
+  cufftHandle f;
+  CF(cufftPlanMany(&f, 3, n, nullptr, 1, (int)K3, nullptr, 1, (int)K3,
+                   c->pme_f32 ? CUFFT_C2C : CUFFT_Z2Z, 3 * ((k + 1) / 2)));
+  if (cufftSetStream(f, c->stream) != CUFFT_SUCCESS) {
     cufftDestroy(f);
     return BD_ERR_CUDA;
   }
-  CF(cufftSetStream(f, c->stream));
-  CF(cufftSetStream(b, c->stream));
   c->pme_mplan_f[slot] = (int)f;
-  c->pme_mplan_b[slot] = (int)b;
   c->pme_mplan_k[slot] = k;
   return BD_OK;
 }
@@ -600,7 +719,6 @@ void pme_free(bd_ctx* c) {
   for (int q = 0; q < 4; q++)
     if (c->pme_mplan_k[q]) {
       cufftDestroy((cufftHandle)c->pme_mplan_f[q]);
-      cufftDestroy((cufftHandle)c->pme_mplan_b[q]);
       c->pme_mplan_k[q] = 0;
     }
   void* ptrs[] = {c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
@@ -702,26 +820,62 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   int K = c->pmeK, N = c->N, p = c->pme_p;
   size_t K3 = (size_t)K * K * K, Ks = (size_t)K * K * (K / 2 + 1);
   if (k < 1 || k > std::max(1, c->nbk)) return BD_ERR_ARG;
-  int pf = c->pme_plan_f, pb = c->pme_plan_b;
-  if (k > 1) {
-    int q = 0;
-    while (q < 4 && c->pme_mplan_k[q] != k) q++;
-    if (q == 4) return BD_ERR_STATE;  // pme_multi_plan(c, k) first
-    pf = c->pme_mplan_f[q];
-    pb = c->pme_mplan_b[q];
-  }
-  R* grid = (R*)c->pme_grid;
-  Cx* spec = (Cx*)c->pme_spec;
-  CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3 * k, c->stream));
-  c->launches += 3;  // spread, influence, gather (the transforms are cuFFT's)
   int nb8 = nblk(N, 8);
-  // measured on the 8000-bead workload with blocks of 8: spreading one
-  // right-hand side per warp and interpolating two per warp is fastest (more
-  // resident warps beat fewer reloads of the weights and pair terms)
-  int cg = k == 1 ? 1 : kGatherChunk;
-  dim3 gs(nb8, k), ggr(nb8, (k + cg - 1) / cg);
-#define PME_SPREAD(P_)                                                                          \
-  k_pme_spread<P_, R, 1><<<gs, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, grid)
+  Cell cell;
+  memcpy(cell.H, c->pme_cellbuf, sizeof(cell.H));
+  memcpy(cell.Hi, c->pme_cellbuf + 9, sizeof(cell.Hi));
+  cell.V = c->pme_cellbuf[18];
+  c->launches += 3;  // spread, influence, gather (the transforms are cuFFT's)
+  if (k == 1) {
+    // one right-hand side: three real grids, R2C / C2R
+    R* grid = (R*)c->pme_grid;
+    Cx* spec = (Cx*)c->pme_spec;
+    CU(cudaMemsetAsync(grid, 0, sizeof(R) * 3 * K3, c->stream));
+#define PME_SPREAD(P_) \
+  k_pme_spread<P_, R, 1><<<nb8, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, 1, grid)
+    switch (p) {
+      case 4: PME_SPREAD(4); break;
+      case 6: PME_SPREAD(6); break;
+      default: PME_SPREAD(8);
+    }
+#undef PME_SPREAD
+    if constexpr (sizeof(R) == 4)
+      CF(cufftExecR2C((cufftHandle)c->pme_plan_f, (cufftReal*)grid, (cufftComplex*)spec));
+    else
+      CF(cufftExecD2Z((cufftHandle)c->pme_plan_f, (cufftDoubleReal*)grid,
+                      (cufftDoubleComplex*)spec));
+    k_pme_apply_influence<R, Cx><<<nblk((long long)Ks, 256), 256, 0, c->stream>>>(
+        (const R*)c->pme_infl, spec, Ks);
+    if constexpr (sizeof(R) == 4)
+      CF(cufftExecC2R((cufftHandle)c->pme_plan_b, (cufftComplex*)spec, (cufftReal*)grid));
+    else
+      CF(cufftExecZ2D((cufftHandle)c->pme_plan_b, (cufftDoubleComplex*)spec,
+                      (cufftDoubleReal*)grid));
+#define PME_GATHER(P_)                                                                        \
+  k_pme_gather<P_, R, 1, false><<<nb8, 256, 0, c->stream>>>(                                  \
+      c->pme_base, c->pme_w, N, K, grid, 1, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,       \
+      c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
+      ostride, orr)
+    switch (p) {
+      case 4: PME_GATHER(4); break;
+      case 6: PME_GATHER(6); break;
+      default: PME_GATHER(8);
+    }
+#undef PME_GATHER
+    return BD_OK;
+  }
+  // k >= 2: packed pairs in the spectrum buffer, in-place complex transforms
+  int q = 0;
+  while (q < 4 && c->pme_mplan_k[q] != k) q++;
+  if (q == 4) return BD_ERR_STATE;  // pme_multi_plan(c, k) first
+  cufftHandle plan = (cufftHandle)c->pme_mplan_f[q];
+  int np = (k + 1) / 2;
+  using C2 = typename Pair<R>::T;
+  C2* cg = (C2*)c->pme_spec;
+  CU(cudaMemsetAsync(cg, 0, sizeof(C2) * 3 * K3 * np, c->stream));
+  dim3 gp(nb8, np);
+#define PME_SPREAD(P_)                                                                       \
+  k_pme_spread_pairs<P_, R><<<gp, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, cg)
   switch (p) {
     case 4: PME_SPREAD(4); break;
     case 6: PME_SPREAD(6); break;
@@ -729,36 +883,26 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   }
 #undef PME_SPREAD
   if constexpr (sizeof(R) == 4)
-    CF(cufftExecR2C((cufftHandle)pf, (cufftReal*)grid, (cufftComplex*)spec));
+    CF(cufftExecC2C(plan, (cufftComplex*)cg, (cufftComplex*)cg, CUFFT_FORWARD));
   else
-    CF(cufftExecD2Z((cufftHandle)pf, (cufftDoubleReal*)grid, (cufftDoubleComplex*)spec));
-  k_pme_apply_influence<R, Cx><<<dim3(nblk((long long)Ks, 256), k), 256, 0, c->stream>>>(
-      (const R*)c->pme_infl, spec, Ks);
+    CF(cufftExecZ2Z(plan, (cufftDoubleComplex*)cg, (cufftDoubleComplex*)cg, CUFFT_FORWARD));
+  k_pme_apply_influence_full<R, C2><<<nblk((long long)K3 * np, 256), 256, 0, c->stream>>>(
+      (const R*)c->pme_infl, cg, K, (size_t)np);
   if constexpr (sizeof(R) == 4)
-    CF(cufftExecC2R((cufftHandle)pb, (cufftComplex*)spec, (cufftReal*)grid));
+    CF(cufftExecC2C(plan, (cufftComplex*)cg, (cufftComplex*)cg, CUFFT_INVERSE));
   else
-    CF(cufftExecZ2D((cufftHandle)pb, (cufftDoubleComplex*)spec, (cufftDoubleReal*)grid));
-  Cell cell;
-  memcpy(cell.H, c->pme_cellbuf, sizeof(cell.H));
-  memcpy(cell.Hi, c->pme_cellbuf + 9, sizeof(cell.Hi));
-  cell.V = c->pme_cellbuf[18];
-#define PME_GATHER_K(P_, C_)                                                                    \
-  k_pme_gather<P_, R, C_><<<ggr, 256, 0, c->stream>>>(                                          \
-      c->pme_base, c->pme_w, N, K, grid, k, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,         \
-      c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2,   \
-      ostride, orr)
-#define PME_GATHER(P_)               \
-  if (cg == 1)                       \
-    PME_GATHER_K(P_, 1);             \
-  else                               \
-    PME_GATHER_K(P_, kGatherChunk)
+    CF(cufftExecZ2Z(plan, (cufftDoubleComplex*)cg, (cufftDoubleComplex*)cg, CUFFT_INVERSE));
+#define PME_GATHER(P_)                                                                        \
+  k_pme_gather<P_, R, 2, true><<<gp, 256, 0, c->stream>>>(                                    \
+      c->pme_base, c->pme_w, N, K, (const R*)cg, k, c->pme_self, c->pme_soff, v, vr,          \
+      c->rl_cnt, c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap,  \
+      o0, o1, o2, ostride, orr)
   switch (p) {
     case 4: PME_GATHER(4); break;
     case 6: PME_GATHER(6); break;
     default: PME_GATHER(8);
   }
 #undef PME_GATHER
-#undef PME_GATHER_K
   return BD_OK;
 }
 
