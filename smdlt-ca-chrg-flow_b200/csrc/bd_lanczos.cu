@@ -675,6 +675,9 @@ void noise_blocks_release(bd_ctx* c) {
   c->blk_next = 0;
 }
 
+// Chunks per right-hand side of the block CGS2 kernels.
+static int block_chunks(int k) { return std::min(kDotBlocks, std::max(8, 4 * kDotBlocks / k)); }
+
 // Layout of a block of k right-hand sides: basis vector j of r at
 // BV + (j k + r) n, alpha_j and beta_j at [j k + r].
 static Kry block_kry(bd_ctx* c, int k) {
@@ -719,7 +722,10 @@ static int block_part(bd_ctx* c, int k, bool pre, int part) {
     return launch_ok(c);
   }
   Kry q = block_kry(c, k);
-  dim3 g(kDotBlocks, k);
+  // 4 x 148 CTAs in all: each right-hand side's vectors in 592 / k chunks
+  // (at most 148), so every CTA re-sums only the chunk partials of its own
+  // right-hand side while enough warps stay resident
+  dim3 g(block_chunks(k), k);
   c->launches += 5;
   k_orth0<<<g, 256, 0, st>>>(q);
   k_orth1<<<g, 256, 0, st>>>(q);
