@@ -182,6 +182,8 @@ struct bd_ctx {
   int rl_cap, rl_ncell_cap;  // real-space pair rows
   int *rl_cnt, *rl_rows, *rl_cell_of, *rl_beads, *rl_cell_count, *rl_cell_start, *rl_cursor;
   void *rl_pos;      // lab-frame positions of the last preparation (double4)
+  float *pme_vpk;    // FP32 block products: per packed pair and bead the pair's
+                     // 6 input values (+2 padding), written by the spread
   void *rl_tt;       // per pair t1 and t2 / r^2 of the real-space tensor (FP64 or FP32)
   double pme_cellbuf[19];  // its cell: H, H^-1, volume
   double pme_alpha_ref;    // calcHI's split parameter at that step

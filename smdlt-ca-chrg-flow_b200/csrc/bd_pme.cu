@@ -157,11 +157,15 @@ struct Pair<double> {
   using T = double2;
 };
 
+// With vpk (FP32), lanes 0..7 of a bead's warp also store the pair's six
+// input values (plus two zeros) at vpk[(p N + i) 8], for the interpolation's
+// real-space part to read as two float4.
 template <int P, typename R>
 __global__ void __launch_bounds__(256) k_pme_spread_pairs(const int* __restrict__ base,
                                                           const double* __restrict__ w, int N,
                                                           int K, VecIn v, size_t vr, int k,
-                                                          typename Pair<R>::T* cgrid) {
+                                                          typename Pair<R>::T* cgrid,
+                                                          float* vpk) {
   using C2 = typename Pair<R>::T;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
@@ -172,6 +176,11 @@ __global__ void __launch_bounds__(256) k_pme_spread_pairs(const int* __restrict_
   R fb_on = rb < k ? (R)1 : (R)0;
   R fa0 = (R)v.p[0][oa], fa1 = (R)v.p[1][oa], fa2 = (R)v.p[2][oa];
   R fb0 = fb_on * (R)v.p[0][ob], fb1 = fb_on * (R)v.p[1][ob], fb2 = fb_on * (R)v.p[2][ob];
+  if (vpk && lane < 8) {
+    R x = lane == 0 ? fa0 : lane == 1 ? fa1 : lane == 2 ? fa2
+        : lane == 3 ? fb0 : lane == 4 ? fb1 : lane == 5 ? fb2 : (R)0;
+    vpk[((size_t)pr * N + i) * 8 + lane] = (float)x;
+  }
   C2* gp = cgrid + (size_t)pr * 3 * K3;
   const double* w0 = w + ((size_t)3 * i + 0) * kMaxOrder;
   const double* w1 = w + ((size_t)3 * i + 1) * kMaxOrder;
@@ -396,7 +405,8 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     const R* __restrict__ grid, int k, double self, const double* __restrict__ soff, VecIn v,
     size_t vr, const int* __restrict__ rcnt, const int* __restrict__ rrows,
     const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
-    double* o0, double* o1, double* o2, int ostride, size_t orr) {
+    double* o0, double* o1, double* o2, int ostride, size_t orr,
+    const float* __restrict__ vpk) {
   constexpr int NA = 3 * KG;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
@@ -468,15 +478,29 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     dz = Lz * s2;
     const R* tk = tt + 2 * ((size_t)i * rcap + kk);
     double t1 = tk[0], t2r = tk[1];  // t1 and t2 / r^2 of the pair
+    if (PK && vpk) {
+      // the pair's six values of bead j, stored by the spread (FP32)
+      const float4* pj4 = (const float4*)(vpk + ((size_t)blockIdx.y * N + j) * 8);
+      float4 a = pj4[0], b = pj4[1];
+      double qa = t2r * (dx * a.x + dy * a.y + dz * a.z);
+      u[0] += t1 * a.x + qa * dx;
+      u[1] += t1 * a.y + qa * dy;
+      u[2] += t1 * a.z + qa * dz;
+      double qb = t2r * (dx * a.w + dy * b.x + dz * b.y);
+      u[3] += t1 * a.w + qb * dx;
+      u[4] += t1 * b.x + qb * dy;
+      u[5] += t1 * b.y + qb * dz;
+    } else {
 #pragma unroll
-    for (int r = 0; r < KG; r++) {
-      if (r >= kc) break;
-      size_t o = (size_t)(r0 + r) * vr + (size_t)j * v.stride;
-      double x0 = v.p[0][o], x1 = v.p[1][o], x2 = v.p[2][o];
-      double qq = t2r * (dx * x0 + dy * x1 + dz * x2);
-      u[3 * r] += t1 * x0 + qq * dx;
-      u[3 * r + 1] += t1 * x1 + qq * dy;
-      u[3 * r + 2] += t1 * x2 + qq * dz;
+      for (int r = 0; r < KG; r++) {
+        if (r >= kc) break;
+        size_t o = (size_t)(r0 + r) * vr + (size_t)j * v.stride;
+        double x0 = v.p[0][o], x1 = v.p[1][o], x2 = v.p[2][o];
+        double qq = t2r * (dx * x0 + dy * x1 + dz * x2);
+        u[3 * r] += t1 * x0 + qq * dx;
+        u[3 * r + 1] += t1 * x1 + qq * dy;
+        u[3 * r + 2] += t1 * x2 + qq * dz;
+      }
     }
   }
 #pragma unroll
@@ -652,6 +676,10 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_cnt, 4 * (size_t)N));
   CU(cudaMalloc(&c->rl_rows, 4 * (size_t)N * c->rl_cap));
   CU(cudaMalloc(&c->rl_pos, 32 * (size_t)N));
+  if (c->pme_f32 && nr > 1) {
+    CU(cudaMalloc(&c->pme_vpk, 32 * (size_t)N * ((nr + 1) / 2)));
+    c->bytes += 32 * (size_t)N * ((nr + 1) / 2);
+  }
   CU(cudaMalloc(&c->rl_tt, 2 * es * (size_t)N * c->rl_cap));
   c->rl_ncell_cap = 4096;
   CU(cudaMalloc(&c->rl_cell_of, 4 * (size_t)N));
@@ -721,7 +749,7 @@ void pme_free(bd_ctx* c) {
       cufftDestroy((cufftHandle)c->pme_mplan_f[q]);
       c->pme_mplan_k[q] = 0;
     }
-  void* ptrs[] = {c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
+  void* ptrs[] = {c->pme_vpk, c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
                   c->rl_cnt, c->rl_rows, c->rl_pos, c->rl_tt, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
                   c->rl_cell_start, c->rl_cursor};
   for (void* q : ptrs)
@@ -855,7 +883,7 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   k_pme_gather<P_, R, 1, false><<<nb8, 256, 0, c->stream>>>(                                  \
       c->pme_base, c->pme_w, N, K, grid, 1, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,       \
       c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
-      ostride, orr)
+      ostride, orr, nullptr)
     switch (p) {
       case 4: PME_GATHER(4); break;
       case 6: PME_GATHER(6); break;
@@ -874,8 +902,10 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   C2* cg = (C2*)c->pme_spec;
   CU(cudaMemsetAsync(cg, 0, sizeof(C2) * 3 * K3 * np, c->stream));
   dim3 gp(nb8, np);
+  float* vpk = sizeof(R) == 4 ? c->pme_vpk : nullptr;
 #define PME_SPREAD(P_)                                                                       \
-  k_pme_spread_pairs<P_, R><<<gp, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, cg)
+  k_pme_spread_pairs<P_, R><<<gp, 256, 0, c->stream>>>(c->pme_base, c->pme_w, N, K, v, vr, k, cg, \
+                                                       vpk)
   switch (p) {
     case 4: PME_SPREAD(4); break;
     case 6: PME_SPREAD(6); break;
@@ -896,7 +926,7 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   k_pme_gather<P_, R, 2, true><<<gp, 256, 0, c->stream>>>(                                    \
       c->pme_base, c->pme_w, N, K, (const R*)cg, k, c->pme_self, c->pme_soff, v, vr,          \
       c->rl_cnt, c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap,  \
-      o0, o1, o2, ostride, orr)
+      o0, o1, o2, ostride, orr, vpk)
   switch (p) {
     case 4: PME_GATHER(4); break;
     case 6: PME_GATHER(6); break;
