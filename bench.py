@@ -658,7 +658,7 @@ def main():
     ap.add_argument("--noise-block", type=int, default=8,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
-    ap.add_argument("--pme-rc", type=float, default=12.1,
+    ap.add_argument("--pme-rc", type=float, default=13.6,
                     help="particle-mesh real-space cutoff; the grid follows it (14.5 L / rc "
                          "points, constant interpolation accuracy)")
     ap.add_argument("--segment", type=int, default=10,

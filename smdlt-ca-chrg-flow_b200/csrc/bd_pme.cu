@@ -465,23 +465,21 @@ __global__ void __launch_bounds__(256) k_pme_gather(
   const double h00 = cell.H[0], h01 = cell.H[1], h10 = cell.H[3], h11 = cell.H[4];
   const double g00 = cell.Hi[0], g01 = cell.Hi[1], g10 = cell.Hi[3], g11 = cell.Hi[4];
   const double Lz = cell.H[8], iLz = cell.Hi[8];
-  for (int kk = lane; kk < n; kk += 32) {
-    int j = prow[kk];
-    double4 pj = pos[j];
-    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
-    s0 -= rint(s0);
-    s1 -= rint(s1);
-    s2 -= rint(s2);
-    dx = h00 * s0 + h01 * s1;
-    dy = h10 * s0 + h11 * s1;
-    dz = Lz * s2;
-    const R* tk = tt + 2 * ((size_t)i * rcap + kk);
-    double t1 = tk[0], t2r = tk[1];  // t1 and t2 / r^2 of the pair
-    if (PK && vpk) {
-      // the pair's six values of bead j, stored by the spread (FP32)
-      const float4* pj4 = (const float4*)(vpk + ((size_t)blockIdx.y * N + j) * 8);
-      float4 a = pj4[0], b = pj4[1];
+  if (PK && vpk) {
+    // packed pair: the neighbour's six values as two float4 stored by the
+    // spread; two pairs per lane and iteration, so two independent chains
+    // of loads (row entry, then position and values) are in flight
+    const float* vp = vpk + (size_t)blockIdx.y * N * 8;
+    const R* tr = tt + 2 * (size_t)i * rcap;
+    auto add = [&](double4 pj, double t1, double t2r, float4 a, float4 b) {
+      double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
+      s0 -= rint(s0);
+      s1 -= rint(s1);
+      s2 -= rint(s2);
+      dx = h00 * s0 + h01 * s1;
+      dy = h10 * s0 + h11 * s1;
+      dz = Lz * s2;
       double qa = t2r * (dx * a.x + dy * a.y + dz * a.z);
       u[0] += t1 * a.x + qa * dx;
       u[1] += t1 * a.y + qa * dy;
@@ -490,7 +488,38 @@ __global__ void __launch_bounds__(256) k_pme_gather(
       u[3] += t1 * a.w + qb * dx;
       u[4] += t1 * b.x + qb * dy;
       u[5] += t1 * b.y + qb * dz;
-    } else {
+    };
+    int kk = lane;
+    for (; kk + 32 < n; kk += 64) {
+      int ja = prow[kk], jb = prow[kk + 32];
+      double4 pa = pos[ja], pb = pos[jb];
+      const float4* va = (const float4*)(vp + (size_t)ja * 8);
+      const float4* vb = (const float4*)(vp + (size_t)jb * 8);
+      float4 a0 = va[0], a1 = va[1], b0 = vb[0], b1 = vb[1];
+      double t1a = tr[2 * kk], t2a = tr[2 * kk + 1];
+      double t1b = tr[2 * (kk + 32)], t2b = tr[2 * (kk + 32) + 1];
+      add(pa, t1a, t2a, a0, a1);
+      add(pb, t1b, t2b, b0, b1);
+    }
+    if (kk < n) {
+      int ja = prow[kk];
+      const float4* va = (const float4*)(vp + (size_t)ja * 8);
+      add(pos[ja], tr[2 * kk], tr[2 * kk + 1], va[0], va[1]);
+    }
+  } else {
+    for (int kk = lane; kk < n; kk += 32) {
+      int j = prow[kk];
+      double4 pj = pos[j];
+      double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
+      s0 -= rint(s0);
+      s1 -= rint(s1);
+      s2 -= rint(s2);
+      dx = h00 * s0 + h01 * s1;
+      dy = h10 * s0 + h11 * s1;
+      dz = Lz * s2;
+      const R* tk = tt + 2 * ((size_t)i * rcap + kk);
+      double t1 = tk[0], t2r = tk[1];  // t1 and t2 / r^2 of the pair
 #pragma unroll
       for (int r = 0; r < KG; r++) {
         if (r >= kc) break;
@@ -503,6 +532,7 @@ __global__ void __launch_bounds__(256) k_pme_gather(
       }
     }
   }
+
 #pragma unroll
   for (int e = 0; e < NA; e++) {
     if (e >= nj) break;
