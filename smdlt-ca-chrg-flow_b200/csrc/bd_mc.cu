@@ -369,7 +369,7 @@ __global__ void k_hop_fill(const int* __restrict__ cell_of, const int* __restric
     if (cell_of[k] == c) idx[p++] = k;
 }
 
-__global__ void __launch_bounds__(256) k_hop_colour(
+__global__ void __launch_bounds__(1024) k_hop_colour(
     Lat l, HGeom g, int colour, const double* __restrict__ rx, const double* __restrict__ ry,
     const double* __restrict__ rz, int N, int Nb, int nch, const int* __restrict__ start,
     const int* __restrict__ idx, const int* __restrict__ cell_of,
@@ -524,7 +524,9 @@ int charge_hop_parallel(bd_ctx* c) {
   for (int colour = 0; colour < 8; colour++) {
     CU(cudaMemcpyAsync(site0, c->track, 4 * (size_t)nch, cudaMemcpyDeviceToDevice, c->stream));
     c->launches++;
-    k_hop_colour<<<ncell, 256, 0, c->stream>>>(
+    // only the cells of one colour work in a launch (ncell / 8 CTAs): 1024
+    // threads share each trial's energy sum over the charges
+    k_hop_colour<<<ncell, 1024, 0, c->stream>>>(
         l, g, colour, c->rx, c->ry, c->rz, N, c->Nb, nch, start, idx, cell_of, site0, qk,
         c->track, c->old, c->cflags, c->nb_count, c->nb_rows, c->maxnb, c->p.lambda_b,
         c->kappa_d, c->p.barrier, c->p.barrier2, c->p.philox_seed, sweep, c->hoplog);
