@@ -21,6 +21,7 @@
 #include <condition_variable>
 #include <map>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -37,6 +38,7 @@ struct bd_batch {
   int pending = 0;
   bool stop = false;
   std::vector<int> status;
+  std::vector<std::string> detail;  // bd_last_error_detail of a failing replica's worker
 };
 
 static void worker(bd_batch* b, int r) {
@@ -59,6 +61,7 @@ static void worker(bd_batch* b, int r) {
     {
       std::lock_guard<std::mutex> lk(b->mu);
       b->status[r] = s;
+      b->detail[r] = s == BD_ERR_CUDA ? bd_last_error_detail() : "";
       if (--b->pending == 0) b->cv_done.notify_all();
     }
   }
@@ -73,6 +76,7 @@ int bd_batch_create(bd_ctx* const* ctxs, int n, bd_batch** out) {
   bd_batch* b = new bd_batch();
   b->ctx.assign(ctxs, ctxs + n);
   b->status.assign(n, BD_OK);
+  b->detail.assign(n, "");
   for (int r = 0; r < n; r++) b->workers.emplace_back(worker, b, r);
   *out = b;
   return BD_OK;
@@ -91,8 +95,13 @@ int bd_batch_step_lanczos(bd_batch* b, unsigned long t0, int nsteps, int with_ho
   b->cv_go.notify_all();
   std::unique_lock<std::mutex> lk(b->mu);
   b->cv_done.wait(lk, [&] { return b->pending == 0; });
-  for (int s : b->status)
-    if (s != BD_OK) return s;
+  for (size_t r = 0; r < b->status.size(); r++)
+    if (b->status[r] != BD_OK) {
+      // the failing replica's call site, readable from this thread
+      if (b->status[r] == BD_ERR_CUDA)
+        bd::set_error_detail(("replica " + std::to_string(r) + ": " + b->detail[r]).c_str());
+      return b->status[r];
+    }
   return BD_OK;
 }
 

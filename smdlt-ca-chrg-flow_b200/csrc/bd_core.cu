@@ -27,6 +27,8 @@ int set_error_from_bits(int bits) {
 
 static thread_local char g_detail[320];
 
+void set_error_detail(const char* msg) { snprintf(g_detail, sizeof(g_detail), "%s", msg); }
+
 int cuda_fail(int code, const char* msg, const char* file, int line) {
   const char* base = file;
   for (const char* q = file; *q; q++)
@@ -340,18 +342,21 @@ __global__ void k_bond(Lat l, const double* __restrict__ rx, const double* __res
 // 12 eps (r6^2 - r6)/r^2 with rc = 5 in shear; extensional/src/main14.c:
 // 625-685: WCA 48 eps (r6^2 - r6/2)/r^2 with rc^2 = 5.03968).  One thread per
 // bead walks its full (sorted) row; the virial counts each pair once.
-__global__ void k_ev(Lat l, const double* __restrict__ rx, const double* __restrict__ ry,
-                     const double* __restrict__ rz, double* fx, double* fy, double* fz, int N,
-                     const int* __restrict__ cnt, const int* __restrict__ rows, int maxnb,
-                     double r2cut, double eps, double* stress) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_ev(Lat l, const double* __restrict__ rx,
+                                            const double* __restrict__ ry,
+                                            const double* __restrict__ rz, double* fx, double* fy,
+                                            double* fz, int N, const int* __restrict__ cnt,
+                                            const int* __restrict__ rows, int maxnb, double r2cut,
+                                            double eps, double* stress) {
+  // one warp per bead: the lanes split its neighbour row, then a butterfly
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   double sxx = 0, syy = 0, sxy = 0;
   if (i < N) {
     double f0 = 0, f1 = 0, f2 = 0;
     int n = cnt[i];
     const int* row = rows + (size_t)i * maxnb;
     double xi = rx[i], yi = ry[i], zi = rz[i];
-    for (int k = 0; k < n; k++) {
+    for (int k = lane; k < n; k += 32) {
       int j = row[k];
       double vx, vy, vz;
       min_image(l, subx(xi, rx[j]), subx(yi, ry[j]), subx(zi, rz[j]), vx, vy, vz);
@@ -373,9 +378,16 @@ __global__ void k_ev(Lat l, const double* __restrict__ rx, const double* __restr
         }
       }
     }
-    fx[i] += f0;
-    fy[i] += f1;
-    fz[i] += f2;
+    for (int o = 16; o > 0; o >>= 1) {
+      f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+      f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+      f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    }
+    if (lane == 0) {
+      fx[i] += f0;
+      fy[i] += f1;
+      fz[i] += f2;
+    }
   }
   if (l.flow != 0) sxy = 0.0;
   block_add3(sxx, syy, sxy, stress);
@@ -711,6 +723,18 @@ int bd_create(const bd_params* p, bd_ctx** out) {
     return s;
   }
   c->btab.assign(c->sbins + 1, 0.0);
+  if (c->nbk > 1) {
+    // pinned host copy of the noise blocks' alpha and beta, allocated here
+    // rather than at the first block: a pinned allocation can synchronise
+    // the device, which would void a stream capture running at that moment
+    // in another thread (replicas of a batch capture their iterations
+    // concurrently)
+    int L1 = (p->lanczos_max > 0 ? p->lanczos_max : 200) + 1;
+    if (cudaMallocHost(&c->Bhost, 8 * (size_t)2 * c->nbk * L1) != cudaSuccess) {
+      bd_destroy(c);
+      return BD_ERR_OOM;
+    }
+  }
   c->use_graphs = true;
   c->t = 0;
   c->tstart = 0;
@@ -1030,7 +1054,7 @@ int bd_bond_force(bd_ctx* c) {
 int bd_ev_force(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
   c->launches++;
-  k_ev<<<nblk(c->N, 128), 128, 0, c->stream>>>(kernel_lat(c), c->rx, c->ry, c->rz, c->fx, c->fy,
+  k_ev<<<nblk(c->N, 8), 256, 0, c->stream>>>(kernel_lat(c), c->rx, c->ry, c->rz, c->fx, c->fy,
                                                 c->fz, c->N, c->nb_count, c->nb_rows, c->maxnb,
                                                 c->r2cut, c->p.epsilon, c->stress);
   return launch_ok(c);

@@ -18,6 +18,8 @@ namespace bd {
 // Records the failing CUDA or cuFFT call (code, message, source line) for
 // bd_last_error_detail and returns BD_ERR_CUDA.
 int cuda_fail(int code, const char* msg, const char* file, int line);
+// Replaces the calling thread's bd_last_error_detail text.
+void set_error_detail(const char* msg);
 
 // Lattice of the deforming cell at one step (updateLattice,
 // shear/src/main26.c:1382-1408, extensional/src/main14.c:1426-1450).  Built

@@ -508,11 +508,11 @@ static int lanczos_iteration_graph(bd_ctx* c, bool pre) {
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     c->capturing = false;
     if (s != BD_OK) return s;
-    if (e != cudaSuccess) return BD_ERR_CUDA;
+    if (e != cudaSuccess) return cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
     cudaGraphExec_t ex;
     e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) return BD_ERR_CUDA;
+    if (e != cudaSuccess) return cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
     c->lan_graph[v] = (void*)ex;
     c->lan_graph_launches[v] = c->launches - l0;
     c->launches = l0;
@@ -638,7 +638,7 @@ static int alloc_blocks(bd_ctx* c) {
   CU(cudaMalloc(&c->Bc, 8 * (size_t)k * L1));
   CU(cudaMalloc(&c->Bm, 4 * (size_t)k));
   CU(cudaMalloc(&c->Bjd, 16));
-  CU(cudaMallocHost(&c->Bhost, 8 * (size_t)2 * k * L1));
+  if (!c->Bhost) return BD_ERR_STATE;  // pinned at bd_create (see there)
   CU(cudaMalloc(&c->Brng, sizeof(Ran1) * (size_t)(k + 1)));
   cudaEvent_t ev;
   CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -765,11 +765,11 @@ static int block_iteration(bd_ctx* c, int k, bool pre) {
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       c->capturing = false;
       if (s2 != BD_OK) return s2;
-      if (e != cudaSuccess) return BD_ERR_CUDA;
+      if (e != cudaSuccess) return cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
       cudaGraphExec_t ex;
       e = cudaGraphInstantiate(&ex, g, 0);
       cudaGraphDestroy(g);
-      if (e != cudaSuccess) return BD_ERR_CUDA;
+      if (e != cudaSuccess) return cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
       c->blk_graph[slot][h] = (void*)ex;
       c->blk_graph_launches[slot][h] = c->launches - l0;
       c->launches = l0;
