@@ -2,21 +2,26 @@
 """Throughput benchmark of the Brownian-dynamics step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0]
+                    [--workload c1|c1s|c2|c3|c0] [--path ...] [--noise-block B]
+                    [--pme-rc RC] [--segment S] [--compare 0|1]
 
 A "step" is one pass of the hydrodynamic step loop over the whole system:
 lattice update, periodic wrap, neighbour check (and rebuild when due),
-spring + excluded-volume + screened-Coulomb forces, Brownian noise,
-mobility rebuild every srpy=100 steps, Brownian displacement, and a
-charge-hop sweep every MStep=100 steps.  The metric is bead-steps/s,
-whole-job (sum over GPUs).
+spring + excluded-volume + Coulomb forces, Brownian noise, mobility rebuild
+every srpy=100 steps, Brownian displacement, and a charge-hop sweep every
+MStep=100 steps.  The metric is bead-steps/s, whole-job (sum over GPUs).
 
 Default workload (c1): planar extension with Kraynik-Reinelt boundaries,
 80 chains x 100 beads (8000 beads), box 60a, Wi = 2, dt = 5e-4, FENE k=30
 Q0=3, WCA, 50% charged, charge hop every 100 steps.  Inputs are seeded
-synthetic chains.  The path timed is the reference-mode step (dense hybrid
-Rotne-Prager-Yamakawa mobility + conformationally averaged TEA noise) with
-Philox Gaussians.
+synthetic chains.  The default path (pme32-learned) computes the
+Ewald-summed Rotne-Prager-Yamakawa mobility by smooth particle-mesh Ewald
+(FP32 grids, cutoff 13.6 with a 64^3 grid, the same interpolation accuracy as
+cutoff 10 with 90^3) and the Brownian displacement sqrt(M) z by a
+preconditioned Lanczos solve at tolerance 1e-6 (learned bead blocks on
+10-bead segment blocks), the displacements of 8 consecutive steps solved by
+one multi-vector Krylov run (noise blocks); --compare 1 also times the plain
+FP64 method (pme64: one solve per step, no preconditioner) on the same grid.
 
 --impl reference times the reference's own CPU code (compiled from its sources
 into oracle/_ref/) on this host's cores for the same workload.
