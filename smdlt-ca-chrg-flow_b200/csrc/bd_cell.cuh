@@ -43,6 +43,27 @@ __device__ __forceinline__ void bspline(double f, int p, double* w) {
   for (int k = 0; k < p; k++) w[k] = a[k];
 }
 
+// bspline with the order known at compile time (loops unrolled, the
+// recursion's arrays in registers).
+template <int P>
+__device__ __forceinline__ void bspline_t(double f, double* w) {
+  double a[P], b[P];
+  a[0] = f;
+  a[1] = 1.0 - f;
+#pragma unroll
+  for (int n = 3; n <= P; n++) {
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+      double hi = k < n - 1 ? a[k] : 0.0, lo = k >= 1 ? a[k - 1] : 0.0;
+      b[k] = ((f + k) * hi + (n - f - k) * lo) / (n - 1);
+    }
+#pragma unroll
+    for (int k = 0; k < n; k++) a[k] = b[k];
+  }
+#pragma unroll
+  for (int k = 0; k < P; k++) w[k] = a[k];
+}
+
 static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
 // Lab-frame cell of the current lattice: columns b1, b2, L e_z with (b1, b2)

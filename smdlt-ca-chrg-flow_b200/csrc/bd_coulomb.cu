@@ -44,16 +44,20 @@ __device__ __forceinline__ void lab_of(double x, double y, double cr, double sr,
 
 // Per charge: base index, B-spline weights of order p and their derivatives
 // d/du M_p(u - g) = M_{p-1}(f + k) - M_{p-1}(f + k - 1) for g = floor(u) - k.
+// One thread per (charge, direction d); the spline order P is a template
+// parameter so the recursion stays in registers.
+template <int P>
 __global__ void k_cw_weights(Cell cell, const double4* __restrict__ cq, int nch, double cr,
-                             double sr, int K, int p, int* base, double* w, double* dw,
-                             int* err) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nch) return;
+                             double sr, int K, int* base, double* w, double* dw, int* err) {
+  constexpr int p = P;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * nch) return;
+  int k = e / 3, d = e % 3;
   double4 q = cq[k];
   double x, y, s[3];
   lab_of(q.x, q.y, cr, sr, x, y);
   frac_of(cell, x, y, q.z, s);
-  for (int d = 0; d < 3; d++) {
+  {
     double sd = s[d] - floor(s[d]);
     double u = sd * K;
     if (!(u >= 0.0 && u <= (double)K)) {
@@ -64,11 +68,12 @@ __global__ void k_cw_weights(Cell cell, const double4* __restrict__ cq, int nch,
     double f = u - fl;
     if (fl >= K) fl -= K;
     base[3 * k + d] = fl;
-    double lo[kMaxOrder], full[kMaxOrder];
-    bspline(f, p - 1, lo);  // M_{p-1}(f + k), k = 0..p-2
-    bspline(f, p, full);
+    double lo[P - 1], full[P];
+    bspline_t<P - 1>(f, lo);  // M_{p-1}(f + k), k = 0..p-2
+    bspline_t<P>(f, full);
     double* wo = w + ((size_t)3 * k + d) * kMaxOrder;
     double* dwo = dw + ((size_t)3 * k + d) * kMaxOrder;
+#pragma unroll
     for (int a = 0; a < p; a++) {
       double hi = a < p - 1 ? lo[a] : 0.0, lm = a >= 1 ? lo[a - 1] : 0.0;
       wo[a] = full[a];
@@ -193,9 +198,10 @@ __global__ void k_cc_fill(const int* __restrict__ cell_of, const int* __restrict
 // Forces on each charge: reciprocal part from the potential grid and the
 // spline derivatives, real-space pairs within rc; adds to the bead forces and
 // writes the charge's real-space energy share (half of its pair sum).
+template <int P>
 __global__ void k_cw_forces(Cell cell, CGeom g, const double4* __restrict__ cq,
                             const int* __restrict__ track, int nch, double cr, double sr, int K,
-                            int p, const int* __restrict__ base, const double* __restrict__ w,
+                            const int* __restrict__ base, const double* __restrict__ w,
                             const double* __restrict__ dw, const double* __restrict__ phi,
                             const int* __restrict__ cell_of, const int* __restrict__ start,
                             const int* __restrict__ idx, double rc2, double beta,
@@ -212,7 +218,11 @@ __global__ void k_cw_forces(Cell cell, CGeom g, const double4* __restrict__ cq,
   const double* d2 = d1 + kMaxOrder;
   int b0 = base[3 * k], b1 = base[3 * k + 1], b2 = base[3 * k + 2];
   double gu0 = 0, gu1 = 0, gu2 = 0;  // dPhi/du_d at the charge
-  for (int e = lane; e < p * p * p; e += 32) {
+  constexpr int p = P;
+#pragma unroll
+  for (int it = 0; it < (p * p * p + 31) / 32; it++) {
+    int e = lane + 32 * it;
+    if (e >= p * p * p) break;
     int c = e % p, b = (e / p) % p, a = e / (p * p);
     int g0 = b0 - a, g1 = b1 - b, g2 = b2 - c;
     g0 += g0 < 0 ? K : 0;
@@ -391,8 +401,15 @@ int coulomb_ewald(bd_ctx* c, const Lat& l, const double4* cq) {
   double* w = c->cw_w;
   double* dw = c->cw_w + 3 * (size_t)nch * kMaxOrder;
   c->launches += 9;
-  k_cw_weights<<<nblk(nch, 128), 128, 0, c->stream>>>(cell, cq, nch, cr, sr, K, p, c->cw_base,
-                                                      w, dw, c->err);
+#define CW_WEIGHTS(P_)                                                                      \
+  k_cw_weights<P_><<<nblk(3 * (long long)nch, 128), 128, 0, c->stream>>>(cell, cq, nch, cr, sr, K, \
+                                                                        c->cw_base, w, dw, c->err)
+  switch (p) {
+    case 4: CW_WEIGHTS(4); break;
+    case 6: CW_WEIGHTS(6); break;
+    default: CW_WEIGHTS(8);
+  }
+#undef CW_WEIGHTS
   CU(cudaMemsetAsync(c->cw_grid, 0, 8 * K3, c->stream));
   k_cw_spread<<<nblk(nch, 8), 256, 0, c->stream>>>(cq, c->cw_base, w, nch, K, p, c->cw_grid);
   CF(cufftExecD2Z((cufftHandle)c->cw_plan_f, c->cw_grid, (cufftDoubleComplex*)c->cw_spec));
@@ -406,10 +423,17 @@ int coulomb_ewald(bd_ctx* c, const Lat& l, const double4* cq) {
   k_cc_scan<<<1, 1024, 0, c->stream>>>(ncell, c->cw_count, c->cw_start, c->cw_cursor);
   k_cc_fill<<<nblk(nch, 256), 256, 0, c->stream>>>(c->cw_cell_of, c->cw_start, c->cw_cursor,
                                                    c->cw_idx, nch);
-  k_cw_forces<<<nblk(nch, 8), 256, 0, c->stream>>>(
-      cell, g, cq, c->track, nch, cr, sr, K, p, c->cw_base, w, dw, c->cw_grid, c->cw_cell_of,
-      c->cw_start, c->cw_idx, rc * rc, c->cw_beta, c->p.lambda_b, c->fx, c->fy, c->fz,
-      c->cw_epart);
+#define CW_FORCES(P_)                                                                        \
+  k_cw_forces<P_><<<nblk(nch, 8), 256, 0, c->stream>>>(                                       \
+      cell, g, cq, c->track, nch, cr, sr, K, c->cw_base, w, dw, c->cw_grid, c->cw_cell_of,    \
+      c->cw_start, c->cw_idx, rc * rc, c->cw_beta, c->p.lambda_b, c->fx, c->fy, c->fz,        \
+      c->cw_epart)
+  switch (p) {
+    case 4: CW_FORCES(4); break;
+    case 6: CW_FORCES(6); break;
+    default: CW_FORCES(8);
+  }
+#undef CW_FORCES
   k_sum_into<<<1, 32, 0, c->stream>>>(c->cw_epart, nch, c->cw_energy);
   c->cw_cell_V = cell.V;
   return launch_ok(c);
