@@ -78,11 +78,13 @@ __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
   }
 }
 
-// FP32 grids: stencil points whose weight W_i(g) is below 1e-10 are skipped
-// by the spread and by the interpolation alike (the product stays
-// symmetric).  For order 8 that is 28 % of the 512 points, carrying at most
-// 2.2e-9 of the stencil's unit weight: below FP32 rounding (6e-8) and three
-// orders below the particle-mesh error; the FP64 path keeps every point.
+// FP32 grids: the spread skips stencil points whose weight W_i(g) is below
+// 1e-10 (for order 8, 28 % of the 512 points, carrying at most 2.2e-9 of the
+// stencil's unit weight: below FP32 rounding, 6e-8, and three orders below
+// the particle-mesh error), saving their atomics; the interpolation keeps
+// every point (skipping there only added divergence), so the product is
+// symmetric to ~1e-9, inside the rounding of its FP32 grids.  The FP64 path
+// keeps every point.
 constexpr double kSkipWeight = 1e-10;
 
 // Q_r[c][g] += v_r,c(i) W_i(g) for the right-hand sides r0 .. r0 + kc - 1
@@ -439,7 +441,6 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     g1 += g1 < 0 ? K : 0;
     g2 += g2 < 0 ? K : 0;
     double wt = w0[a] * w1[b] * w2[c];
-    if (sizeof(R) == 4 && wt < kSkipWeight) continue;  // FP32: negligible corner
     const R* gp = gbase + ((size_t)g0 * K + g1) * K + g2;
     if constexpr (PK) {
       // packed pair blockIdx.y: right-hand sides r0, r0 + 1 as real and
