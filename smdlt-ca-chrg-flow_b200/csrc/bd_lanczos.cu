@@ -4,8 +4,9 @@
 // The reference draws its Brownian displacement with the conformationally
 // averaged truncated-expansion approximation (updateHI,
 // shear/src/main26.c:745-857).  This path computes sqrt(M) z itself:
-// Lanczos on M from v_1 = z/|z| with full reorthogonalisation in FP64
-// (classical Gram-Schmidt, applied twice), T_m = V_m^T M V_m tridiagonal,
+// Lanczos on M from v_1 = z/|z| with full reorthogonalisation in FP64 (the
+// three-term recurrence, then one classical Gram-Schmidt pass against the
+// whole basis), T_m = V_m^T M V_m tridiagonal,
 // sqrt(M) z ~= |z| V_m T_m^(1/2) e_1, stopped when the relative change of the
 // iterate between successive m is below the tolerance (the criterion of Ando,
 // Chow and Skolnick, J. Chem. Phys. 137, 064106 (2012)).  T_m^(1/2) e_1 comes
@@ -195,23 +196,51 @@ struct Kry {
 // The iteration index j lives on the device (*jd) so that one iteration's
 // launches are the same every iteration and can be replayed as a CUDA graph;
 // k_next_j advances it at the end of the iteration.
+// Lanczos step j with full reorthogonalisation: the three-term recurrence
+// w -= alpha v_j + beta_{j-1} v_{j-1} (alpha = v_j . w), then one classical
+// Gram-Schmidt pass against the whole basis, w -= V (V^T w), whose
+// coefficient on v_j corrects alpha.  Two passes over the basis per step.
+//   k_orth0: partial v_j . w per chunk
+//   k_orth1: alpha; three-term update; partial V^T w per chunk
+//   k_orth2: d = V^T w; w -= V d; |w|^2 partials; alpha_j = alpha + d_j
+//   k_orth3: beta_j = |w|; v_{j+1} = w / beta_j
 __global__ void __launch_bounds__(256) k_orth0(Kry q) {
-  int r = blockIdx.y, nv = *q.jd + 1, lo, hi;
+  __shared__ double red[8];
+  int r = blockIdx.y, j = *q.jd, lo, hi;
+  const double* vj = q.V + (size_t)r * q.n + (size_t)j * q.bs;
+  const double* w = q.w + (size_t)r * q.n;
   chunk_range(q.n, lo, hi);
-  chunk_dots(q.V + (size_t)r * q.n, q.bs, nv, q.w + (size_t)r * q.n, lo, hi,
-             q.part1 + r * q.pst);
+  double s = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) s += vj[i] * w[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int p = 0; p < (int)(blockDim.x >> 5); p++) t += red[p];
+    q.part1[r * q.pst + blockIdx.x] = t;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_orth1(Kry q) {
-  __shared__ double h[kMaxKrylov + 1];
-  int r = blockIdx.y, nv = *q.jd + 1, lo, hi;
+  __shared__ double sa;
+  int r = blockIdx.y, j = *q.jd, nv = j + 1, lo, hi;
   const double* V = q.V + (size_t)r * q.n;
   double* w = q.w + (size_t)r * q.n;
   chunk_range(q.n, lo, hi);
-  sum_parts(q.part1 + r * q.pst, nv, h);
-  if (blockIdx.x == 0)
-    for (int k = threadIdx.x; k < nv; k += blockDim.x) q.hsave[(size_t)r * q.hst + k] = h[k];
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) w[i] -= combo_row(V, q.bs, h, nv, i);
+  if (threadIdx.x < 32) {
+    double a = warp_sum_parts(q.part1 + r * q.pst, gridDim.x, 1);
+    if (threadIdx.x == 0) {
+      sa = a;
+      if (blockIdx.x == 0) q.hsave[(size_t)r * q.hst + j] = a;
+    }
+  }
+  __syncthreads();
+  double alpha = sa, bprev = j > 0 ? q.beta[(size_t)(j - 1) * q.kst + r] : 0.0;
+  const double* vj = V + (size_t)j * q.bs;
+  const double* vp = V + (size_t)(j > 0 ? j - 1 : 0) * q.bs;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x)
+    w[i] = w[i] - alpha * vj[i] - bprev * vp[i];
   __syncthreads();
   chunk_dots(V, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
 }
@@ -444,7 +473,7 @@ int alloc_lanczos(bd_ctx* c) {
 
 // One Lanczos iteration's launches: w = A v with v = vcur (A = M, or
 // G M G^T with the block preconditioner when pre; with force also M F into
-// c->MF), CGS2 against the basis, beta, v_{j+1}, j += 1.  Every argument is
+// c->MF), reorthogonalisation against the basis, beta, v_{j+1}, j += 1.  Every argument is
 // the same in every iteration (the index j is read on the device), so the
 // launches can be captured once and replayed as a CUDA graph.
 static int lanczos_iteration(bd_ctx* c, bool pre, bool force) {
@@ -616,7 +645,7 @@ void lanczos_graphs_reset(bd_ctx* c) {
 // steps by one Lanczos run over k right-hand sides.  Each right-hand side has
 // its own basis, coefficients and stopping point; they share the launches
 // (the particle-mesh product of 3 k grids, the preconditioner blocks and the
-// CGS2 kernels with blockIdx.y = r), which turns k latency-bound iterations
+// orthogonalisation kernels with blockIdx.y = r), which turns k latency-bound iterations
 // into one.  The host checks convergence for all right-hand sides at once,
 // one iteration behind the device (the next iteration is already queued
 // while the tridiagonal problems are solved, on several host threads).
@@ -675,7 +704,7 @@ void noise_blocks_release(bd_ctx* c) {
   c->blk_next = 0;
 }
 
-// Chunks per right-hand side of the block CGS2 kernels.
+// Chunks per right-hand side of the block orthogonalisation kernels.
 static int block_chunks(int k) { return std::min(kDotBlocks, std::max(8, 4 * kDotBlocks / k)); }
 
 // Layout of a block of k right-hand sides: basis vector j of r at
@@ -703,7 +732,7 @@ static Kry block_kry(bd_ctx* c, int k) {
 }
 
 // One iteration of the block, in two parts: the product W = A V_cur for the
-// k inputs (part 0), then CGS2 of each against its own basis, beta, next
+// k inputs (part 0), then the orthogonalisation of each against its own basis, beta, next
 // vectors, j += 1 (part 1).  The same launches every iteration (j is read on
 // the device), so each part can be captured as a graph; the product is timed
 // on its own (BD_PROF_BLOCK) between the two.
