@@ -857,6 +857,10 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
   const double* hb = c->Bhost + (size_t)L1 * k;
   // convergence of every open right-hand side at Krylov dimension mm, from the
   // alpha and beta copied after iteration mm
+  // the square root at the previous check, reused as the m - 1 iterate when
+  // the checks are consecutive
+  std::vector<std::vector<double>> clast(k);
+  std::vector<int> mlast(k, -1);
   auto evaluate = [&](int mm) -> int {
     CU(cudaEventSynchronize(ev));
     std::vector<int> open;
@@ -871,7 +875,10 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
       }
       std::vector<double> cm;
       int neg = sqrt_e1(alpha, beta, mm, cm, 0.5);
-      sqrt_e1(alpha, beta, mm - 1, cprev, 0.5);
+      if (mlast[r] == mm - 1)
+        cprev.swap(clast[r]);
+      else
+        sqrt_e1(alpha, beta, mm - 1, cprev, 0.5);
       double dn = 0, cn = 0;
       for (int i = 0; i < mm; i++) {
         double prev = i < mm - 1 ? cprev[i] : 0.0;
@@ -885,6 +892,9 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
         mr[r] = mm;
         negs[r] = neg;
         cc[r].swap(cm);
+      } else {
+        clast[r].swap(cm);
+        mlast[r] = mm;
       }
     });
     ndone = 0;
@@ -910,7 +920,7 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
                          cudaMemcpyDeviceToHost, st));
       CU(cudaEventRecord(ev, st));
       pending = m;
-      next_check = m + 2;
+      next_check = m + 1;  // from the first check on, every iteration
     }
   }
   if (pending && (s = evaluate(pending)) != BD_OK) return s;
