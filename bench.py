@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload c1|c1s|c2|c3|c0] [--path ...] [--noise-block B]
-                    [--pme-rc RC] [--segment S] [--compare 0|1]
+                    [--pme-rc RC] [--pme-grid K] [--segment S] [--compare 0|1]
 
 A "step" is one pass of the hydrodynamic step loop over the whole system:
 lattice update, periodic wrap, neighbour check (and rebuild when due),
@@ -16,8 +16,8 @@ Default workload (c1): planar extension with Kraynik-Reinelt boundaries,
 Q0=3, WCA, 50% charged, charge hop every 100 steps.  Inputs are seeded
 synthetic chains.  The default path (pme32-learned) computes the
 Ewald-summed Rotne-Prager-Yamakawa mobility by smooth particle-mesh Ewald
-(FP32 grids, cutoff 13.6 with a 64^3 grid, the same interpolation accuracy as
-cutoff 10 with 90^3) and the Brownian displacement sqrt(M) z by a
+(FP32 grids, cutoff 12.1 with a 64^3 grid, the same interpolation accuracy as
+cutoff 10 with 80^3) and the Brownian displacement sqrt(M) z by a
 preconditioned Lanczos solve at tolerance 1e-6 (learned bead blocks on
 10-bead segment blocks), the displacements of 8 consecutive steps solved by
 one multi-vector Krylov run (noise blocks); --compare 1 also times the plain
@@ -280,7 +280,7 @@ PATHS = {
     # the reference-physics paths).  The dense-tile paths
     # keep the reference's (Debye-Hueckel, unsigned charges, sequential sweep).
     # the same Ewald sum applied matrix-free by smooth particle-mesh Ewald
-    # (grid 1.45 L, B-spline order 8, real-space cutoff 10)
+    # (B-spline order 8; grid and real-space cutoff from --pme-rc / --pme-grid)
     "pme64": dict(mobility="pme", precision="fp64", step="lanczos", bytes_per_block=None,
                   physics="north"),
     # the same in FP32 storage (grids, FFTs, influence, pair tensors) with FP64
@@ -363,13 +363,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0):
+def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pme_grid=0):
     """Times K steps of one path after W warm-up steps; returns a dict."""
     import torch
     N = w["Nb"] * w["Nc"]
     pp = PATHS[path]
     nb = noise_block if pp["mobility"] == "pme" else 1
-    extra = dict(noise_block=nb, pme_rc=pme_rc) if pp["mobility"] == "pme" else {}
+    extra = (dict(noise_block=nb, pme_rc=pme_rc, pme_grid=pme_grid)
+             if pp["mobility"] == "pme" else {})
     c = build_context(w, 1000 + rank, path, **extra)
     step = c.step_lanczos if pp["step"] == "lanczos" else c.step_reference
     step(0, W, True)
@@ -427,7 +428,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0):
         # bead vectors and weights 48 N (s/4) plus 8 passes over 3 grids
         # 96 K^3 (s/4)
         import bd_b200 as B
-        Kg = B.pme_default_grid(w["L"], pme_rc)
+        Kg = pme_grid or B.pme_default_grid(w["L"], pme_rc)
         sb = 8 if pp["precision"] == "fp64" else 4
         alg_bytes = (48 * N + 96 * Kg ** 3) * sb / 4
     else:
@@ -578,7 +579,8 @@ def run_ours(args, rank, world, dist):
     K, W = args.steps, args.warmup
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps, args.noise_block, args.pme_rc)
+    main = measure(w, args.path, K, W, rank, dist, args.e2e_steps, args.noise_block, args.pme_rc,
+                   args.pme_grid)
     value = world * N * K / (main["t_max_ms"] / 1e3)
     peak, kind = peaks()
     pme = PATHS[args.path]["mobility"] == "pme"
@@ -610,7 +612,8 @@ def run_ours(args, rank, world, dist):
             "data": "synthetic",
             "config": {"workload": w["name"], "beads": N, "path": args.path,
                        "mobility": ("Ewald-summed RPY by smooth PME, grid %d^3, order 8, cutoff %g"
-                                    % (__import__("bd_b200").pme_default_grid(w["L"], args.pme_rc),
+                                    % (args.pme_grid or
+                                       __import__("bd_b200").pme_default_grid(w["L"], args.pme_rc),
                                        args.pme_rc) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
                        "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation" +
@@ -641,7 +644,7 @@ def run_ours(args, rank, world, dist):
     plain = "pme64" if pme else "lanczos64"
     if args.compare and args.path != plain:
         # the plain method: same mobility in FP64, no preconditioner
-        ref64 = measure(w, plain, K, W, rank, dist, 1, 1, args.pme_rc)
+        ref64 = measure(w, plain, K, W, rank, dist, 1, 1, args.pme_rc, args.pme_grid)
         line["plain_fp64"] = {"path": plain, "value": world * N * K / (ref64["t_max_ms"] / 1e3),
                               "ms_per_step": ref64["t_max_ms"] / K,
                               "lanczos_iters_per_step": ref64["lanczos_iters_per_step"],
@@ -663,9 +666,12 @@ def main():
     ap.add_argument("--noise-block", type=int, default=8,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
-    ap.add_argument("--pme-rc", type=float, default=13.6,
-                    help="particle-mesh real-space cutoff; the grid follows it (14.5 L / rc "
+    ap.add_argument("--pme-rc", type=float, default=12.1,
+                    help="particle-mesh real-space cutoff; the grid follows it (12.9 L / rc "
                          "points, constant interpolation accuracy)")
+    ap.add_argument("--pme-grid", type=int, default=0,
+                    help="particle-mesh grid points per cell edge (0: the library's rule "
+                         "for the cutoff)")
     ap.add_argument("--segment", type=int, default=10,
                     help="beads per segment block of the preconditioned paths")
     ap.add_argument("--compare", type=int, default=1,

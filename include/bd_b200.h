@@ -123,8 +123,9 @@ typedef struct {
   double lanczos_tol;        /* relative change of sqrt(M) z between iterations; 0 -> 1e-6 */
   int lanczos_max;           /* Krylov dimension cap, at most 400; 0 -> 200 */
   /* BD_MOB_PME discretisation (no reference counterpart): grid points per
-   * reduced lattice direction (0 -> smallest 2^a 3^b 5^c >= 14.5 L / rc,
-   * i.e. 1.45 L at the default cutoff 10: spacing proportional to the cutoff),
+   * reduced lattice direction (0 -> smallest 2^a 3^b 5^c >= 12.9 L / rc,
+   * i.e. 1.29 L at the default cutoff 10: spacing proportional to the cutoff,
+   * split parameter times spacing at most 0.31),
    * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> the smaller
    * of 10 and 0.43 L; at most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
    * real-space pairs per bead (0 -> 2.5 times the mean number of beads within
@@ -385,7 +386,7 @@ int bd_batch_create(bd_ctx *const *ctxs, int n, bd_batch **out);
 int bd_batch_step_lanczos(bd_batch *batch, unsigned long t0, int nsteps, int with_hop);
 int bd_batch_destroy(bd_batch *batch);
 /* Particle-mesh grid for a box of edge L: of the 2^a 3^b 5^c sizes between
- * 1.45 L (the accuracy bound of the default discretisation) and 25 % above,
+ * 1.29 L (the accuracy bound of the default discretisation) and 25 % above,
  * the one with the fastest three-component FFT round trip on the current
  * device (bd_precision for the storage); results are cached per process. */
 int bd_autotune_pme_grid(double L, int precision, int *K_out);

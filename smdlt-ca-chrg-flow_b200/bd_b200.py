@@ -308,11 +308,12 @@ def train_preconditioner(ctx, configs, steps_per_config=20, lr=3e-3, seed=0, ste
 
 def pme_default_grid(L, rc=None):
     """bd_create's default particle-mesh grid: the smallest 2^a 3^b 5^c at or
-    above 14.5 L / rc (cuFFT is markedly slower on sizes with a factor 7); rc
-    defaults to the smaller of 10 and 0.43 L, giving 1.45 L at rc = 10."""
+    above 12.9 L / rc (split parameter 4 / rc times spacing at most 0.31; cuFFT
+    is markedly slower on sizes with a factor 7); rc defaults to the smaller of
+    10 and 0.43 L, giving 1.29 L at rc = 10."""
     if rc is None:
         rc = min(10.0, 0.43 * L)
-    K = int(np.ceil(14.5 * L / rc - 1e-9))
+    K = int(np.ceil(12.9 * L / rc - 1e-9))
     while True:
         r = K
         for f in (2, 3, 5):

@@ -10,7 +10,7 @@
 // when every replica has finished, with the first failing replica's status.
 //
 // bd_autotune_pme_grid picks the particle-mesh grid for a box: among the
-// FFT-friendly sizes (2^a 3^b 5^c) from the accuracy bound 1.45 L up to 25 %
+// FFT-friendly sizes (2^a 3^b 5^c) from the accuracy bound 1.29 L up to 25 %
 // above it, the one whose batched three-component R2C + C2R round trip is
 // fastest on this GPU (timed with CUDA events, cached per size and
 // precision).
@@ -121,7 +121,7 @@ int bd_autotune_pme_grid(double L, int precision, int* K_out) {
   if (!(L > 0) || !K_out || precision < 0 || precision > 1) return BD_ERR_ARG;
   static std::mutex mu;
   static std::map<std::pair<int, int>, float> cache;  // (K, precision) -> ms
-  int K0 = (int)ceil(1.45 * L), K1 = (int)ceil(1.25 * K0);
+  int K0 = (int)ceil(1.29 * L), K1 = (int)ceil(1.25 * K0);
   std::vector<int> cand;
   for (int K = K0; K <= std::max(K1, K0); K++) {
     int r = K;

@@ -611,12 +611,13 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   // smooth-PME discretisation
   {
     // default grid: spacing proportional to the cutoff (the split parameter is
-    // 4 / rc, so alpha h stays 0.276 and the interpolation error stays that of
-    // 1.45 L points at rc = 10); the smallest 2^a 3^b 5^c at or above it
+    // 4 / rc, so alpha h stays at most 0.31 and the error at most 3e-6 of the
+    // converged Ewald sum, 1.29 L points at rc = 10); the smallest 2^a 3^b 5^c
+    // at or above it
     double rc0 = p->pme_rc > 0 ? p->pme_rc : std::min(10.0, 0.43 * p->L);
     int K = p->pme_grid;
     if (K <= 0) {
-      K = (int)ceil(14.5 * p->L / rc0 - 1e-9);
+      K = (int)ceil(12.9 * p->L / rc0 - 1e-9);
       for (;; K++) {
         int r = K;
         for (int f : {2, 3, 5})

@@ -8,7 +8,7 @@ counterpart).
   relative after a few steps, also with noise blocks (every replica solving
   several steps' displacements per Krylov run while the others capture and
   replay their own iterations);
-* the autotuned grid is a 2^a 3^b 5^c size within [1.45 L, 1.25 x 1.45 L].
+* the autotuned grid is a 2^a 3^b 5^c size within [1.29 L, 1.25 x 1.29 L].
 """
 import numpy as np
 import pytest
@@ -80,4 +80,4 @@ def test_autotuned_grid(L):
     for f in (2, 3, 5):
         while r % f == 0:
             r //= f
-    assert r == 1 and np.ceil(1.45 * L) <= K <= np.ceil(1.25 * np.ceil(1.45 * L))
+    assert r == 1 and np.ceil(1.29 * L) <= K <= np.ceil(1.25 * np.ceil(1.29 * L))

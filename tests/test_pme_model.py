@@ -9,9 +9,13 @@
   longer holds every k inside its cutoff once the cell is strongly skewed:
   there the dense sum is 1e-4 to 2e-3 from the converged one, which the
   model (and the CUDA particle-mesh path) follow instead;
-* its smooth-PME sum at the default discretisation (grid 1.45 L, order 8,
-  cutoff 10, split 0.4) against that Ewald sum, 1e-5 relative, in shear and
-  in planar extension at several points of the lattice period;
+* its smooth-PME sum (grid 1.5 L, order 8, cutoff 10, split 0.4) against
+  that Ewald sum, 1e-5 relative, in shear and in planar extension at several
+  points of the lattice period;
+* the default grid rule at its accuracy bound (12.9 L / rc points: split
+  parameter 4 / rc times spacing 0.31 at L = 30, rc = 12.9, K = 30): within
+  5e-6 of the converged Ewald sum over the lattice period of both flows
+  (3.3e-6 at most on these systems);
 * the Gauss-reduced cell spans the same lattice.
 """
 import numpy as np
@@ -59,6 +63,23 @@ def test_pme_model_vs_ewald_model(flow, t):
     ref = P.ewald_apply(H, pos, v, alpha=ar, tol_exp=30.0) - v @ P.self_offdiag(H, ar, 30.0).T
     got = P.pme_apply(H, pos, v, K=45, p=8, alpha=0.4, rc=10.0, alpha_ref=ar)
     assert rel_err(got, ref) < 1e-5
+
+
+@pytest.mark.parametrize("flow", [0, 1])
+@pytest.mark.parametrize("frac", [0.0, 0.25, 0.5, 0.7, 0.9])
+def test_default_grid_rule_accuracy(flow, frac):
+    L, rc = 30.0, 12.9
+    K = B.pme_default_grid(L, rc)
+    assert K == 30 and abs(4.0 / rc * L / K - 0.31) < 1e-3
+    o = O.Oracle(flow, 25, 8, L, 0.2, 5e-4)
+    t = int(frac * o.s.tp)
+    o, _, pos = _system(flow, t, seed=41)
+    v = np.random.default_rng(5).normal(size=(o.N, 3))
+    ar = P.ref_alpha(t, o.s.tp, o.s.L2yp)
+    H = P.reduced_cell(list(o.s.L1), list(o.s.L2), L)
+    ref = P.ewald_apply(H, pos, v, alpha=ar, tol_exp=30.0) - v @ P.self_offdiag(H, ar, 30.0).T
+    got = P.pme_apply(H, pos, v, K=K, p=8, alpha=4.0 / rc, rc=rc, alpha_ref=ar)
+    assert rel_err(got, ref) < 5e-6
 
 
 @pytest.mark.parametrize("flow,t", [(0, 7000), (1, 5000)])
