@@ -265,6 +265,11 @@ long long bd_launch_count(const bd_ctx *ctx);
 /* out = M v for a host vector v[3N] (bead-interleaved), using the mobility of
  * the last bd_calc_hi (diagonal blocks included). */
 int bd_mobility_apply(bd_ctx *ctx, const double *v, double *out);
+/* out_r = M v_r for k host vectors (v[r 3N + 3 i + a], out likewise), the
+ * product the noise blocks use: with BD_MOB_PME and 2 <= k <= noise_block the
+ * right-hand sides go through the particle-mesh transforms together, packed
+ * in complex pairs; otherwise one product each. */
+int bd_mobility_apply_block(bd_ctx *ctx, int k, const double *v, double *out);
 /* out = sqrt(M) z by Lanczos with full FP64 reorthogonalisation, stopped when
  * the relative change between successive iterates is below lanczos_tol;
  * *iters receives the Krylov dimension used. */

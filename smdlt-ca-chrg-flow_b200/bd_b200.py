@@ -135,6 +135,7 @@ def _lib() -> C.CDLL:
         L.bd_download_hop_log.argtypes = [vp, _ip]
         L.bd_step_reference.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
         L.bd_mobility_apply.argtypes = [vp, _dp, _dp]
+        L.bd_mobility_apply_block.argtypes = [vp, C.c_int, _dp, _dp]
         L.bd_lanczos_sqrt.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
         L.bd_lanczos_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
         L.bd_noise_block_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
@@ -498,6 +499,14 @@ class Context:
     def mobility_apply(self, v):
         out = np.zeros(3 * self.N)
         self._call("bd_mobility_apply", np.ascontiguousarray(v, np.float64), out)
+        return out
+
+    def mobility_apply_block(self, V):
+        """M v_r for the rows v_r of V (k x 3N, bead-interleaved), through the
+        noise blocks' multi-vector product where it applies."""
+        V = np.ascontiguousarray(V, np.float64)
+        out = np.zeros_like(V)
+        self._call("bd_mobility_apply_block", V.shape[0], V.reshape(-1), out.reshape(-1))
         return out
 
     def lanczos_sqrt(self, z):

@@ -1058,6 +1058,47 @@ int bd_mobility_apply(bd_ctx* c, const double* v, double* out) {
   return BD_OK;
 }
 
+int bd_mobility_apply_block(bd_ctx* c, int k, const double* v, double* out) {
+  if (!c || !v || !out || k < 1) return BD_ERR_ARG;
+  if (!c->hi_built) return BD_ERR_STATE;
+  if (!(c->p.mobility == BD_MOB_PME && k >= 2 && k <= c->nbk)) {
+    for (int r = 0; r < k; r++) {
+      int s = bd_mobility_apply(c, v + 3 * (size_t)r * c->N, out + 3 * (size_t)r * c->N);
+      if (s != BD_OK) return s;
+    }
+    return BD_OK;
+  }
+  int s;
+  if ((s = pme_multi_plan(c, k)) != BD_OK) return s;
+  int N = c->N, NTp = c->NT * 32;
+  size_t n = 3 * (size_t)NTp;
+  std::vector<double> soa(n * k, 0.0), res(n * k);
+  for (int r = 0; r < k; r++)
+    for (int i = 0; i < N; i++)
+      for (int a = 0; a < 3; a++) soa[r * n + (size_t)a * NTp + i] = v[(size_t)r * 3 * N + 3 * i + a];
+  double *X = nullptr, *Y = nullptr;
+  if (cudaMalloc(&X, 8 * n * k) != cudaSuccess || cudaMalloc(&Y, 8 * n * k) != cudaSuccess) {
+    cudaFree(X);
+    return BD_ERR_OOM;
+  }
+  cudaError_t e = cudaMemcpyAsync(X, soa.data(), 8 * n * k, cudaMemcpyHostToDevice, c->stream);
+  s = e == cudaSuccess ? pme_apply_multi(c, k, X, n, Y, n)
+                       : bd::cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
+  if (s == BD_OK) {
+    e = cudaMemcpyAsync(res.data(), Y, 8 * n * k, cudaMemcpyDeviceToHost, c->stream);
+    s = e == cudaSuccess ? check(c)
+                         : bd::cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  cudaStreamSynchronize(c->stream);
+  cudaFree(X);
+  cudaFree(Y);
+  if (s != BD_OK) return s;
+  for (int r = 0; r < k; r++)
+    for (int i = 0; i < N; i++)
+      for (int a = 0; a < 3; a++) out[(size_t)r * 3 * N + 3 * i + a] = res[r * n + (size_t)a * NTp + i];
+  return BD_OK;
+}
+
 int bd_lanczos_sqrt(bd_ctx* c, const double* z, double* out, int* iters) {
   if (!c || !z || !out) return BD_ERR_ARG;
   int s;

@@ -16,6 +16,12 @@ No reference counterpart; checked against
   accumulation) against the FP64 path, 1e-5 relative;
 * the dense square root: Lanczos sqrt(M) z with the PME product against
   numpy.linalg.eigh of the dense Ewald matrix, 3e-5 relative;
+* the noise blocks' multi-vector product (bd_mobility_apply_block: right-hand
+  sides packed in complex pairs, in-place complex transforms, influence on
+  the full spectrum) against one product per vector (real-to-complex
+  transforms), FP64 1e-12, FP32 2e-6, and FP32 blocks against FP64 single
+  products 1e-5, with an odd number of vectors (a lone right-hand side in the
+  last pair);
 * a few hundred Krylov Brownian steps with the PME mobility run without error.
 """
 import numpy as np
@@ -110,6 +116,21 @@ def test_pme_fp32_storage(flow, t):
     assert err < 1e-5, err
     Mf = O.full_mobility(o.calc_hi_ewald(x, y, z), o.N)
     assert rel_err(c32.mobility_apply(v), Mf @ v) < 2e-5
+
+
+@pytest.mark.parametrize("precision,K,tol", [("fp32", 64, 2e-6), ("fp32", 40, 2e-6),
+                                             ("fp64", 64, 1e-12)])
+@pytest.mark.parametrize("flow,t", [(0, 3000), (1, 7000)])
+def test_block_product_matches_single(precision, K, tol, flow, t):
+    c, o, _ = _prepared(flow, t, precision=precision, pme_grid=K, noise_block=8)
+    V = np.random.default_rng(7).normal(size=(7, 3 * o.N))
+    got = c.mobility_apply_block(V)
+    errs = [rel_err(got[r], c.mobility_apply(V[r])) for r in range(7)]
+    assert max(errs) < tol, errs
+    if precision == "fp32":
+        c64, _, _ = _prepared(flow, t, pme_grid=K)
+        errs = [rel_err(got[r], c64.mobility_apply(V[r])) for r in range(7)]
+        assert max(errs) < 1e-5, errs
 
 
 def test_pme_rejects_dense_download():
