@@ -199,14 +199,14 @@ __global__ void k_cc_fill(const int* __restrict__ cell_of, const int* __restrict
 // spline derivatives, real-space pairs within rc; adds to the bead forces and
 // writes the charge's real-space energy share (half of its pair sum).
 template <int P>
-__global__ void k_cw_forces(Cell cell, CGeom g, const double4* __restrict__ cq,
-                            const int* __restrict__ track, int nch, double cr, double sr, int K,
-                            const int* __restrict__ base, const double* __restrict__ w,
-                            const double* __restrict__ dw, const double* __restrict__ phi,
-                            const int* __restrict__ cell_of, const int* __restrict__ start,
-                            const int* __restrict__ idx, double rc2, double beta,
-                            double lambda_b, double* fx, double* fy, double* fz,
-                            double* ereal) {
+__global__ void __launch_bounds__(256)
+    k_cw_forces(Cell cell, CGeom g, const double4* __restrict__ cq, const int* __restrict__ track,
+                int nch, double cr, double sr, int K, const int* __restrict__ base,
+                const double* __restrict__ w, const double* __restrict__ dw,
+                const double* __restrict__ phi, const int* __restrict__ cell_of,
+                const int* __restrict__ start, const int* __restrict__ idx, double rc2,
+                double beta, double lambda_b, double* fx, double* fy, double* fz,
+                double* ereal) {
   int k = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (k >= nch) return;
   double4 me = cq[k];
@@ -246,37 +246,60 @@ __global__ void k_cw_forces(Cell cell, CGeom g, const double4* __restrict__ cq,
     lo[d] = g.n[d] >= 3 ? -1 : 0;
     hi[d] = g.n[d] >= 3 ? 1 : g.n[d] - 1;
   }
-  for (int a = lo[0]; a <= hi[0]; a++)
-    for (int b = lo[1]; b <= hi[1]; b++)
-      for (int c = lo[2]; c <= hi[2]; c++) {
-        int e0 = g.n[0] >= 3 ? (cd[0] + a + g.n[0]) % g.n[0] : a;
-        int e1 = g.n[1] >= 3 ? (cd[1] + b + g.n[1]) % g.n[1] : b;
-        int e2 = g.n[2] >= 3 ? (cd[2] + c + g.n[2]) % g.n[2] : c;
-        int cc = (e0 * g.n[1] + e1) * g.n[2] + e2;
-        int s0 = start[cc], s1 = start[cc + 1];
-        for (int q = s0 + lane; q < s1; q += 32) {
-          int j = idx[q];
-          if (j == k) continue;
-          double4 ot = cq[j];
-          double xj, yj;
-          lab_of(ot.x, ot.y, cr, sr, xj, yj);
-          double dx = xi - xj, dy = yi - yj, dz = zi - ot.z, s[3];
-          frac_of(cell, dx, dy, dz, s);
-          for (int d = 0; d < 3; d++) s[d] -= rint(s[d]);
-          dx = cell.H[0] * s[0] + cell.H[1] * s[1] + cell.H[2] * s[2];
-          dy = cell.H[3] * s[0] + cell.H[4] * s[1] + cell.H[5] * s[2];
-          dz = cell.H[6] * s[0] + cell.H[7] * s[1] + cell.H[8] * s[2];
-          double rr = dx * dx + dy * dy + dz * dz;
-          if (rr >= rc2) continue;
-          double r = sqrt(rr), qq = lambda_b * me.w * ot.w;
-          double ec = erfc(beta * r) / r;
-          double fr = qq * (ec + 2.0 * beta / rtpi * exp(-beta * beta * rr)) / rr;
-          f0 += fr * dx;
-          f1 += fr * dy;
-          f2 += fr * dz;
-          en += 0.5 * qq * ec;
-        }
-      }
+  // the (at most 27) neighbour cells as one candidate list: lane l < ncell
+  // takes cell l's range; a warp scan of the counts places candidate m in
+  // the cell whose range holds it, so the lanes walk all cells at once (no
+  // chain of dependent loads per cell)
+  __shared__ int c_start[8][32], c_excl[8][32], c_incl[8][32];
+  const int wl = threadIdx.x >> 5;
+  int nd[3] = {hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1};
+  int ncell = nd[0] * nd[1] * nd[2];
+  int my_s = 0, my_n = 0;
+  if (lane < ncell) {
+    int a = lo[0] + lane / (nd[1] * nd[2]), b = lo[1] + (lane / nd[2]) % nd[1],
+        c = lo[2] + lane % nd[2];
+    int e0 = g.n[0] >= 3 ? (cd[0] + a + g.n[0]) % g.n[0] : a;
+    int e1 = g.n[1] >= 3 ? (cd[1] + b + g.n[1]) % g.n[1] : b;
+    int e2 = g.n[2] >= 3 ? (cd[2] + c + g.n[2]) % g.n[2] : c;
+    int cc = (e0 * g.n[1] + e1) * g.n[2] + e2;
+    my_s = start[cc];
+    my_n = start[cc + 1] - my_s;
+  }
+  int incl = my_n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  c_start[wl][lane] = my_s;
+  c_excl[wl][lane] = incl - my_n;
+  c_incl[wl][lane] = incl;
+  __syncwarp();
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  int cl = 0;
+  for (int m = lane; m < total; m += 32) {
+    while (m >= c_incl[wl][cl]) cl++;  // ends at the last cell: m < total
+    int j = idx[c_start[wl][cl] + (m - c_excl[wl][cl])];
+    if (j == k) continue;
+    double4 ot = cq[j];
+    double xj, yj;
+    lab_of(ot.x, ot.y, cr, sr, xj, yj);
+    double dx = xi - xj, dy = yi - yj, dz = zi - ot.z, s[3];
+    frac_of(cell, dx, dy, dz, s);
+    for (int d = 0; d < 3; d++) s[d] -= rint(s[d]);
+    dx = cell.H[0] * s[0] + cell.H[1] * s[1] + cell.H[2] * s[2];
+    dy = cell.H[3] * s[0] + cell.H[4] * s[1] + cell.H[5] * s[2];
+    dz = cell.H[6] * s[0] + cell.H[7] * s[1] + cell.H[8] * s[2];
+    double rr = dx * dx + dy * dy + dz * dz;
+    if (rr >= rc2) continue;
+    double r = sqrt(rr), qq = lambda_b * me.w * ot.w;
+    double ec = erfc(beta * r) / r;
+    double fr = qq * (ec + 2.0 * beta / rtpi * exp(-beta * beta * rr)) / rr;
+    f0 += fr * dx;
+    f1 += fr * dy;
+    f2 += fr * dz;
+    en += 0.5 * qq * ec;
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     gu0 += __shfl_xor_sync(0xffffffffu, gu0, o);

@@ -18,10 +18,10 @@
 #include <string.h>
 
 #include <algorithm>
-#include <thread>
 #include <vector>
 
 #include "bd_ctx.cuh"
+#include "bd_hostpool.h"
 
 using namespace bd;
 
@@ -813,21 +813,10 @@ static int block_iteration(bd_ctx* c, int k, bool pre) {
   return BD_OK;
 }
 
-// f(i) for i < n on up to 16 host threads.
+// f(i) for i < n on the calling thread and the process's host workers.
 template <class F>
 static void parallel_for(int n, F f) {
-  int nt = std::min(n, (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-  if (nt <= 1) {
-    for (int i = 0; i < n; i++) f(i);
-    return;
-  }
-  std::vector<std::thread> th;
-  for (int t = 1; t < nt; t++)
-    th.emplace_back([&f, t, nt, n] {
-      for (int i = t; i < n; i += nt) f(i);
-    });
-  for (int i = 0; i < n; i += nt) f(i);
-  for (auto& x : th) x.join();
+  HostPool::get().run(n, f);
 }
 
 // Lanczos for sqrt(A) z_r, r < k, z_r = BR + 3 N r; the results
