@@ -395,6 +395,11 @@ int bd_batch_destroy(bd_batch *batch);
  * the one with the fastest three-component FFT round trip on the current
  * device (bd_precision for the storage); results are cached per process. */
 int bd_autotune_pme_grid(double L, int precision, int *K_out);
+/* The default particle-mesh grid bd_create picks for a box of edge L and a
+ * real-space cutoff rc (rc <= 0: the default cutoff, the smaller of 10 and
+ * 0.43 L): the smallest 2^a 3^b 5^c >= 12.9 L / rc.  Host arithmetic only
+ * (no device needed); BD_ERR_ARG for L <= 0 or a grid above 4096. */
+int bd_pme_default_grid(double L, double rc, int *K_out);
 
 /* ---- learned preconditioner network (no reference counterpart) ----------
  * Per bead, the BD_MPNN_NEIGHBORS nearest beads within BD_MPNN_CUTOFF

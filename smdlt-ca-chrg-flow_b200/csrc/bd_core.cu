@@ -538,6 +538,27 @@ extern "C" {
 
 const char* bd_last_error_detail(void) { return g_detail; }
 
+// Spacing proportional to the cutoff: the split parameter is 4 / rc, so
+// alpha h stays at most 0.31, within 3.3e-6 of the converged Ewald sum over
+// the lattice period of both flows (1.29 L points at rc = 10); cuFFT is
+// markedly slower on sizes with a factor 7, hence 2^a 3^b 5^c.
+int bd_pme_default_grid(double L, double rc, int* K_out) {
+  if (!(L > 0) || !K_out) return BD_ERR_ARG;
+  double rc0 = rc > 0 ? rc : std::min(10.0, 0.43 * L);
+  double x = 12.9 * L / rc0;
+  if (!(x <= 4096.0)) return BD_ERR_ARG;
+  int K = std::max(1, (int)ceil(x - 1e-9));
+  for (;; K++) {
+    int r = K;
+    for (int f : {2, 3, 5})
+      while (r % f == 0) r /= f;
+    if (r == 1) break;
+  }
+  if (K > 4096) return BD_ERR_ARG;
+  *K_out = K;
+  return BD_OK;
+}
+
 const char* bd_status_string(int s) {
   switch (s) {
     case BD_OK: return "ok";
@@ -610,20 +631,15 @@ int bd_create(const bd_params* p, bd_ctx** out) {
   }
   // smooth-PME discretisation
   {
-    // default grid: spacing proportional to the cutoff (the split parameter is
-    // 4 / rc, so alpha h stays at most 0.31 and the error at most 3e-6 of the
-    // converged Ewald sum, 1.29 L points at rc = 10); the smallest 2^a 3^b 5^c
-    // at or above it
-    double rc0 = p->pme_rc > 0 ? p->pme_rc : std::min(10.0, 0.43 * p->L);
+    // default grid (bd_pme_default_grid): only the particle-mesh mobility
+    // and Ewald Coulomb use it
     int K = p->pme_grid;
-    if (K <= 0) {
-      K = (int)ceil(12.9 * p->L / rc0 - 1e-9);
-      for (;; K++) {
-        int r = K;
-        for (int f : {2, 3, 5})
-          while (r % f == 0) r /= f;
-        if (r == 1) break;
+    if (K <= 0 && bd_pme_default_grid(p->L, p->pme_rc, &K) != BD_OK) {
+      if (p->mobility == BD_MOB_PME || p->coulomb == BD_COULOMB_EWALD) {
+        bd_destroy(c);
+        return BD_ERR_ARG;
       }
+      K = 0;
     }
     c->pmeK = K;
     c->pme_p = p->pme_order > 0 ? p->pme_order : 8;

@@ -4,6 +4,8 @@ import ctypes
 import os
 import subprocess
 
+import numpy as np
+
 import pytest
 
 import bd_b200 as B
@@ -33,6 +35,23 @@ def test_library_exports_every_declared_symbol(libpath):
                          text=True, check=True).stdout
     exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
     assert set(B.exported_symbols()) <= exported
+
+
+def test_default_grid_rule_matches_python(libpath):
+    """bd_pme_default_grid (the grid bd_create picks) against the module's own
+    statement of the rule, over boxes 10..200 and cutoffs 4..25 and the
+    default cutoff; invalid boxes are rejected."""
+    lib = ctypes.CDLL(libpath)
+    lib.bd_pme_default_grid.argtypes = [ctypes.c_double, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_int)]
+    K = ctypes.c_int()
+    for L in np.linspace(10.0, 200.0, 39):
+        for rc in [0.0] + list(np.linspace(4.0, min(25.0, 0.43 * L), 9)):
+            assert lib.bd_pme_default_grid(L, rc, ctypes.byref(K)) == 0
+            assert K.value == B.pme_default_grid(L, rc if rc > 0 else None), (L, rc)
+    assert lib.bd_pme_default_grid(60.0, 12.1, ctypes.byref(K)) == 0 and K.value == 64
+    assert lib.bd_pme_default_grid(0.0, 10.0, ctypes.byref(K)) != 0
+    assert lib.bd_pme_default_grid(60.0, 1e-4, ctypes.byref(K)) != 0
 
 
 def test_status_strings(libpath):
