@@ -1067,6 +1067,7 @@ int bd_mobility_apply_block(bd_ctx* c, int k, const double* v, double* out) {
       for (int a = 0; a < 3; a++) soa[r * n + (size_t)a * NTp + i] = v[(size_t)r * 3 * N + 3 * i + a];
   double *X = nullptr, *Y = nullptr;
   if (cudaMalloc(&X, 8 * n * k) != cudaSuccess || cudaMalloc(&Y, 8 * n * k) != cudaSuccess) {
+    cudaGetLastError();  // not a sticky error: the next launch check must not see it
     cudaFree(X);
     return BD_ERR_OOM;
   }
