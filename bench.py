@@ -11,20 +11,25 @@ spring + excluded-volume + Coulomb forces, Brownian noise, mobility rebuild
 every srpy=100 steps, Brownian displacement, and a charge-hop sweep every
 MStep=100 steps.  The metric is bead-steps/s, whole-job (sum over GPUs).
 
-Default workload (c1): planar extension with Kraynik-Reinelt boundaries,
-80 chains x 100 beads (8000 beads), box 60a, Wi = 2, dt = 5e-4, FENE k=30
-Q0=3, WCA, 50% charged, charge hop every 100 steps.  Inputs are seeded
-synthetic chains.  The default path (pme32-learned) computes the
-Ewald-summed Rotne-Prager-Yamakawa mobility by smooth particle-mesh Ewald
-(FP32 grids, cutoff 12.1 with a 64^3 grid, the same interpolation accuracy as
-cutoff 10 with 80^3) and the Brownian displacement sqrt(M) z by a
-preconditioned Lanczos solve at tolerance 1e-6 (learned bead blocks on
-10-bead segment blocks), the displacements of 8 consecutive steps solved by
-one multi-vector Krylov run (noise blocks); --compare 1 also times the plain
-FP64 method (pme64: one solve per step, no preconditioner) on the same grid.
+Default workload (c3): planar extension with Kraynik-Reinelt boundaries,
+500 chains x 100 beads (50 000 beads), box 110a, Wi = 3, dt = 5e-4, FENE k=30
+Q0=3, WCA, 50% charged, charge hop every 100 steps (c1: 80 x 100 beads in a
+box of 60a at Wi = 2).  Inputs are seeded synthetic chains.  The default path
+(pme32-learned) computes the Ewald-summed Rotne-Prager-Yamakawa mobility by
+smooth particle-mesh Ewald (FP32 grids, cutoff 12.1 with the grid from the
+library's rule) and the Brownian displacement sqrt(M) z by a preconditioned
+Lanczos solve at tolerance 1e-6 (learned bead blocks on 10-bead segment
+blocks), the displacements of 8 consecutive steps solved by one multi-vector
+Krylov run (noise blocks).  --compare 1 also times the plain FP64 method
+(pme64, no preconditioner) on the same grid, with one solve per step and with
+the same noise blocks; --errors 1 reports the per-result error of the path
+against pme64 on the same configuration.  The rebuild (every 100 steps) and
+the sweep (every 100 steps) are timed on the device once each and carried at
+their frequency in every figure (breakdown.amortised).
 
 --impl reference times the reference's own CPU code (compiled from its sources
-into oracle/_ref/) on this host's cores for the same workload.
+into oracle/_ref/) on this host's cores; every part of its value is measured
+(a workload too large for its dense mobility is timed at 8000 beads).
 
 One process per GPU (torchrun for N > 1); the path does not shard, so each
 rank advances its own independent replica ("replicas only"); timing is the
@@ -142,24 +147,64 @@ def time_reference(w, steps, warmup, threads):
         return _time_reference(w, steps, warmup, threads)
 
 
+REF_MAX_BEADS = 8000  # largest system whose dense mobility (9 N^2 doubles, 4.6 GB) is timed
+
+
+def _ref_sweep_seconds(O, w, Nc, seed, edot, threads, kw):
+    """Wall time of one reference charge-hop sweep on a system with w's
+    density, chain length and charge fraction but Nc chains."""
+    ws = dict(w, Nc=Nc, L=w["L"] * (Nc / w["Nc"]) ** (1 / 3))
+    xs, ys, zs, qs, _, _ = synth_inputs(ws, seed)
+    refs = O.RefSim(w["flow"], ws["Nb"], ws["Nc"], ws["L"], edot, w["dt"], Ncharges=len(qs),
+                    threads=threads, **kw)
+    refs.set_pos(xs, ys, zs)
+    refs.set_charges(qs, len(qs))
+    refs.update_lattice(0)
+    refs.set_t(0)
+    if w["flow"] == 1:
+        refs.transform()
+    refs.apply_pbc()
+    t0 = refs.wtime()
+    refs.charge_hop()
+    return refs.wtime() - t0, ws["Nb"] * ws["Nc"]
+
+
 def _time_reference(w, steps, warmup, threads):
     """Per-step wall time of the reference's own routines (oracle/_ref) on the
-    workload: plain steps at full size, plus the amortised mobility rebuild
-    (timed once at full size) and charge-hop sweep.  The reference's sweep is
-    O(Ncharges N^2) (~10 min at 8000 beads), so it is timed on a system with
-    the same density, chain length and charge fraction but 1/8 of the beads
-    and scaled by N^3 (labelled in the sample string)."""
+    workload, every part measured:
+
+    * plain hydrodynamic steps (updateHI with the dense mobility, forces,
+      neighbour check) at full size;
+    * the dense mobility rebuild (calcHI) at full size, timed once and
+      amortised over its period of srpy steps;
+    * the charge-hop sweep, which is O(Ncharges N^2) (about 17 min at 8000
+      beads): timed at three smaller sizes of the same density, chain length
+      and charge fraction, and a power law fitted to them.  The extrapolated
+      sweep at full size is reported beside the measured value, not inside
+      it, so the measured value leaves the sweep out (in the reference's
+      favour).
+
+    Systems above REF_MAX_BEADS (the 50 000-bead workload: a dense mobility of
+    180 GB) cannot run; they are timed at the 8000-bead size of the same
+    density and chain length, whose per-bead cost is lower (the dense product
+    is O(N^2)), so the number is an upper bound on the reference's
+    throughput at the larger size."""
     import oracle as O
     if not O.ref_available(w["flow"]):
         return None
-    edot = edot_of(w)
-    N = w["Nb"] * w["Nc"]
-    x, y, z, q, beta, C = synth_inputs(w, 1234)
-    kw = force_params(w)
+    N_full = w["Nb"] * w["Nc"]
+    at = w
+    if N_full > REF_MAX_BEADS:
+        Nc = REF_MAX_BEADS // w["Nb"]
+        at = dict(w, Nc=Nc, L=w["L"] * (Nc / w["Nc"]) ** (1 / 3))
+    edot = edot_of(at)
+    N = at["Nb"] * at["Nc"]
+    x, y, z, q, beta, C = synth_inputs(at, 1234)
+    kw = force_params(at)
     kw.pop("srpy")
-    ref = O.RefSim(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
+    ref = O.RefSim(at["flow"], at["Nb"], at["Nc"], at["L"], edot, at["dt"], Ncharges=len(q),
                    threads=threads, **kw)
-    G = grid_table_host(w)
+    G = grid_table_host(at)
     for nt in range(COMMON["nt_avg"]):
         ref.set_grid(nt, np.ascontiguousarray(G[nt]))
     for sb in range(21):
@@ -178,34 +223,34 @@ def _time_reference(w, steps, warmup, threads):
     t0 = ref.wtime()
     ref.calc_hi()
     t_hi = ref.wtime() - t0
-    # charge-hop sweep on the 1/8 system (same density: box edge halved)
-    ws = dict(w, Nc=max(1, w["Nc"] // 8), L=w["L"] / 2)
-    xs, ys, zs, qs, _, _ = synth_inputs(ws, 99)
-    Ns = ws["Nb"] * ws["Nc"]
     del ref
-    refs = O.RefSim(w["flow"], ws["Nb"], ws["Nc"], ws["L"], edot, w["dt"], Ncharges=len(qs),
-                    threads=threads, **kw)
-    refs.set_pos(xs, ys, zs)
-    refs.set_charges(qs, len(qs))
-    refs.update_lattice(0)
-    refs.set_t(0)
-    if w["flow"] == 1:
-        refs.transform()
-    refs.apply_pbc()
-    t0 = refs.wtime()
-    refs.charge_hop()
-    t_sweep_s = refs.wtime() - t0
-    t_sweep = t_sweep_s * (N / Ns) ** 3
-    per_step = t_plain + t_hi / COMMON["srpy"] + t_sweep / COMMON["MStep"]
-    sample = (f"reference routines on {threads} host threads: {steps} full-size steps "
-              f"({t_plain*1e3:.1f} ms each) + mobility rebuild at full size "
-              f"({t_hi:.2f} s, amortised over {COMMON['srpy']} steps) + one charge-hop sweep "
-              f"timed at {Ns} beads ({t_sweep_s:.2f} s) scaled by (N/{Ns})^3 to "
-              f"{t_sweep:.0f} s, amortised over {COMMON['MStep']} steps")
+    # sweeps at 1/16, 1/8 and 1/4 of the chains; log-log least squares
+    sizes, times = [], []
+    for f in (16, 8, 4):
+        ts, ns = _ref_sweep_seconds(O, at, max(1, at["Nc"] // f), 99 + f, edot, threads, kw)
+        sizes.append(ns)
+        times.append(ts)
+    pw, lc = np.polyfit(np.log(sizes), np.log(times), 1)
+    t_sweep = float(np.exp(lc) * N ** pw)
+    per_step = t_plain + t_hi / COMMON["srpy"]
+    per_step_x = per_step + t_sweep / COMMON["MStep"]
+    where = (f"{N} beads" if at is w else
+             f"{N} beads (the {N_full}-bead system's dense mobility, 9 N^2 doubles = "
+             f"{9 * 8 * N_full ** 2 / 1e9:.0f} GB, cannot be allocated; same density and chain "
+             f"length, lower per-bead cost, so an upper bound on the reference's throughput "
+             f"there)")
+    sample = (f"reference routines on {threads} host threads at {where}: {steps} plain steps "
+              f"({t_plain*1e3:.1f} ms each) + dense mobility rebuild ({t_hi:.2f} s, amortised "
+              f"over {COMMON['srpy']} steps), all measured; the charge-hop sweep (not in the "
+              f"value) timed at {sizes} beads ({', '.join('%.2f' % v for v in times)} s), "
+              f"fitted t ~ N^{pw:.2f}, extrapolated to {t_sweep:.0f} s at {N} beads")
     return dict(per_step=per_step, value=N / per_step, sample=sample, threads=threads,
+                beads=N, value_with_extrapolated_sweep=N / per_step_x,
                 components={"plain_step_s": t_plain, "mobility_build_s": t_hi,
-                            "hop_sweep_s_scaled": t_sweep, "hop_sweep_s_sampled": t_sweep_s,
-                            "hop_sample_beads": Ns})
+                            "hop_sweep_sizes": sizes, "hop_sweep_s": times,
+                            "hop_sweep_exponent": float(pw),
+                            "hop_sweep_s_extrapolated": t_sweep,
+                            "measured_at_beads": N, "workload_beads": N_full})
 
 
 # ---------------------------------------------------------------------------
@@ -398,11 +443,6 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
     pre1 = c.precond_stats()
     blk1 = c.noise_block_stats()
     step_ms = prof["STEP"][0]
-    t_max = step_ms
-    if dist:
-        tt = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
     # end to end through the C ABI with pinned host buffers: upload the
     # positions, one step, download the positions, every step
     Ke = max(1, min(K, e2e_steps))
@@ -418,10 +458,47 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
         for a, b in zip(hb, c.positions()):
             a[:] = b
     e2e_s = time.perf_counter() - t0
+    # the periodic parts: a mobility rebuild every srpy steps and a charge-hop
+    # sweep every MStep steps.  A window shorter than their period holds none
+    # (or one, over-weighted), so one of each is timed on the device here, at
+    # the next step that has both, and every timed figure carries them at
+    # their own frequency (amortise below)
+    c.noise_block_release()
+    tp = (W + K + Ke + 99) // 100 * 100
+    c.set_time(tp, 0)
+    c.update_lattice(tp)
+    c.profile(True)
+    ext = w["flow"] == 1
+    if ext:
+        c.transform_coords()
+    c.apply_pbc()
+    c.calc_hi()
+    if c.p.Ncharges > 0:
+        c.charge_hop()
+    if ext:
+        c.inverse_coords()
+    c.sync()
+    per = {k: c.profile_read(getattr(c, "PROF_" + k)) for k in ("HI_BUILD", "HOP")}
+    c.profile(False)
+    t_build = per["HI_BUILD"][0] / max(per["HI_BUILD"][1], 1)
+    t_sweep = per["HOP"][0] / max(per["HOP"][1], 1)
+    srpy, mstep = COMMON["srpy"], COMMON["MStep"]
+
+    def amortise(ms, t_first, n):
+        # remove the rebuilds and sweeps that fell in steps [t_first, t_first + n)
+        # and add n / period of each, at the times measured above
+        nb = sum(1 for t in range(t_first, t_first + n) if t % srpy == 0)
+        ns = sum(1 for t in range(t_first, t_first + n) if t % mstep == 0)
+        return ms - nb * t_build - ns * t_sweep + n * (t_build / srpy + t_sweep / mstep)
+
+    step_ms_raw = step_ms
+    step_ms = amortise(step_ms, W, K)
+    e2e_s = amortise(e2e_s * 1e3, W + K, Ke) / 1e3
+    t_max = step_ms
     if dist:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        tt = torch.tensor([step_ms, e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+        t_max, e2e_s = float(tt[0].item()), float(tt[1].item())
     mv_ms, mv_n = prof["MATVEC"]
     if pp["mobility"] == "pme":
         # compulsory bytes of one particle-mesh product, s bytes per value:
@@ -458,10 +535,14 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
                lanczos_maxed=lan1["maxed"] - lan0["maxed"],
                precond_fallbacks=pre1["fallbacks"] - pre0["fallbacks"],
                precond_calls=pre1["calls"] - pre0["calls"],
-               breakdown={"mobility_build_ms": prof["HI_BUILD"][0], "mobility_builds": prof["HI_BUILD"][1],
-                          "hop_sweep_ms": prof["HOP"][0], "hop_sweeps": prof["HOP"][1],
-                          "forces_ms": prof["FORCES"][0], "matvec_ms": mv_ms,
-                          "step_total_ms": step_ms})
+               breakdown={"window_ms": step_ms_raw,
+                          "window_mobility_builds": prof["HI_BUILD"][1],
+                          "window_hop_sweeps": prof["HOP"][1],
+                          "mobility_build_ms_each": t_build, "hop_sweep_ms_each": t_sweep,
+                          "amortised": "window - its rebuilds and sweeps + K/%d rebuilds + "
+                                       "K/%d sweeps at the times measured" % (srpy, mstep),
+                          "steps_ms_amortised": step_ms,
+                          "forces_ms": prof["FORCES"][0], "matvec_ms": mv_ms})
     c.close()
     return out
 
@@ -573,6 +654,50 @@ def run_batch(args, world):
     return line
 
 
+def accuracy_vs_fp64(w, path, noise_block, pme_rc, pme_grid, seed=1000):
+    """Per-result relative error (2-norm over all beads) of the measured path
+    against the plain FP64 path (pme64: FP64 grids, transforms and pair
+    tensors, no preconditioner) on the same configuration at the bench's
+    discretisation: the forces, the mobility product M F, and the Brownian
+    displacement sqrt(M) z for one seeded z (each solve at tolerance 1e-6).
+    The FP64 path is itself checked against the CPU oracle's dense Ewald sum
+    at sizes the oracle can hold (the particle-mesh tests)."""
+    N = w["Nb"] * w["Nc"]
+    z = np.random.default_rng(seed).normal(size=3 * N)
+    res = {}
+    for name in (path, "pme64"):
+        c = build_context(w, seed, name, noise_block=noise_block if name == path else 1,
+                          pme_rc=pme_rc, pme_grid=pme_grid)
+        ext = w["flow"] == 1
+        # the step's order: forces and the mobility build in the flow frame,
+        # the products after rotating back
+        c.reset_force()
+        if ext:
+            c.transform_coords()
+        c.apply_pbc()
+        c.build_neighbors()
+        c.bond_force()
+        c.ev_force()
+        c.coulomb_force()
+        F = c.forces()
+        c.calc_hi()
+        if ext:
+            c.inverse_coords()
+        f = np.ascontiguousarray(F.T).reshape(-1)
+        mf = c.mobility_apply(f)
+        y, it = c.lanczos_sqrt(z)
+        res[name] = (F, mf, y, it)
+        c.close()
+    a, b = res[path], res["pme64"]
+    rel = lambda u, v: float(np.linalg.norm(u - v) / np.linalg.norm(v))
+    return {"against": "pme64 on the same configuration (FP64 storage, plain Lanczos)",
+            "forces": rel(a[0], b[0]), "mobility_product": rel(a[1], b[1]),
+            "displacement": rel(a[2], b[2]),
+            "krylov_iterations": {path: a[3], "pme64": b[3]}, "gate": 1e-5,
+            "note": "forces are FP64 in every path (springs, excluded volume, Ewald Coulomb); "
+                    "the displacement holds both solves' tolerance and the FP32 storage error"}
+
+
 def run_ours(args, rank, world, dist):
     w = WORKLOADS[args.workload]
     N = w["Nb"] * w["Nc"]
@@ -643,13 +768,32 @@ def run_ours(args, rank, world, dist):
             "gpu_launches": main["launches"], "breakdown": main["breakdown"]}
     plain = "pme64" if pme else "lanczos64"
     if args.compare and args.path != plain:
-        # the plain method: same mobility in FP64, no preconditioner
+        # the plain method: the same mobility in FP64 storage, no
+        # preconditioner, one Krylov solve per step
         ref64 = measure(w, plain, K, W, rank, dist, 1, 1, args.pme_rc, args.pme_grid)
-        line["plain_fp64"] = {"path": plain, "value": world * N * K / (ref64["t_max_ms"] / 1e3),
+        line["plain_fp64"] = {"path": plain, "noise_block": 1,
+                              "value": world * N * K / (ref64["t_max_ms"] / 1e3),
                               "ms_per_step": ref64["t_max_ms"] / K,
                               "lanczos_iters_per_step": ref64["lanczos_iters_per_step"],
                               "matvec_gbs": ref64["achieved_gbs"]}
         line["speedup_vs_plain_fp64"] = line["value"] / line["plain_fp64"]["value"]
+        if pme and args.noise_block > 1:
+            # the plain method with the same noise blocks: isolates what FP32
+            # storage and the preconditioner gain
+            refb = measure(w, plain, K, W, rank, dist, 1, args.noise_block, args.pme_rc,
+                           args.pme_grid)
+            line["plain_fp64_noise_blocks"] = {
+                "path": plain, "noise_block": args.noise_block,
+                "value": world * N * K / (refb["t_max_ms"] / 1e3),
+                "ms_per_step": refb["t_max_ms"] / K,
+                "block_iterations_per_step": (refb["block"] or {}).get(
+                    "block_iterations_per_step"),
+                "lanczos_iters_per_step": refb["lanczos_iters_per_step"]}
+            line["speedup_vs_plain_fp64_noise_blocks"] = (
+                line["value"] / line["plain_fp64_noise_blocks"]["value"])
+    if pme and args.errors and args.path != "pme64":
+        line["errors"] = accuracy_vs_fp64(w, args.path, args.noise_block, args.pme_rc,
+                                          args.pme_grid)
     return line
 
 
@@ -659,7 +803,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--path", choices=sorted(PATHS), default="pme32-learned")
@@ -675,7 +819,11 @@ def main():
     ap.add_argument("--segment", type=int, default=10,
                     help="beads per segment block of the preconditioned paths")
     ap.add_argument("--compare", type=int, default=1,
-                    help="also time the plain FP64 Krylov path (reported as plain_fp64)")
+                    help="also time the plain FP64 Krylov path, one solve per step "
+                         "(plain_fp64) and with the same noise blocks "
+                         "(plain_fp64_noise_blocks)")
+    ap.add_argument("--errors", type=int, default=1,
+                    help="per-result error of the path against pme64 at the bench config")
     args = ap.parse_args()
     SEGMENT[0] = args.segment
     args.warmup = max(args.warmup, 3)
@@ -698,9 +846,11 @@ def main():
                 "warmup": args.warmup, "ms_per_step": r["per_step"] * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": {"workload": w["name"], "beads": N},
+                "config": {"workload": w["name"], "beads": N,
+                           "measured_at_beads": r["beads"]},
                 "cpu_baseline": {"value": r["value"], "unit": "bead-steps/s", "cores": th,
                                  "kind": "reference", "sample": r["sample"]},
+                "value_with_extrapolated_sweep": r["value_with_extrapolated_sweep"],
                 "components": r["components"],
                 "e2e": {"value": r["value"], "unit": "bead-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
@@ -725,7 +875,9 @@ def main():
             if r is not None:
                 line["cpu_baseline"] = {"value": r["value"], "unit": "bead-steps/s",
                                         "cores": r["threads"], "kind": "reference",
-                                        "sample": r["sample"]}
+                                        "sample": r["sample"], "beads": r["beads"],
+                                        "value_with_extrapolated_sweep":
+                                            r["value_with_extrapolated_sweep"]}
         if rank == 0:
             print(json.dumps(line))
     finally:

@@ -233,10 +233,25 @@ int bd_calc_hi(bd_ctx *ctx);                           /* [calcHI] main26.c:1530
 int bd_download_mobility(bd_ctx *ctx, double *M9);
 int bd_update_hi(bd_ctx *ctx);                         /* [updateHI] main26.c:745 */
 int bd_update_fd(bd_ctx *ctx);                         /* [updateFD] main26.c:731 */
-int bd_charge_hop(bd_ctx *ctx);                        /* [chargeHop] main26.c:1926 */
+/* [chargeHop] main26.c:1926.  With hop = BD_HOP_PARALLEL the sweep runs on
+ * independent sets: cells at least hop_radius wide in eight parity colours,
+ * each cell's charges in index order, a trial seeing the charges of other
+ * cells at their sites at the colour's start.  Its acceptance test uses the
+ * energy the forces use: the Debye-Hueckel pair energy with
+ * coulomb = BD_COULOMB_DH, the Ewald-summed unscreened energy in FP64 with
+ * BD_COULOMB_EWALD (real-space pairs, the mesh reciprocal potential of the
+ * colour's start, the moved charge's own reciprocal term and those of the
+ * cell's earlier moves).  The coupling of simultaneous moves in different
+ * cells is left out: at most 2 lambda_B d^2 / R^3 per pair (hop distance
+ * d <= 2.1, cells R apart). */
+int bd_charge_hop(bd_ctx *ctx);
 /* Per-charge outcome of the last sweep: (0 skipped,1 accepted,2 rejected),
  * target bead, move kind; 3 ints per charge. */
 int bd_download_hop_log(bd_ctx *ctx, int *log3);
+/* Energy change (kT) each charge's trial of the last parallel sweep saw, in
+ * track order (NaN where the move was blocked).  No reference counterpart:
+ * the parallel sweep's check against its CPU model. */
+int bd_download_hop_energies(bd_ctx *ctx, double *dE);
 
 /* ---- measurement -----------------------------------------------------
  * Device time of selected kernels, measured with CUDA events recorded on
@@ -296,7 +311,10 @@ int bd_noise_block_release(bd_ctx *ctx);
  * N may not exceed BD_NOALLOC_MAX_BEADS (else BD_ERR_CAPACITY).  All calls on
  * a device share that array: calls that overlap on the GPU race.  The first
  * call on a device looks up the array's device address; make it before any
- * stream capture.  The context's device must be current. */
+ * stream capture.  The context's device must be current.  Dense-tile
+ * mobilities only (BD_MOB_EWALD, BD_MOB_HYBRID): a particle-mesh context gets
+ * BD_ERR_STATE.  The address is kept for the process's life: calls after a
+ * cudaDeviceReset are not supported. */
 #define BD_NOALLOC_MAX_BEADS 4096
 int bd_mobility_apply_noalloc(bd_ctx *ctx, const double *v, double *out);
 
@@ -400,6 +418,16 @@ int bd_autotune_pme_grid(double L, int precision, int *K_out);
  * 0.43 L): the smallest 2^a 3^b 5^c >= 12.9 L / rc.  Host arithmetic only
  * (no device needed); BD_ERR_ARG for L <= 0 or a grid above 4096. */
 int bd_pme_default_grid(double L, double rc, int *K_out);
+
+/* Raw Philox4x32-10 (Salmon et al., SC'11) on the device: block k of out
+ * (4 words) is the generator applied to counter ctr[4k..4k+3] under key
+ * key[2k..2k+1], for 1 <= n <= 2^20 blocks.  No reference counterpart (the
+ * reference's generator is ran1); this is the function behind the
+ * library's Philox noise and charge-hop draws, exposed so that it can be
+ * checked against the published Random123 known-answer vectors.  Uses the
+ * current device and the default stream; allocates and frees a small device
+ * buffer. */
+int bd_philox4x32_10(const unsigned *ctr, const unsigned *key, unsigned *out, int n);
 
 /* ---- learned preconditioner network (no reference counterpart) ----------
  * Per bead, the BD_MPNN_NEIGHBORS nearest beads within BD_MPNN_CUTOFF

@@ -23,7 +23,12 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 
-def build(ref_root: str | None = "/root/reference") -> None:
+# where the reference sources lie (only the recipe that compiles them reads
+# this); override with the REF_ROOT environment variable
+REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+
+
+def build(ref_root: str | None = REF_ROOT) -> None:
     """Compile liboracle.so and, when the reference sources exist, _ref/."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref_root and os.path.isdir(ref_root):

@@ -133,6 +133,7 @@ def _lib() -> C.CDLL:
         L.bd_download_neighbors.argtypes = [vp, _ip, _ip, C.c_int]
         L.bd_download_mobility.argtypes = [vp, _dp]
         L.bd_download_hop_log.argtypes = [vp, _ip]
+        L.bd_download_hop_energies.argtypes = [vp, _dp]
         L.bd_step_reference.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
         L.bd_mobility_apply.argtypes = [vp, _dp, _dp]
         L.bd_mobility_apply_block.argtypes = [vp, C.c_int, _dp, _dp]
@@ -495,6 +496,14 @@ class Context:
         o = np.zeros(3 * max(n, 1), np.int32)
         self._call("bd_download_hop_log", o)
         return o.reshape(-1, 3)[:n]
+
+    def hop_energies(self):
+        """Energy change each charge's trial of the last parallel sweep saw
+        (NaN where the move was blocked)."""
+        n = getattr(self, "nch", 0)
+        o = np.zeros(max(n, 1))
+        self._call("bd_download_hop_energies", o)
+        return o[:n]
 
     def mobility_apply(self, v):
         out = np.zeros(3 * self.N)

@@ -542,6 +542,41 @@ const char* bd_last_error_detail(void) { return g_detail; }
 // alpha h stays at most 0.31, within 3.3e-6 of the converged Ewald sum over
 // the lattice period of both flows (1.29 L points at rc = 10); cuFFT is
 // markedly slower on sizes with a factor 7, hence 2^a 3^b 5^c.
+// The raw generator behind every Philox draw of the library: block k is
+// Philox4x32-10 of counter ctr[4k..4k+3] under key key[2k..2k+1].
+__global__ void k_philox_raw(const uint32_t* __restrict__ ctr, const uint32_t* __restrict__ key,
+                             uint32_t* __restrict__ out, int n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint4 x = philox4x32_10(make_uint4(ctr[4 * k], ctr[4 * k + 1], ctr[4 * k + 2], ctr[4 * k + 3]),
+                          make_uint2(key[2 * k], key[2 * k + 1]));
+  out[4 * k] = x.x;
+  out[4 * k + 1] = x.y;
+  out[4 * k + 2] = x.z;
+  out[4 * k + 3] = x.w;
+}
+
+int bd_philox4x32_10(const unsigned* ctr, const unsigned* key, unsigned* out, int n) {
+  if (!ctr || !key || !out || n < 1 || n > (1 << 20)) return BD_ERR_ARG;
+  uint32_t* d = nullptr;
+  size_t bytes = 4 * (size_t)n * 10;
+  cudaError_t e = cudaMalloc(&d, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return BD_ERR_OOM;
+  }
+  e = cudaMemcpy(d, ctr, 16 * (size_t)n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + 4 * (size_t)n, key, 8 * (size_t)n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_philox_raw<<<(n + 255) / 256, 256>>>(d, d + 4 * (size_t)n, d + 6 * (size_t)n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + 6 * (size_t)n, 16 * (size_t)n, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return bd::cuda_fail((int)e, cudaGetErrorString(e), __FILE__, __LINE__);
+  return BD_OK;
+}
+
 int bd_pme_default_grid(double L, double rc, int* K_out) {
   if (!(L > 0) || !K_out) return BD_ERR_ARG;
   double rc0 = rc > 0 ? rc : std::min(10.0, 0.43 * L);
@@ -778,6 +813,7 @@ int bd_destroy(bd_ctx* c) {
   pme_free(c);
   coulomb_free(c);
   if (c->hop_cells) cudaFree(c->hop_cells);
+  if (c->hop_de) cudaFree(c->hop_de);
   if (c->cb_part) cudaFree(c->cb_part);
   if (c->cb_tileI) cudaFree(c->cb_tileI);
   precond_free(c);

@@ -144,6 +144,63 @@ __global__ void __launch_bounds__(256) k_cw_influence(Cell cell, int K, double b
   if (threadIdx.x == 0) epart[blockIdx.x] = red[0];
 }
 
+// Per-block partial sums of sum_{k != 0} A_k k_a k_b over the mesh spectrum,
+// A_k = (2 pi lambda_B / V k^2) exp(-k^2/4 beta^2) (the reciprocal energy is
+// sum_k A_k |S(k)|^2 over all k), six components (xx xy xz yy yz zz).
+__global__ void __launch_bounds__(256) k_cw_quad(Cell cell, int K, double beta, double lambda_b,
+                                                 double* part) {
+  int Kh = K / 2 + 1;
+  size_t n = (size_t)K * K * Kh;
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (e < n) {
+    int m2 = (int)(e % Kh), m1 = (int)((e / Kh) % K), m0 = (int)(e / ((size_t)Kh * K));
+    if (m0 || m1 || m2) {
+      int s0 = m0 < (K + 1) / 2 ? m0 : m0 - K, s1 = m1 < (K + 1) / 2 ? m1 : m1 - K, s2 = m2;
+      double kv[3];
+      for (int a = 0; a < 3; a++)
+        kv[a] = 2.0 * M_PI *
+                (s0 * cell.Hi[0 * 3 + a] + s1 * cell.Hi[1 * 3 + a] + s2 * cell.Hi[2 * 3 + a]);
+      double kk = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+      double mult = (m2 == 0 || (K % 2 == 0 && m2 == K / 2)) ? 1.0 : 2.0;
+      double A = mult * 2.0 * M_PI * lambda_b / (cell.V * kk) * exp(-kk / (4.0 * beta * beta));
+      acc[0] = A * kv[0] * kv[0];
+      acc[1] = A * kv[0] * kv[1];
+      acc[2] = A * kv[0] * kv[2];
+      acc[3] = A * kv[1] * kv[1];
+      acc[4] = A * kv[1] * kv[2];
+      acc[5] = A * kv[2] * kv[2];
+    }
+  }
+  __shared__ double red[8][6];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int c = 0; c < 6; c++) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double v = 0;
+    for (int q = 0; q < 8; q++) v += red[q][threadIdx.x];
+    part[(size_t)blockIdx.x * 6 + threadIdx.x] = v;
+  }
+}
+
+// Q = -sum_k A_k k k^T + lambda_B (2 beta^3 / (3 sqrt(pi))) I from the block
+// partials (one warp per component, fixed order).
+__global__ void k_cw_quad_fin(const double* __restrict__ part, int nblk, double beta,
+                              double lambda_b, double* Q) {
+  int c = blockIdx.x;
+  double v = 0;
+  for (int b = threadIdx.x; b < nblk; b += 32) v += part[(size_t)b * 6 + c];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) {
+    bool diag = c == 0 || c == 3 || c == 5;
+    Q[c] = -v + (diag ? lambda_b * 2.0 * beta * beta * beta / (3.0 * sqrt(M_PI)) : 0.0);
+  }
+}
+
 // Cell list of the charged beads (fractional cells of the reduced cell).
 __global__ void k_cc_count(Cell cell, CGeom g, const double4* __restrict__ cq, int nch,
                            double cr, double sr, int* cell_of, int* count) {
@@ -346,7 +403,7 @@ static int coul_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->cw_spec, 16 * Ks));
   CU(cudaMalloc(&c->cw_bsq, 24 * (size_t)K));
   c->cw_nblk = (int)((Ks + 255) / 256);
-  CU(cudaMalloc(&c->cw_epart, 8 * (size_t)std::max(c->cw_nblk, n)));
+  CU(cudaMalloc(&c->cw_epart, 8 * (size_t)std::max(6 * c->cw_nblk, n)));
   CU(cudaMalloc(&c->cw_energy, 8 * 4));
   CU(cudaMalloc(&c->cw_base, 12 * (size_t)n));
   CU(cudaMalloc(&c->cw_w, 2 * 8 * 3 * (size_t)n * kMaxOrder));
@@ -357,7 +414,7 @@ static int coul_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->cw_cursor, 4 * (size_t)kCellCap));
   CU(cudaMemsetAsync(c->cw_count, 0, 4 * (size_t)kCellCap, c->stream));
   CU(cudaMemsetAsync(c->cw_energy, 0, 32, c->stream));
-  c->bytes += 8 * K3 + 16 * Ks + 24 * (size_t)K + 8 * (size_t)std::max(c->cw_nblk, n) + 32 +
+  c->bytes += 8 * K3 + 16 * Ks + 24 * (size_t)K + 8 * (size_t)std::max(6 * c->cw_nblk, n) + 32 +
               (size_t)n * (12 + 48 * kMaxOrder + 8) + 12 * (size_t)kCellCap;
   int dims[3] = {K, K, K};
   cufftHandle f, b;
@@ -383,6 +440,60 @@ void coulomb_free(bd_ctx* c) {
                   c->cw_w, c->cw_cell_of, c->cw_idx, c->cw_count, c->cw_start, c->cw_cursor};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+}
+
+// Reciprocal-space potential of the charges gathered in cq on the mesh:
+// c->cw_grid = phi with Phi(r) = sum_g W(r - g) phi(g) the smooth-PME
+// reciprocal potential (kT per unit charge, lambda_B included) at any point r
+// (the same weights, spread, transform and influence as coulomb_ewald; the
+// energies it keeps are not touched).  Used by the charge-hop sweep's Ewald
+// energy differences.
+int coulomb_mesh_potential(bd_ctx* c, const Lat& l, const double4* cq) {
+  int s;
+  if ((s = coul_alloc(c)) != BD_OK) return s;
+  int K = c->pmeK, p = c->pme_p, nch = c->nch;
+  Cell cell = make_cell(l);
+  double cr = 1.0, sr = 0.0;
+  if (l.flow == BD_FLOW_EXT) {
+    cr = l.cth;
+    sr = l.sth;
+  }
+  size_t K3 = (size_t)K * K * K;
+  double* w = c->cw_w;
+  double* dw = c->cw_w + 3 * (size_t)nch * kMaxOrder;
+  c->launches += 5;
+#define CW_WEIGHTS(P_)                                                                      \
+  k_cw_weights<P_><<<nblk(3 * (long long)nch, 128), 128, 0, c->stream>>>(cell, cq, nch, cr, sr, K, \
+                                                                        c->cw_base, w, dw, c->err)
+  switch (p) {
+    case 4: CW_WEIGHTS(4); break;
+    case 6: CW_WEIGHTS(6); break;
+    default: CW_WEIGHTS(8);
+  }
+#undef CW_WEIGHTS
+  CU(cudaMemsetAsync(c->cw_grid, 0, 8 * K3, c->stream));
+  k_cw_spread<<<nblk(nch, 8), 256, 0, c->stream>>>(cq, c->cw_base, w, nch, K, p, c->cw_grid);
+  CF(cufftExecD2Z((cufftHandle)c->cw_plan_f, c->cw_grid, (cufftDoubleComplex*)c->cw_spec));
+  k_cw_influence<<<c->cw_nblk, 256, 0, c->stream>>>(cell, K, c->cw_beta, c->p.lambda_b,
+                                                    c->cw_bsq, (cufftDoubleComplex*)c->cw_spec,
+                                                    c->cw_epart);
+  CF(cufftExecZ2D((cufftHandle)c->cw_plan_b, (cufftDoubleComplex*)c->cw_spec, c->cw_grid));
+  return launch_ok(c);
+}
+
+// Quadratic form of the periodic remainder of the reciprocal pair term near
+// the origin: G(r) = lambda_B erf(beta r)/r + r^T Q r + const + O(r^4), into
+// Q6 (device, xx xy xz yy yz zz), for the lattice l.  For a cubic lattice
+// Q = (2 pi lambda_B / 3 V) I.
+int coulomb_quadform(bd_ctx* c, const Lat& l, double* Q6) {
+  int s;
+  if ((s = coul_alloc(c)) != BD_OK) return s;
+  Cell cell = make_cell(l);
+  c->launches += 2;
+  k_cw_quad<<<c->cw_nblk, 256, 0, c->stream>>>(cell, c->pmeK, c->cw_beta, c->p.lambda_b,
+                                              c->cw_epart);
+  k_cw_quad_fin<<<6, 32, 0, c->stream>>>(c->cw_epart, c->cw_nblk, c->cw_beta, c->p.lambda_b, Q6);
+  return launch_ok(c);
 }
 
 // Ewald Coulomb forces for the charges gathered in cq (positions in the frame

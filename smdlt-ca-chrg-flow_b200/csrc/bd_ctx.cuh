@@ -141,6 +141,7 @@ struct bd_ctx {
   // parallel charge-hop sweep
   double hop_R;
   int *hop_cells;
+  double *hop_de;  // energy change of each charge's last parallel-sweep trial
   unsigned long long hop_sweeps;
 
   // Ewald Coulomb (bd_coulomb.cu)
@@ -244,6 +245,8 @@ int ewald_bin(bd_ctx* c, double* eps, std::vector<double>& rowsum);
 
 // Ewald Coulomb
 int coulomb_ewald(bd_ctx* c, const Lat& l, const double4* cq);
+int coulomb_mesh_potential(bd_ctx* c, const Lat& l, const double4* cq);
+int coulomb_quadform(bd_ctx* c, const Lat& l, double* Q6);
 void coulomb_free(bd_ctx* c);
 
 // block preconditioner

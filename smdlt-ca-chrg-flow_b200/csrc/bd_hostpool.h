@@ -41,6 +41,12 @@ class HostPool {
       return;
     }
     auto job = std::make_shared<Job>();
+    // f is held by reference and lives on this frame.  That is safe only
+    // because of the order in work(): a thread calls f only for an index it
+    // claimed below n, and counts the call down after it returns; run returns
+    // once every claimed call has been counted, so no call of f can start or
+    // still run after that.  Keep claim -> call -> count down in that order
+    // (never count down first, never retry an index).
     job->f = std::function<void(int)>(std::ref(f));
     job->n = n;
     job->left.store(n);

@@ -7,9 +7,12 @@
 // Lanczos on M from v_1 = z/|z| with full reorthogonalisation in FP64 (the
 // three-term recurrence, then one classical Gram-Schmidt pass against the
 // whole basis), T_m = V_m^T M V_m tridiagonal,
-// sqrt(M) z ~= |z| V_m T_m^(1/2) e_1, stopped when the relative change of the
-// iterate between successive m is below the tolerance (the criterion of Ando,
-// Chow and Skolnick, J. Chem. Phys. 137, 064106 (2012)).  T_m^(1/2) e_1 comes
+// sqrt(M) z ~= |z| V_m T_m^(1/2) e_1.  The relative change d_m of the iterate
+// between successive m (the quantity of Ando, Chow and Skolnick, J. Chem.
+// Phys. 137, 064106 (2012)) decays geometrically; the solve stops when the
+// tail it implies, d_m rho / (1 - rho) with rho the largest of the last three
+// ratios d_j / d_(j-1), is below the tolerance, an estimate of the error of
+// the iterate itself rather than of its last change.  T_m^(1/2) e_1 comes
 // from an eigen-decomposition of T_m on the host by the implicit symmetric QR
 // iteration with Wilkinson shifts (Golub and Van Loan, Matrix Computations,
 // section 8.3).  Vectors live on the device in component-major SoA with the
@@ -442,6 +445,36 @@ static int sqrt_e1(const std::vector<double>& alpha, const std::vector<double>& 
   return neg;
 }
 
+
+// Relative change d_m = |c_m - (c_(m-1), 0)| / |c_m| of the tridiagonal
+// coefficients between Krylov dimensions m - 1 and m (the basis is
+// orthonormal, so this is the relative change of the iterate itself).
+static double rel_change(const std::vector<double>& cm, const std::vector<double>& cprev) {
+  double dn = 0, cn = 0;
+  for (size_t i = 0; i < cm.size(); i++) {
+    double prev = i < cprev.size() ? cprev[i] : 0.0;
+    dn += (cm[i] - prev) * (cm[i] - prev);
+    cn += cm[i] * cm[i];
+  }
+  return cn > 0 ? sqrt(dn / cn) : 0.0;
+}
+
+// Stopping test at dimension m from the changes dh[m-3 .. m] (negative where
+// unknown): with the changes decaying at rate rho the error left in the
+// iterate is the geometric tail d_m rho / (1 - rho).  rho is the largest of
+// the last three ratios d_j / d_(j-1), capped at 0.99, so one fast step does
+// not end the solve; the cap makes d_m <= tol / 99 sufficient on its own.
+static bool tail_converged(const std::vector<double>& dh, int m, double tol) {
+  if (m < 4 || (int)dh.size() <= m) return false;
+  double rho = 0;
+  for (int j = m - 2; j <= m; j++) {
+    if (dh[j] < 0 || dh[j - 1] < 0) return false;
+    rho = std::max(rho, dh[j - 1] > 0 ? dh[j] / dh[j - 1] : 0.0);
+  }
+  rho = std::min(rho, 0.99);
+  return dh[m] * rho / (1.0 - rho) <= tol;
+}
+
 namespace bd {
 
 int alloc_lanczos(bd_ctx* c) {
@@ -573,16 +606,31 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
   CU(cudaMemsetAsync(c->Ljd, 0, sizeof(int), st));
   double zn = 0;
   CU(cudaMemcpyAsync(&zn, c->Lsc, 8, cudaMemcpyDeviceToHost, st));
-  std::vector<double> alpha, beta, cc, cprev;
+  std::vector<double> alpha, beta, cc;
   int m = 0, neg = 0;
   bool conv = false;
   // alpha_j, beta_j stay on the device (Lh, Lsc + 8); the host reads them
   // only at checkpoints: from two before the previous call's Krylov
-  // dimension on, every second iteration
+  // dimension on, every second iteration.  Each check needs the changes at
+  // the last four dimensions: the coefficients of the dimensions it lacks
+  // are solved for (cs: the last few, by dimension), the previous check's
+  // reused.
   double* d_alpha = c->Lh;
   double* d_beta = c->Lsc + 8;
   int& last = pre ? c->pre_last : c->lan_last;
-  int next_check = std::max(4, last - 2);
+  int next_check = std::max(5, last - 2);
+  std::vector<double> dh;
+  std::vector<std::vector<double>> cs;
+  std::vector<int> cs_m;
+  auto coeffs = [&](int mm) -> std::vector<double> {
+    for (size_t i = 0; i < cs_m.size(); i++)
+      if (cs_m[i] == mm) return cs[i];
+    cs.emplace_back();
+    cs_m.push_back(mm);
+    int ng = sqrt_e1(alpha, beta, mm, cs.back(), q);
+    if (mm == m) neg = ng;
+    return cs.back();
+  };
   for (int j = 0; j < c->lmax; j++) {
     if (j == 0 && with_force)
       s = lanczos_iteration(c, pre, true);
@@ -598,15 +646,19 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
     CU(cudaMemcpyAsync(alpha.data(), d_alpha, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
     CU(cudaMemcpyAsync(beta.data(), d_beta, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    neg = sqrt_e1(alpha, beta, m, cc, q);
-    sqrt_e1(alpha, beta, m - 1, cprev, q);
-    double dn = 0, cn = 0;
-    for (int i = 0; i < m; i++) {
-      double prev = i < m - 1 ? cprev[i] : 0.0;
-      dn += (cc[i] - prev) * (cc[i] - prev);
-      cn += cc[i] * cc[i];
-    }
-    if (sqrt(dn) <= c->ltol * sqrt(cn) || beta[m - 1] <= 1e-300) {
+    // keep only the coefficients that later checks can reuse
+    for (size_t i = 0; i < cs_m.size();)
+      if (cs_m[i] < m - 4) {
+        cs.erase(cs.begin() + i);
+        cs_m.erase(cs_m.begin() + i);
+      } else {
+        i++;
+      }
+    dh.resize(m + 1, -1.0);
+    for (int mm = std::max(2, m - 3); mm <= m; mm++)
+      if (dh[mm] < 0) dh[mm] = rel_change(coeffs(mm), coeffs(mm - 1));
+    cc = coeffs(m);
+    if (tail_converged(dh, m, c->ltol) || beta[m - 1] <= 1e-300) {
       conv = true;
       break;
     }
@@ -841,14 +893,16 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
   mr.assign(k, 0);
   conv.assign(k, 0);
   int ndone = 0, pending = 0, m = 0;
-  int next_check = std::max(4, c->blk_last - 2);
+  int next_check = std::max(5, c->blk_last - 2);
   const double* ha = c->Bhost;
   const double* hb = c->Bhost + (size_t)L1 * k;
   // convergence of every open right-hand side at Krylov dimension mm, from the
-  // alpha and beta copied after iteration mm
-  // the square root at the previous check, reused as the m - 1 iterate when
-  // the checks are consecutive
-  std::vector<std::vector<double>> clast(k);
+  // alpha and beta copied after iteration mm.  Per right-hand side: the
+  // changes at every checked dimension (dh), and the coefficients of the
+  // previous check (clast at dimension mlast), reused as the m - 1 iterate
+  // when the checks are consecutive (every iteration after the first check,
+  // which solves the three dimensions below it as well)
+  std::vector<std::vector<double>> clast(k), dh(k);
   std::vector<int> mlast(k, -1);
   auto evaluate = [&](int mm) -> int {
     CU(cudaEventSynchronize(ev));
@@ -857,24 +911,30 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
       if (!done[r]) open.push_back(r);
     parallel_for((int)open.size(), [&](int q) {
       int r = open[q];
-      std::vector<double> alpha(mm), beta(mm), cprev;
+      std::vector<double> alpha(mm), beta(mm);
       for (int i = 0; i < mm; i++) {
         alpha[i] = ha[(size_t)i * k + r];
         beta[i] = hb[(size_t)i * k + r];
       }
-      std::vector<double> cm;
+      std::vector<double>& d = dh[r];
+      d.resize(mm + 1, -1.0);
+      std::vector<double> cm, cprev;
       int neg = sqrt_e1(alpha, beta, mm, cm, 0.5);
-      if (mlast[r] == mm - 1)
+      if (mlast[r] == mm - 1) {
         cprev.swap(clast[r]);
-      else
+      } else {
+        // first check: the changes at mm - 1 .. mm - 3 as well
+        std::vector<double> ca, cb;
         sqrt_e1(alpha, beta, mm - 1, cprev, 0.5);
-      double dn = 0, cn = 0;
-      for (int i = 0; i < mm; i++) {
-        double prev = i < mm - 1 ? cprev[i] : 0.0;
-        dn += (cm[i] - prev) * (cm[i] - prev);
-        cn += cm[i] * cm[i];
+        ca = cprev;
+        for (int j = mm - 1; j >= std::max(2, mm - 3); j--) {
+          sqrt_e1(alpha, beta, j - 1, cb, 0.5);
+          d[j] = rel_change(ca, cb);
+          ca.swap(cb);
+        }
       }
-      bool ok = sqrt(dn) <= c->ltol * sqrt(cn) || beta[mm - 1] <= 1e-300;
+      d[mm] = rel_change(cm, cprev);
+      bool ok = tail_converged(d, mm, c->ltol) || beta[mm - 1] <= 1e-300;
       if (ok || mm >= c->lmax) {
         done[r] = 1;
         conv[r] = ok;

@@ -288,13 +288,29 @@ int charge_hop(bd_ctx* c) {
 // eight colours in turn; within a colour every cell is one CTA that visits its
 // charges in index order, each exactly once.  A trial follows the reference's
 // proposal rules (partner search, chain ends, occupancy, the two barriers) and
-// accepts with min(1, exp(-barrier - dE/2)), dE the Debye-Hueckel energy change
-// of the move against every other charge (the reference's energy and factor;
-// without its stale starting energy).  The other charges are taken at their
-// sites at the start of the colour, those of the own cell at their current
-// sites; a move therefore ignores only the change of its interaction with
-// charges moved in the same colour, which are at least R away
-// (|dU| <= lambda_B exp(-R kappa)/R per pair).  The draws are Philox4x32-10
+// accepts with min(1, exp(-barrier - dE/2)) (the reference's factor, without
+// its stale starting energy), dE the energy change of the move against every
+// other charge: with Debye-Hueckel electrostatics the reference's screened
+// pair energy; with Ewald electrostatics the unscreened energy the forces
+// use, in FP64:
+//   dE = q sum_o q_o [erfc(beta r)/r]_a^b   (real space, within the cutoff)
+//      + q [Phi0(b) - Phi0(a)]               (mesh reciprocal potential of all
+//                                              charges at the colour's start)
+//      - q^2 [G(b - a) - G(0)]               (the moved charge's own term)
+//      + q sum_j q_j [G(b-b_j) - G(b-a_j) - G(a-b_j) + G(a-a_j)]
+//                                            (charges of the own cell moved
+//                                              earlier in the colour, a_j -> b_j)
+// with G(r) = lambda_B erf(beta r)/r + r^T Q r the reciprocal pair term near
+// the origin (Q the quadratic form of its periodic remainder, from the
+// lattice's k-space sum, (2 pi lambda_B / 3 V) I for a cubic cell; the rest is
+// O(r^4 / L^5); G(0) = 2 beta lambda_B/sqrt(pi)).  The other
+// charges are taken at their sites at the start of the colour, those of the
+// own cell at their current sites; a move therefore ignores only the change
+// of its interaction with charges moved in the same colour in other cells,
+// which are at least R away: the second difference of the pair energy over
+// both hops, |dU| <= 2 lambda_B d^2 / R^3 per pair (hop distance d <= 2.1),
+// 0.005 kT at R = 15 for the bare Coulomb energy, less when screened.  The
+// draws are Philox4x32-10
 // counters (charge, sweep, purpose) under philox_seed, so a sweep does not
 // depend on the launch order.  The partner is the first bead of the charge's
 // Verlet row (sorted ascending, radius 6 > 2.1 plus twice the skin) within
@@ -369,6 +385,64 @@ __global__ void k_hop_fill(const int* __restrict__ cell_of, const int* __restric
     if (cell_of[k] == c) idx[p++] = k;
 }
 
+// The Ewald energy terms of a trial (P > 0): the lab-frame reduced cell, the
+// stored-frame rotation, the reciprocal potential on the mesh, the split.
+struct HopEwald {
+  Cell cell;
+  double cr, sr;
+  const double* phi;
+  const double* Q;  // quadratic form of the reciprocal pair term's periodic remainder
+  int K;
+  double beta, rc2, lambda_b;
+};
+
+__device__ __forceinline__ void hop_lab(const HopEwald& ew, double x, double y, double& lx,
+                                        double& ly) {
+  lx = x * ew.cr - y * ew.sr;
+  ly = x * ew.sr + y * ew.cr;
+}
+
+// Minimum image of d in the reduced cell.
+__device__ __forceinline__ void hop_minimg(const HopEwald& ew, double& dx, double& dy,
+                                           double& dz) {
+  double s[3];
+  frac_of(ew.cell, dx, dy, dz, s);
+  for (int d = 0; d < 3; d++) s[d] -= rint(s[d]);
+  const double* H = ew.cell.H;
+  dx = H[0] * s[0] + H[1] * s[1] + H[2] * s[2];
+  dy = H[3] * s[0] + H[4] * s[1] + H[5] * s[2];
+  dz = H[6] * s[0] + H[7] * s[1] + H[8] * s[2];
+}
+
+__device__ __forceinline__ double hop_rr(const HopEwald& ew, double dx, double dy, double dz) {
+  hop_minimg(ew, dx, dy, dz);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// Real-space pair term lambda_B erfc(beta r)/r within the cutoff.
+__device__ __forceinline__ double hop_real(const HopEwald& ew, double dx, double dy, double dz) {
+  double rr = hop_rr(ew, dx, dy, dz);
+  if (rr >= ew.rc2) return 0.0;
+  double r = sqrt(rr);
+  return ew.lambda_b * erfc(ew.beta * r) / r;
+}
+
+// Reciprocal pair term near the origin, G(r) = lambda_B erf(beta r)/r + r^T Q r
+// (the Gaussian-screened part and the quadratic term of the periodic remainder;
+// its constant cancels in every difference, its O(r^4 / L^5) rest is left
+// out); G(0) = 2 beta lambda_B / sqrt(pi).
+__device__ __forceinline__ double hop_recip(const HopEwald& ew, double dx, double dy, double dz) {
+  hop_minimg(ew, dx, dy, dz);
+  double rr = dx * dx + dy * dy + dz * dz, r = sqrt(rr);
+  if (r <= 1e-12) return ew.lambda_b * 2.0 * ew.beta / sqrt(M_PI);
+  const double* Q = ew.Q;
+  double quad = Q[0] * dx * dx + Q[3] * dy * dy + Q[5] * dz * dz +
+                2.0 * (Q[1] * dx * dy + Q[2] * dx * dz + Q[4] * dy * dz);
+  return ew.lambda_b * erf(ew.beta * r) / r + quad;
+}
+
+// P = 0: Debye-Hueckel trial energies; P = 4, 6, 8: Ewald, B-spline order P.
+template <int P>
 __global__ void __launch_bounds__(1024) k_hop_colour(
     Lat l, HGeom g, int colour, const double* __restrict__ rx, const double* __restrict__ ry,
     const double* __restrict__ rz, int N, int Nb, int nch, const int* __restrict__ start,
@@ -376,7 +450,7 @@ __global__ void __launch_bounds__(1024) k_hop_colour(
     const int* __restrict__ site0, const double* __restrict__ qk, int* track, int* old,
     int* flags, const int* __restrict__ nb_count, const int* __restrict__ nb_rows, int maxnb,
     double lambda_b, double kappa_d, double barrier, double barrier2, unsigned long long seed,
-    unsigned long long sweep, int* log) {
+    unsigned long long sweep, int* log, double* hop_de, HopEwald ew) {
   int cell = blockIdx.x;
   int cz = cell % g.n[2], cy = (cell / g.n[2]) % g.n[1], cx = cell / (g.n[1] * g.n[2]);
   int col = ((g.n[0] > 1 ? cx & 1 : 0) << 2) | ((g.n[1] > 1 ? cy & 1 : 0) << 1) |
@@ -384,6 +458,8 @@ __global__ void __launch_bounds__(1024) k_hop_colour(
   if (col != colour) return;
   __shared__ double red[33];
   __shared__ int s_first, s_c2, s_test, s_block;
+  __shared__ double s_w[2][3][P > 0 ? P : 1];  // Ewald: spline weights of both sites
+  __shared__ int s_base[2][3];
   int t = threadIdx.x, nt = blockDim.x;
   for (int q = start[cell]; q < start[cell + 1]; q++) {
     int k = idx[q];
@@ -436,21 +512,84 @@ __global__ void __launch_bounds__(1024) k_hop_colour(
         log[3 * k] = 0;
         log[3 * k + 1] = c2;
         log[3 * k + 2] = 0;
+        hop_de[k] = __longlong_as_double(0x7ff8000000000000LL);  // no trial energy
       }
       __syncthreads();
       continue;
     }
     double x2 = rx[c2], y2 = ry[c2], z2 = rz[c2], de = 0, qme = qk[k];
-    for (int o = t; o < nch; o += nt) {
-      if (o == k) continue;
-      int b = cell_of[o] == cell ? track[o] : site0[o];
-      double xb = rx[b], yb = ry[b], zb = rz[b];
-      de += qme * qk[o] *
-            (dh_pair(l, x2, y2, z2, xb, yb, zb, lambda_b, kappa_d) -
-             dh_pair(l, xc, yc, zc, xb, yb, zb, lambda_b, kappa_d));
+    if constexpr (P == 0) {
+      for (int o = t; o < nch; o += nt) {
+        if (o == k) continue;
+        int b = cell_of[o] == cell ? track[o] : site0[o];
+        double xb = rx[b], yb = ry[b], zb = rz[b];
+        de += qme * qk[o] *
+              (dh_pair(l, x2, y2, z2, xb, yb, zb, lambda_b, kappa_d) -
+               dh_pair(l, xc, yc, zc, xb, yb, zb, lambda_b, kappa_d));
+      }
+    } else {
+      double ax, ay, bx, by, az = zc, bz = z2;
+      hop_lab(ew, xc, yc, ax, ay);
+      hop_lab(ew, x2, y2, bx, by);
+      // real space against every other charge
+      for (int o = t; o < nch; o += nt) {
+        if (o == k) continue;
+        int b = cell_of[o] == cell ? track[o] : site0[o];
+        double ox, oy, oz = rz[b];
+        hop_lab(ew, rx[b], ry[b], ox, oy);
+        de += qme * qk[o] *
+              (hop_real(ew, bx - ox, by - oy, bz - oz) - hop_real(ew, ax - ox, ay - oy, az - oz));
+      }
+      // spline weights of the two sites (thread 3 pt + d: site pt, direction d)
+      if (t < 6) {
+        int pt = t / 3, d = t % 3;
+        double sv[3];
+        frac_of(ew.cell, pt ? bx : ax, pt ? by : ay, pt ? bz : az, sv);
+        double u = (sv[d] - floor(sv[d])) * ew.K;
+        if (!(u >= 0.0 && u <= (double)ew.K)) u = 0.0;
+        int fl = (int)floor(u);
+        double f = u - fl;
+        if (fl >= ew.K) fl -= ew.K;
+        s_base[pt][d] = fl;
+        double wv[P];
+        bspline_t<P>(f, wv);
+#pragma unroll
+        for (int a = 0; a < P; a++) s_w[pt][d][a] = wv[a];
+      }
+      __syncthreads();
+      // q [Phi0(b) - Phi0(a)] from the mesh
+      constexpr int P3 = P * P * P;
+      const int K = ew.K;
+      for (int e = t; e < 2 * P3; e += nt) {
+        int pt = e / P3, m = e - pt * P3;
+        int cc = m % P, bb = (m / P) % P, aa = m / (P * P);
+        int g0 = s_base[pt][0] - aa, g1 = s_base[pt][1] - bb, g2 = s_base[pt][2] - cc;
+        g0 += g0 < 0 ? K : 0;
+        g1 += g1 < 0 ? K : 0;
+        g2 += g2 < 0 ? K : 0;
+        double v = s_w[pt][0][aa] * s_w[pt][1][bb] * s_w[pt][2][cc] *
+                   ew.phi[((size_t)g0 * K + g1) * K + g2];
+        de += pt ? qme * v : -qme * v;
+      }
+      // the moved charge's own reciprocal term
+      if (t == 0)
+        de -= qme * qme * (hop_recip(ew, bx - ax, by - ay, bz - az) - hop_recip(ew, 0, 0, 0));
+      // charges of this cell that moved earlier in this colour (a_j -> b_j)
+      for (int q2 = start[cell] + t; q2 < q; q2 += nt) {
+        int j = idx[q2];
+        if (log[3 * j] != 1) continue;
+        int aj = old[j], bj = track[j];
+        double ajx, ajy, bjx, bjy, ajz = rz[aj], bjz = rz[bj];
+        hop_lab(ew, rx[aj], ry[aj], ajx, ajy);
+        hop_lab(ew, rx[bj], ry[bj], bjx, bjy);
+        de += qme * qk[j] *
+              (hop_recip(ew, bx - bjx, by - bjy, bz - bjz) - hop_recip(ew, bx - ajx, by - ajy, bz - ajz) -
+               hop_recip(ew, ax - bjx, ay - bjy, az - bjz) + hop_recip(ew, ax - ajx, ay - ajy, az - ajz));
+      }
     }
     de = block_sum(de, red);
     if (t == 0) {
+      hop_de[k] = de;
       double bar = (s_test == 2) ? barrier2 : barrier;
       double x = exp(-bar - 0.5 * de);
       int acc = (1 <= x) ? 1 : (philox_u01(k, sweep, 1, seed) <= x);
@@ -468,6 +607,16 @@ __global__ void __launch_bounds__(1024) k_hop_colour(
   }
 }
 
+// (x, y, z, q) of each charge at its current site, in track order.
+__global__ void k_gather_sites(const double* __restrict__ rx, const double* __restrict__ ry,
+                               const double* __restrict__ rz, const int* __restrict__ track,
+                               const double* __restrict__ qk, int nch, double4* cq) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nch) return;
+  int b = track[k];
+  cq[k] = make_double4(rx[b], ry[b], rz[b], qk[k]);
+}
+
 }  // namespace
 
 namespace bd {
@@ -478,6 +627,11 @@ int charge_hop_parallel(bd_ctx* c) {
     CU(cudaMalloc(&c->hop_cells, 4 * ((size_t)3 * N + 2 * (kHopCellCap + 1))));
     c->bytes += 4 * ((size_t)3 * N + 2 * (kHopCellCap + 1));
     CU(cudaMemsetAsync(c->hop_cells, 0, 4 * ((size_t)3 * N + 2 * (kHopCellCap + 1)), c->stream));
+  }
+  if (!c->hop_de) {
+    CU(cudaMalloc(&c->hop_de, 8 * (size_t)N));
+    c->bytes += 8 * (size_t)N;
+    CU(cudaMemsetAsync(c->hop_de, 0, 8 * (size_t)N, c->stream));
   }
   int* cell_of = c->hop_cells;
   int* idx = cell_of + N;
@@ -520,16 +674,53 @@ int charge_hop_parallel(bd_ctx* c) {
   k_hop_scan<<<1, 1024, 0, c->stream>>>(ncell, count, start);
   k_hop_fill<<<(ncell + 127) / 128, 128, 0, c->stream>>>(cell_of, start, ncell, nch, idx);
   unsigned long long sweep = c->hop_sweeps++;
+  bool ewald = c->p.coulomb == BD_COULOMB_EWALD;
+  HopEwald ew = {};
+  int P = 0;
+  if (ewald) {
+    ew.cell = cell;
+    ew.cr = cr;
+    ew.sr = sr;
+    ew.K = c->pmeK;
+    ew.beta = c->cw_beta;
+    ew.rc2 = c->cw_rc * c->cw_rc;
+    ew.lambda_b = c->p.lambda_b;
+    P = c->pme_p == 4 || c->pme_p == 6 ? c->pme_p : 8;
+    // dE scratch (64 N doubles): [0, 4 nch) the gathered sites, [6 nch, 7 nch)
+    // the charge values, then the six entries of Q
+    double* Q6 = c->dE + 7 * (size_t)nch;
+    int s;
+    if ((s = coulomb_quadform(c, l, Q6)) != BD_OK) return s;
+    ew.Q = Q6;
+  }
+  double4* cq = (double4*)c->dE;  // [0, 4 nch): charges at their sites (Ewald mesh)
   prof_begin(c, BD_PROF_HOP);
   for (int colour = 0; colour < 8; colour++) {
     CU(cudaMemcpyAsync(site0, c->track, 4 * (size_t)nch, cudaMemcpyDeviceToDevice, c->stream));
+    if (ewald) {
+      // the reciprocal potential of the charges at the colour's start
+      c->launches++;
+      k_gather_sites<<<(nch + 255) / 256, 256, 0, c->stream>>>(c->rx, c->ry, c->rz, c->track,
+                                                              qk, nch, cq);
+      int s;
+      if ((s = coulomb_mesh_potential(c, l, cq)) != BD_OK) return s;
+      ew.phi = c->cw_grid;
+    }
     c->launches++;
     // only the cells of one colour work in a launch (ncell / 8 CTAs): 1024
     // threads share each trial's energy sum over the charges
-    k_hop_colour<<<ncell, 1024, 0, c->stream>>>(
-        l, g, colour, c->rx, c->ry, c->rz, N, c->Nb, nch, start, idx, cell_of, site0, qk,
-        c->track, c->old, c->cflags, c->nb_count, c->nb_rows, c->maxnb, c->p.lambda_b,
-        c->kappa_d, c->p.barrier, c->p.barrier2, c->p.philox_seed, sweep, c->hoplog);
+#define HOP_COLOUR(P_)                                                                         \
+  k_hop_colour<P_><<<ncell, 1024, 0, c->stream>>>(                                             \
+      l, g, colour, c->rx, c->ry, c->rz, N, c->Nb, nch, start, idx, cell_of, site0, qk,        \
+      c->track, c->old, c->cflags, c->nb_count, c->nb_rows, c->maxnb, c->p.lambda_b,           \
+      c->kappa_d, c->p.barrier, c->p.barrier2, c->p.philox_seed, sweep, c->hoplog, c->hop_de, ew)
+    switch (P) {
+      case 0: HOP_COLOUR(0); break;
+      case 4: HOP_COLOUR(4); break;
+      case 6: HOP_COLOUR(6); break;
+      default: HOP_COLOUR(8);
+    }
+#undef HOP_COLOUR
   }
   prof_end(c, BD_PROF_HOP);
   c->launches += 2;
@@ -539,3 +730,11 @@ int charge_hop_parallel(bd_ctx* c) {
 }
 
 }  // namespace bd
+
+extern "C" int bd_download_hop_energies(bd_ctx* c, double* de) {
+  if (!c || (c->nch > 0 && !de)) return BD_ERR_ARG;
+  if (c->nch == 0) return BD_OK;
+  if (!c->hop_de) return BD_ERR_STATE;
+  CU(cudaMemcpyAsync(de, c->hop_de, 8 * (size_t)c->nch, cudaMemcpyDeviceToHost, c->stream));
+  return check(c);
+}

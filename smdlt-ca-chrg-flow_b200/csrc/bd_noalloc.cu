@@ -19,7 +19,12 @@
 //    GPU (two streams at once, or two contexts on one device) race on it;
 //  - the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (a host name for a __device__ array is not a
-//    device address); make that first call before any stream capture.
+//    device address); make that first call before any stream capture;
+//  - the address is kept per device ordinal for the life of the process: a
+//    cudaDeviceReset destroys the array with the device's context (and every
+//    bd_ctx made before it), and calls after a reset are not supported;
+//  - it applies to the dense-tile mobilities (BD_MOB_EWALD, BD_MOB_HYBRID);
+//    a particle-mesh context has no tiles and gets BD_ERR_STATE.
 #include <math.h>
 
 #include <mutex>
@@ -149,8 +154,13 @@ static double* scratch_address(int dev, int* status) {
   }
   if (!addr[dev]) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-      *status = BD_ERR_CUDA;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      // not a sticky error: clear it so that the next launch check of another
+      // entry point does not report it as its own
+      cudaGetLastError();
+      *status = bd::cuda_fail((int)(e != cudaSuccess ? e : cudaErrorInvalidSymbol),
+                              "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
       return nullptr;
     }
     addr[dev] = (double*)p;
@@ -177,5 +187,5 @@ extern "C" int bd_mobility_apply_noalloc(bd_ctx* c, const double* v, double* out
   k_na_reduce1<<<dim3(NT, kSplit), 96, 0, c->stream>>>(NT, scratch);
   k_na_reduce2<<<NT, 96, 0, c->stream>>>(c->N, scratch, v, c->Dtr[0], c->Dtr[1], c->Dtr[2], out);
   c->launches += 3;
-  return cudaGetLastError() == cudaSuccess ? BD_OK : BD_ERR_CUDA;
+  return launch_ok(c);
 }

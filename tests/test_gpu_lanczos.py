@@ -4,9 +4,11 @@ oracle is the project's FP64 restatement and a dense eigendecomposition):
 * the Ewald-summed RPY tensor for every pair against oracle/bd_oracle.c's
   bdo_calc_hi_ewald, FP64, 1e-10 relative;
 * M v against the dense product, FP64 1e-10 and FP32-stored tiles 1e-6;
-* the Lanczos sqrt(M) z (tolerance 1e-6 on the relative change between
-  iterates) against numpy.linalg.eigh's square root, 1e-5 relative for FP64
-  and FP32 storage;
+* the Lanczos sqrt(M) z at tolerance 1e-6 (the solve stops when the geometric
+  tail of its successive changes, an estimate of the iterate's own error, is
+  below the tolerance) against numpy.linalg.eigh's square root: 1e-6
+  relative with FP64 tiles; with FP32-stored tiles the operator itself is off
+  by about 1e-7, so 2e-6;
 * a few hundred Krylov Brownian steps run without error and keep every FENE
   bond inside qmax.
 """
@@ -67,8 +69,8 @@ def test_mobility_product(flow, precision, tol):
 
 
 @pytest.mark.parametrize("flow", [0, 1])
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_lanczos_sqrt_vs_eigh(flow, precision):
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-6), ("fp32", 2e-6)])
+def test_lanczos_sqrt_vs_eigh(flow, precision, tol):
     c, o, (x, y, z) = _prepared(flow, 500, precision)
     Mf = O.full_mobility(o.calc_hi_ewald(x, y, z), o.N)
     zz = np.random.default_rng(7).normal(size=3 * o.N)
@@ -76,7 +78,7 @@ def test_lanczos_sqrt_vs_eigh(flow, precision):
     assert lmin > 0
     got, iters = c.lanczos_sqrt(zz)
     assert 2 <= iters < 80
-    assert rel_err(got, ref) < 1e-5, (iters, rel_err(got, ref))
+    assert rel_err(got, ref) < tol, (iters, rel_err(got, ref))
     st = c.lanczos_stats()
     assert st["calls"] == 1 and st["maxed"] == 0 and st["negative"] == 0
 

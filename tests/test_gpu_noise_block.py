@@ -155,8 +155,12 @@ def test_default_tolerance_fp32():
     blk = _run(10, tol=1e-6, precision="fp32", steps=10, srpy=100, precond="segment")
     (ca, x0, xa), (cb, _, xb) = ref, blk
     assert np.array_equal(ca.noise(), cb.noise())
-    # each displacement within a few tolerances of the per-step one
-    assert np.linalg.norm(xa - xb) <= 1e-5 * np.linalg.norm(xa - x0)
+    # each run within the tolerance (1e-6) of its own operator's root; the
+    # block product (complex-packed pairs) and the single product (real
+    # transforms) differ by up to 2e-6 in FP32 storage, so 3e-6 of the
+    # displacement over the ten steps
+    assert np.linalg.norm(xa - xb) <= 3e-6 * np.linalg.norm(xa - x0), (
+        np.linalg.norm(xa - xb) / np.linalg.norm(xa - x0))
     ia = ca.lanczos_stats()["iterations"] / 10
     ib = cb.lanczos_stats()["iterations"] / 10
     assert abs(ia - ib) <= 2.0, (ia, ib)

@@ -14,8 +14,11 @@ No reference counterpart; checked against
   the converged Ewald model of oracle/pme_oracle.py;
 * FP32 storage of grids, transforms, influence and pair tensors (FP64
   accumulation) against the FP64 path, 1e-5 relative;
-* the dense square root: Lanczos sqrt(M) z with the PME product against
-  numpy.linalg.eigh of the dense Ewald matrix, 3e-5 relative;
+* the square root: Lanczos sqrt(M) z at tolerance 1e-6 with the FP64 PME
+  product against numpy.linalg.eigh of the PME operator itself (assembled
+  column by column from the same product), 1e-6 relative (the Krylov gate);
+  and against eigh of the dense Ewald matrix, 3e-5 (the gate plus the
+  particle-mesh discretisation);
 * the noise blocks' multi-vector product (bd_mobility_apply_block: right-hand
   sides packed in complex pairs, in-place complex transforms, influence on
   the full spectrum) against one product per vector (real-to-complex
@@ -104,6 +107,12 @@ def test_pme_lanczos_vs_eigh(flow):
     got, iters = c.lanczos_sqrt(zz)
     assert 2 <= iters < 80
     assert rel_err(got, ref) < 3e-5, (iters, rel_err(got, ref))
+    # the operator the solve sees: symmetric to rounding
+    Mp = np.stack([c.mobility_apply(e) for e in np.eye(3 * o.N)], 1)
+    assert rel_err(Mp, Mp.T) < 1e-12
+    ref_p, lmin_p = O.sqrtm_apply(0.5 * (Mp + Mp.T), zz)
+    assert lmin_p > 0
+    assert rel_err(got, ref_p) < 1e-6, (iters, rel_err(got, ref_p))
 
 
 @pytest.mark.parametrize("flow,t", [(0, 3000), (1, 4500)])
