@@ -429,7 +429,9 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
     lan0 = c.lanczos_stats()
     pre0 = c.precond_stats()
     blk0 = c.noise_block_stats()
-    c.profile(True)
+    # step-level events only: per-product events would put the noise blocks'
+    # Krylov loop back on the host (the products are timed in a pass below)
+    c.profile(2)
     n0 = c.launches()
     dev = int(os.environ.get("LOCAL_RANK", 0))
     with ClockSampler(dev) as clk:
@@ -479,6 +481,15 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
         c.inverse_coords()
     c.sync()
     per = {k: c.profile_read(getattr(c, "PROF_" + k)) for k in ("HI_BUILD", "HOP")}
+    c.profile(False)
+    # the dominant kernel, timed: the products of one noise block, each between
+    # CUDA events on the library's stream (this pass checks convergence on the
+    # host; the product kernels are those of the timed steps)
+    c.noise_block_release()
+    c.profile(True)
+    step(tp + 1, nb, False)
+    c.sync()
+    prof["BLOCK"] = c.profile_read(c.PROF_BLOCK)
     c.profile(False)
     t_build = per["HI_BUILD"][0] / max(per["HI_BUILD"][1], 1)
     t_sweep = per["HOP"][0] / max(per["HOP"][1], 1)

@@ -269,7 +269,25 @@ enum {
  * graph captured on first use (default on; off launches the kernels one by
  * one).  Captured products do not record BD_PROF_MATVEC events. */
 int bd_enable_graphs(bd_ctx *ctx, int on);
-int bd_profile_enable(bd_ctx *ctx, int on); /* clears the accumulated events */
+/* Convergence of the noise blocks' Krylov runs checked on the device (default
+ * on; no reference counterpart).  After every iteration one CTA per
+ * right-hand side forms T^(1/2) e_1 of its tridiagonal T in FP64 by a
+ * trapezoidal quadrature of (2/pi) int T (t^2 + T)^-1 e_1 dt (one tridiagonal
+ * solve per node, no eigen-decomposition) and applies the stopping test; with
+ * graphs on, the whole solve of a block is one CUDA graph whose conditional
+ * while node repeats the iteration until every right-hand side has stopped,
+ * with no host round trip.  Off (or with profiling on, which times each
+ * product): the host checks one iteration behind with the implicit QR.  A
+ * tridiagonal that is not positive definite (never expected of a mobility)
+ * is re-solved on the host, which clamps its negative Ritz values. */
+int bd_set_device_krylov(bd_ctx *ctx, int on);
+/* Noise-block solves controlled on the device, and blocks re-solved on the
+ * host (non-positive tridiagonal), since creation. */
+int bd_krylov_check_stats(bd_ctx *ctx, long *out2);
+/* on = 1: every slot; on = 2: every slot but BD_PROF_BLOCK, whose per-product
+ * events need the host-checked Krylov loop (so 2 times the device-checked
+ * one); 0: off.  Clears the accumulated events. */
+int bd_profile_enable(bd_ctx *ctx, int on);
 int bd_profile_read(bd_ctx *ctx, int slot, double *total_ms, long *count);
 /* Number of kernels the library has launched on this context. */
 long long bd_launch_count(const bd_ctx *ctx);

@@ -139,6 +139,8 @@ def _lib() -> C.CDLL:
         L.bd_mobility_apply_block.argtypes = [vp, C.c_int, _dp, _dp]
         L.bd_lanczos_sqrt.argtypes = [vp, _dp, _dp, C.POINTER(C.c_int)]
         L.bd_lanczos_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        L.bd_krylov_check_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        L.bd_set_device_krylov.argtypes = [vp, C.c_int]
         L.bd_noise_block_stats.argtypes = [vp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
         L.bd_noise_block_release.argtypes = [vp]
         L.bd_step_lanczos.argtypes = [vp, C.c_ulong, C.c_int, C.c_int]
@@ -662,7 +664,18 @@ class Context:
         self._call("bd_mpnn_adam", float(lr), float(beta1), float(beta2), float(eps), int(step))
 
     def profile(self, on=True):
-        self._call("bd_profile_enable", int(bool(on)))
+        """True / 1: every event slot (noise-block products timed one by one,
+        which runs the host-checked Krylov loop); 2: every slot but the
+        block products (the device-checked loop); False: off."""
+        self._call("bd_profile_enable", 2 if on == 2 else int(bool(on)))
+
+    def set_device_krylov(self, on=True):
+        self._call("bd_set_device_krylov", int(bool(on)))
+
+    def krylov_check_stats(self):
+        o = np.zeros(2, np.int64)
+        self._call("bd_krylov_check_stats", o)
+        return dict(device_solves=int(o[0]), host_fallbacks=int(o[1]))
 
     def profile_read(self, slot):
         ms, n = C.c_double(), C.c_long()

@@ -788,6 +788,7 @@ int bd_create(const bd_params* p, bd_ctx** out) {
     }
   }
   c->use_graphs = true;
+  c->device_krylov = true;
   c->t = 0;
   c->tstart = 0;
   host_lattice(c, 0, &c->lat);
@@ -838,11 +839,26 @@ int bd_enable_graphs(bd_ctx* c, int on) {
   return BD_OK;
 }
 
+int bd_set_device_krylov(bd_ctx* c, int on) {
+  if (!c) return BD_ERR_ARG;
+  CU(cudaStreamSynchronize(c->stream));
+  c->device_krylov = on != 0;
+  return BD_OK;
+}
+
+int bd_krylov_check_stats(bd_ctx* c, long* out2) {
+  if (!c || !out2) return BD_ERR_ARG;
+  out2[0] = (long)c->dev_solves;
+  out2[1] = (long)c->host_fallbacks;
+  return BD_OK;
+}
+
 int bd_profile_enable(bd_ctx* c, int on) {
   if (!c) return BD_ERR_ARG;
   CU(cudaStreamSynchronize(c->stream));
   prof_clear(c);
   c->prof_on = on != 0;
+  c->prof_products = on == 1;
   return BD_OK;
 }
 
@@ -1251,6 +1267,7 @@ void rotate_coords(bd_ctx* c, int inverse) {
 namespace bd {
 void prof_begin(bd_ctx* c, int slot) {
   if (!c->prof_on || c->capturing) return;
+  if (slot == BD_PROF_BLOCK && !c->prof_products) return;
   cudaEvent_t e;
   cudaEventCreate(&e);
   cudaEventRecord(e, c->stream);
@@ -1258,6 +1275,7 @@ void prof_begin(bd_ctx* c, int slot) {
 }
 void prof_end(bd_ctx* c, int slot) {
   if (!c->prof_on || c->capturing) return;
+  if (slot == BD_PROF_BLOCK && !c->prof_products) return;
   cudaEvent_t e;
   cudaEventCreate(&e);
   cudaEventRecord(e, c->stream);

@@ -113,6 +113,17 @@ struct bd_ctx {
   double *Bc;          // nbk x (lmax+1) combination coefficients
   int *Bm;             // nbk Krylov dimensions
   int *Bjd;
+  int *Bctl;           // device convergence check, k ints each: done, conv, neg, last
+                       // checked dimension, consecutive changes known; then the first
+                       // dimension to check
+  double *Bdh;         // the last four relative changes per right-hand side
+  double *Bpsi;        // quadrature pivots of the device check (k L1 nodes)
+  void *blk_while[4];  // whole noise-block solves as one graph (conditional while node),
+  int blk_while_key[4];
+  long long blk_while_launches[4];
+  bool device_krylov;  // convergence checks on the device (default); host QR otherwise
+  long long dev_solves, host_fallbacks;
+  bool while_failed;   // the conditional graph could not be built: host checks
   double *Bhost;       // pinned host copy of alpha, beta
   void *blk_ev;        // cudaEvent_t of the pending convergence check
   void *blk_graph[4][2];  // captured block iterations (product, orthogonalisation),
@@ -193,6 +204,7 @@ struct bd_ctx {
 
   // profiling: CUDA events around selected kernels on the context's stream
   bool prof_on;
+  bool prof_products;  // per-product events of noise blocks (host-checked Krylov loop)
   std::vector<cudaEvent_t> prof_ev[BD_PROF_SLOTS][2];
   long long launches;  // kernels launched by the library
 };

@@ -303,6 +303,174 @@ __global__ void k_next_j(int* jd) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *jd += 1;
 }
 
+// ---------------------------------------------------------------------------
+// Convergence of the noise blocks' Krylov runs, checked on the device.
+//
+// T^(1/2) e_1 = (2/pi) int_0^inf T (t^2 I + T)^(-1) e_1 dt.  With t = e^u the
+// component along an eigenvector of T (eigenvalue lambda) is
+// (2/pi) sqrt(lambda) / (2 cosh(u - ln sqrt(lambda))), analytic in the strip
+// |Im u| < pi/2, so the trapezoidal rule with step h converges like
+// exp(-pi^2/h) (Trefethen and Weideman, SIAM Rev. 56, 385 (2014)): nodes on
+// u in [-33, 41] with h = 74/255 form T^(1/2) e_1 to about 1e-14 for every
+// eigenvalue in [1e-4, 1e8], with no estimate of the spectrum.  Each node is
+// one tridiagonal solve x = (T + s)^(-1) e_1, s = t^2, by the backward (UL)
+// elimination, pivots psi_(m-1) = alpha_(m-1) + s,
+// psi_i = alpha_i + s - beta_i^2 / psi_(i+1), then x_0 = 1/psi_0,
+// x_(i+1) = -beta_i x_i / psi_(i+1); the node adds w (T x) (not e_1 - s x,
+// which cancels for large s).  One CTA per right-hand side, one node per
+// thread; the pivots go through a global scratch row per node.
+constexpr int kQuadNodes = 256;
+constexpr double kQuadU0 = -33.0, kQuadU1 = 41.0;
+
+struct BlkCheck {
+  const double* alpha;  // alpha_j of right-hand side r at [j k + r]
+  const double* beta;
+  int k, L1, lmax;
+  double tol;
+  const int* jd;        // Krylov dimension reached
+  int* done;
+  int* conv;
+  int* neg;
+  int* last;            // dimension of the coefficients in c (-1: none)
+  int* nd;              // consecutive relative changes known (up to 4)
+  const int* first;     // first dimension to check
+  int* mr;              // Krylov dimension used per right-hand side
+  double* dh;           // 4 per right-hand side, ring indexed by dimension % 4
+  double* c;            // coefficients, L1 per right-hand side
+  double* psi;          // k x L1 x kQuadNodes scratch
+};
+
+// One quadrature solve of T_mm^(1/2) e_1 into cm (shared, zeroed here).
+__device__ void quad_sqrt_e1(const double* a, const double* b, int mm, double* cm,
+                             double* psi_row, int* bad) {
+  int t = threadIdx.x, lane = t & 31;
+  for (int i = t; i < mm; i += blockDim.x) cm[i] = 0.0;
+  __syncthreads();
+  const double h = (kQuadU1 - kQuadU0) / (kQuadNodes - 1);
+  double u = kQuadU0 + h * t, et = exp(u);
+  double sN = et * et, w = (2.0 / M_PI) * h * et;
+  // backward pivots (their inverses), node t at psi_row[i * kQuadNodes + t]
+  double p = a[mm - 1] + sN;
+  int badp = !(p > 0.0);
+  double ip = 1.0 / p;
+  psi_row[(size_t)(mm - 1) * kQuadNodes + t] = ip;
+  for (int i = mm - 2; i >= 0; i--) {
+    p = a[i] + sN - b[i] * b[i] * ip;
+    badp |= !(p > 0.0);
+    ip = 1.0 / p;
+    psi_row[(size_t)i * kQuadNodes + t] = ip;
+  }
+  // forward: x_i, and (T x)_i = beta_(i-1) x_(i-1) + alpha_i x_i + beta_i x_(i+1)
+  double xm1 = 0.0, x = ip;  // ip = 1/psi_0
+  for (int i = 0; i < mm; i++) {
+    double xp1 = i + 1 < mm ? -b[i] * x * psi_row[(size_t)(i + 1) * kQuadNodes + t] : 0.0;
+    double y = (i > 0 ? b[i - 1] * xm1 : 0.0) + a[i] * x + (i + 1 < mm ? b[i] * xp1 : 0.0);
+    double v = badp ? 0.0 : w * y;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(&cm[i], v);
+    xm1 = x;
+    x = xp1;
+  }
+  if (badp) atomicOr(bad, 1);
+  __syncthreads();
+}
+
+// After an iteration: for every open right-hand side at or past the first
+// checked dimension, the coefficients c_m = T_m^(1/2) e_1, the relative
+// change against c_(m-1) (the previous check's, or solved here at a first
+// check, with those of m-2 .. m-4), and the host path's stopping test (tail
+// d_m rho/(1-rho) <= tol, rho the largest of the last three ratios, capped at
+// 0.99; or a breakdown beta_(m-1) <= 1e-300; or the Krylov cap).
+__global__ void __launch_bounds__(kQuadNodes) k_block_check(BlkCheck q) {
+  extern __shared__ double sh[];
+  int r = blockIdx.x, t = threadIdx.x, L1 = q.L1;
+  int m = *q.jd;
+  if (q.done[r] || (m < *q.first && m < q.lmax)) return;  // uniform over the CTA
+  double* a = sh;
+  double* b = sh + L1;
+  double* cm = sh + 2 * L1;
+  double* red = sh + 3 * L1;
+  __shared__ int bad;
+  if (t == 0) bad = 0;
+  for (int i = t; i < m; i += blockDim.x) {
+    a[i] = q.alpha[(size_t)i * q.k + r];
+    b[i] = q.beta[(size_t)i * q.k + r];
+  }
+  __syncthreads();
+  double* crow = q.c + (size_t)r * L1;
+  double* psi_row = q.psi + (size_t)r * L1 * kQuadNodes;
+  int mm0 = q.last[r] == m - 1 ? m : max(1, m - 4);
+  if (mm0 < m && t == 0) q.nd[r] = 0;
+  for (int mm = mm0; mm <= m; mm++) {
+    quad_sqrt_e1(a, b, mm, cm, psi_row, &bad);
+    // relative change against the coefficients of mm - 1 in crow
+    double dn = 0.0, cn = 0.0;
+    bool have_prev = q.last[r] == mm - 1;
+    for (int i = t; i < mm; i += blockDim.x) {
+      double prev = (have_prev && i < mm - 1) ? crow[i] : 0.0;
+      dn += (cm[i] - prev) * (cm[i] - prev);
+      cn += cm[i] * cm[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      dn += __shfl_xor_sync(0xffffffffu, dn, o);
+      cn += __shfl_xor_sync(0xffffffffu, cn, o);
+    }
+    if ((t & 31) == 0) {
+      red[2 * (t >> 5)] = dn;
+      red[2 * (t >> 5) + 1] = cn;
+    }
+    __syncthreads();
+    if (t == 0) {
+      double D = 0.0, Cn = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+        D += red[2 * w];
+        Cn += red[2 * w + 1];
+      }
+      if (have_prev) {
+        q.dh[4 * r + (mm & 3)] = Cn > 0 ? sqrt(D / Cn) : 0.0;
+        q.nd[r] = min(q.nd[r] + 1, 4);
+      }
+    }
+    __syncthreads();  // every thread has read crow and last before they change
+    for (int i = t; i < mm; i += blockDim.x) crow[i] = cm[i];
+    if (t == 0) q.last[r] = mm;
+    __syncthreads();
+  }
+  if (t == 0) {
+    if (bad) q.neg[r] = 1;
+    bool ok = false;
+    if (q.nd[r] >= 4) {
+      double rho = 0.0;
+      for (int j = m - 2; j <= m; j++) {
+        double d1 = q.dh[4 * r + (j & 3)], d0 = q.dh[4 * r + ((j - 1) & 3)];
+        rho = fmax(rho, d0 > 0 ? d1 / d0 : 0.0);
+      }
+      rho = fmin(rho, 0.99);
+      ok = q.dh[4 * r + (m & 3)] * rho / (1.0 - rho) <= q.tol;
+    }
+    ok = ok || b[m - 1] <= 1e-300;
+    if (ok || m >= q.lmax || bad) {
+      q.done[r] = 1;
+      q.conv[r] = ok && !bad;
+      q.mr[r] = m;
+    }
+  }
+}
+
+// The while node's condition: another iteration while a right-hand side is
+// open and the cap is not reached.
+__global__ void k_block_cond(const int* __restrict__ done, int k, const int* __restrict__ jd,
+                             int lmax, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  int nd = 0;
+  for (int r = 0; r < k; r++) nd += done[r];
+  cudaGraphSetConditional(h, (nd < k && *jd < lmax) ? 1u : 0u);
+}
+
+__global__ void k_set_int(int* p, int v) {
+  if (threadIdx.x == 0) *p = v;
+}
+
 // |z|^2 partials over the bead-interleaved noise (right-hand side blockIdx.y:
 // z zs entries further on, partials gridDim.x further on)
 __global__ void __launch_bounds__(256) k_sumsq(const double* __restrict__ z, size_t zs, int n,
@@ -690,6 +858,11 @@ void lanczos_graphs_reset(bd_ctx* c) {
         cudaGraphExecDestroy((cudaGraphExec_t)c->blk_graph[v][h]);
         c->blk_graph[v][h] = nullptr;
       }
+  for (int v = 0; v < 4; v++)
+    if (c->blk_while[v]) {
+      cudaGraphExecDestroy((cudaGraphExec_t)c->blk_while[v]);
+      c->blk_while[v] = nullptr;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -719,6 +892,10 @@ static int alloc_blocks(bd_ctx* c) {
   CU(cudaMalloc(&c->Bc, 8 * (size_t)k * L1));
   CU(cudaMalloc(&c->Bm, 4 * (size_t)k));
   CU(cudaMalloc(&c->Bjd, 16));
+  CU(cudaMalloc(&c->Bctl, 4 * (size_t)(5 * k + 4)));
+  CU(cudaMalloc(&c->Bdh, 8 * 4 * (size_t)k));
+  CU(cudaMalloc(&c->Bpsi, 8 * (size_t)k * L1 * kQuadNodes));
+  c->bytes += 4 * (size_t)(5 * k + 4) + 32 * (size_t)k + 8 * (size_t)k * L1 * kQuadNodes;
   if (!c->Bhost) return BD_ERR_STATE;  // pinned at bd_create (see there)
   CU(cudaMalloc(&c->Brng, sizeof(Ran1) * (size_t)(k + 1)));
   cudaEvent_t ev;
@@ -735,6 +912,11 @@ void lanczos_blocks_free(bd_ctx* c) {
     if (q) cudaFree(q);
   if (c->Bm) cudaFree(c->Bm);
   if (c->Bjd) cudaFree(c->Bjd);
+  if (c->Bctl) cudaFree(c->Bctl);
+  if (c->Bdh) cudaFree(c->Bdh);
+  if (c->Bpsi) cudaFree(c->Bpsi);
+  c->Bctl = nullptr;
+  c->Bdh = c->Bpsi = nullptr;
   if (c->Bhost) cudaFreeHost(c->Bhost);
   if (c->Brng) cudaFree(c->Brng);
   c->Brng = nullptr;
@@ -871,11 +1053,192 @@ static void parallel_for(int n, F f) {
   HostPool::get().run(n, f);
 }
 
+static BlkCheck block_check_args(bd_ctx* c, int k) {
+  int L1 = c->lmax + 1;
+  BlkCheck q;
+  q.alpha = c->Bab;
+  q.beta = c->Bab + (size_t)L1 * k;
+  q.k = k;
+  q.L1 = L1;
+  q.lmax = c->lmax;
+  q.tol = c->ltol;
+  q.jd = c->Bjd;
+  q.done = c->Bctl;
+  q.conv = c->Bctl + k;
+  q.neg = c->Bctl + 2 * k;
+  q.last = c->Bctl + 3 * k;
+  q.nd = c->Bctl + 4 * k;
+  q.first = c->Bctl + 5 * k;
+  q.mr = c->Bm;
+  q.dh = c->Bdh;
+  q.c = c->Bc;
+  q.psi = c->Bpsi;
+  return q;
+}
+
+// The whole solve of a block of k right-hand sides (preconditioned or not) as
+// one graph: a conditional while node whose body is one block iteration
+// (product, orthogonalisation), the device check and the condition kernel.
+// Built once per (k, pre) and kept until the captured buffers change.
+static int block_while_graph(bd_ctx* c, int k, bool pre, cudaGraphExec_t* out) {
+  int key = 2 * k + (pre ? 1 : 0), slot = -1;
+  for (int q = 0; q < 4 && slot < 0; q++)
+    if (c->blk_while[q] && c->blk_while_key[q] == key) slot = q;
+  if (slot >= 0) {
+    *out = (cudaGraphExec_t)c->blk_while[slot];
+    return BD_OK;
+  }
+  for (int q = 0; q < 4 && slot < 0; q++)
+    if (!c->blk_while[q]) slot = q;
+  if (slot < 0) {
+    slot = 3;
+    cudaGraphExecDestroy((cudaGraphExec_t)c->blk_while[slot]);
+    c->blk_while[slot] = nullptr;
+  }
+  cudaStream_t st = c->stream;
+  cudaGraph_t g = nullptr;
+  CU(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t node;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+  int s = BD_OK;
+  long long l0 = c->launches;
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      c->capturing = true;
+      s = block_part(c, k, pre, 0);
+      if (s == BD_OK) s = block_part(c, k, pre, 1);
+      if (s == BD_OK) {
+        BlkCheck q = block_check_args(c, k);
+        size_t smem = 8 * (3 * (size_t)q.L1 + 16);
+        if (smem > 48 * 1024)
+          cudaFuncSetAttribute(k_block_check, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+        k_block_check<<<k, kQuadNodes, smem, st>>>(q);
+        k_block_cond<<<1, 32, 0, st>>>(c->Bctl, k, c->Bjd, c->lmax, h);
+        c->launches += 2;
+      }
+      cudaGraph_t cap = nullptr;
+      cudaError_t e2 = cudaStreamEndCapture(st, &cap);
+      c->capturing = false;
+      if (e == cudaSuccess) e = e2;
+    }
+  }
+  cudaGraphExec_t ex = nullptr;
+  if (s == BD_OK && e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  long long per_iter = c->launches - l0;
+  c->launches = l0;
+  if (s != BD_OK || e != cudaSuccess) {
+    // not sticky: the host-checked path takes over for this context
+    cudaGetLastError();
+    c->while_failed = true;
+    return BD_ERR_STATE;
+  }
+  c->blk_while[slot] = (void*)ex;
+  c->blk_while_key[slot] = key;
+  c->blk_while_launches[slot] = per_iter;
+  *out = ex;
+  return BD_OK;
+}
+
+// lanczos_run_multi with the convergence checks and the iteration loop on the
+// device: one graph launch for the whole block, one synchronisation at its end.
+static int lanczos_run_multi_device(bd_ctx* c, int k, bool pre, double* out,
+                                    std::vector<int>& mr, std::vector<char>& conv,
+                                    int* iters_run) {
+  int s, N = c->N, NTp = c->NT * 32, blk = kDotBlocks, L1 = c->lmax + 1;
+  size_t n = 3 * (size_t)NTp;
+  cudaStream_t st = c->stream;
+  cudaGraphExec_t ex;
+  if ((s = block_while_graph(c, k, pre, &ex)) != BD_OK) return s;
+  long long per_iter = 0;
+  for (int q = 0; q < 4; q++)
+    if (c->blk_while[q] == (void*)ex) per_iter = c->blk_while_launches[q];
+  c->launches += 5;
+  k_sumsq<<<dim3(blk, k), 256, 0, st>>>(c->BR, 3 * (size_t)N, 3 * N, c->Bpart);
+  k_norm_fin<<<k, 32, 0, st>>>(c->Bpart, blk, c->Bsc);
+  k_interleaved_to_soa<<<dim3((NTp + 255) / 256, k), 256, 0, st>>>(c->BR, 3 * (size_t)N, c->Bsc,
+                                                                   c->BV, n, N, NTp);
+  CU(cudaMemcpyAsync(c->Bvcur, c->BV, 8 * n * k, cudaMemcpyDeviceToDevice, st));
+  CU(cudaMemsetAsync(c->Bjd, 0, sizeof(int), st));
+  CU(cudaMemsetAsync(c->Bctl, 0, 4 * 3 * (size_t)k, st));             // done, conv, neg
+  CU(cudaMemsetAsync(c->Bctl + 3 * k, 0xff, 4 * (size_t)k, st));      // last = -1
+  CU(cudaMemsetAsync(c->Bctl + 4 * k, 0, 4 * (size_t)k, st));         // nd
+  k_set_int<<<1, 32, 0, st>>>(c->Bctl + 5 * k, std::max(5, c->blk_last - 2));
+  if ((s = launch_ok(c)) != BD_OK) return s;
+  CU(cudaGraphLaunch(ex, st));
+  k_combo_m<<<dim3(blk, k), 256, 0, st>>>(c->BV, n * k, c->Bc, L1, c->Bm, c->Bsc, out, (int)n);
+  // Krylov dimensions, outcomes, negative-pivot flags and iterations run
+  int* h = (int*)c->Bhost;
+  CU(cudaMemcpyAsync(h, c->Bm, 4 * (size_t)k, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(h + k, c->Bctl + k, 4 * 2 * (size_t)k, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(h + 3 * k, c->Bjd, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  if ((s = launch_ok(c)) != BD_OK) return s;
+  int j = h[3 * k];
+  mr.assign(h, h + k);
+  conv.assign(k, 0);
+  std::vector<int> negr;
+  for (int r = 0; r < k; r++) {
+    conv[r] = (char)h[k + r];
+    if (h[2 * k + r]) negr.push_back(r);
+  }
+  c->launches += per_iter * j;
+  if (!negr.empty()) {
+    // a tridiagonal that is not positive definite: the host's QR square root
+    // (negative Ritz values clamped to zero), as the host-checked path does
+    c->host_fallbacks++;
+    std::vector<double> ab(2 * (size_t)L1 * k);
+    CU(cudaMemcpyAsync(ab.data(), c->Bab, 8 * ab.size(), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    for (int r : negr) {
+      int mm = mr[r];
+      std::vector<double> alpha(mm), beta(mm), cm;
+      for (int i = 0; i < mm; i++) {
+        alpha[i] = ab[(size_t)i * k + r];
+        beta[i] = ab[(size_t)L1 * k + (size_t)i * k + r];
+      }
+      c->lan_negative += sqrt_e1(alpha, beta, mm, cm, 0.5);
+      conv[r] = 0;
+      CU(cudaMemcpyAsync(c->Bc + (size_t)r * L1, cm.data(), 8 * (size_t)mm,
+                         cudaMemcpyHostToDevice, st));
+    }
+    c->launches++;
+    k_combo_m<<<dim3(blk, k), 256, 0, st>>>(c->BV, n * k, c->Bc, L1, c->Bm, c->Bsc, out, (int)n);
+    CU(cudaStreamSynchronize(st));  // the host vectors above are read by the copies
+  }
+  int mmin = c->lmax;
+  for (int r = 0; r < k; r++) mmin = std::min(mmin, mr[r]);
+  c->blk_last = mmin;
+  c->blk_runs++;
+  c->blk_products += j;
+  c->blk_rhs_products += (long long)j * k;
+  c->dev_solves++;
+  if (iters_run) *iters_run = j;
+  return launch_ok(c);
+}
+
 // Lanczos for sqrt(A) z_r, r < k, z_r = BR + 3 N r; the results
 // |z_r| V_r,m f(T_r,m) e_1 go to out + r n.  mr[r] is the Krylov dimension of
 // right-hand side r, conv[r] whether it met the tolerance within the cap.
+// With device checks (and graphs, without per-product profiling) the loop runs
+// on the device; otherwise the host checks one iteration behind.
 static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vector<int>& mr,
                              std::vector<char>& conv, int* iters_run) {
+  if (c->device_krylov && c->use_graphs && !c->prof_products && !c->while_failed) {
+    int s = lanczos_run_multi_device(c, k, pre, out, mr, conv, iters_run);
+    if (s != BD_ERR_STATE || !c->while_failed) return s;
+  }
   int s, N = c->N, NTp = c->NT * 32, blk = kDotBlocks, L1 = c->lmax + 1;
   size_t n = 3 * (size_t)NTp;
   cudaStream_t st = c->stream;

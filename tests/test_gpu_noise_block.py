@@ -17,7 +17,10 @@ so a run with blocks must reproduce the per-step run:
   block solves is the count of those cut points);
 * at the default tolerance 1e-6 and FP32 grids, the per-right-hand-side
   Krylov dimensions stay those of the per-step solves (within the check
-  interval) and the displacements within the tolerance.
+  interval) and the displacements within the tolerance;
+* the block solve with its convergence checks and loop on the device (one
+  graph with a conditional while node) takes the Krylov dimensions of the
+  host-checked loop and the same displacements to 1e-10.
 """
 import numpy as np
 import pytest
@@ -28,7 +31,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _run(nb, *, flow=1, steps=12, srpy=5, precond="none", noise="philox", hop="parallel",
-         with_hop=False, tol=1e-10, precision="fp64", charges=False, MStep=4, t0=0):
+         with_hop=False, tol=1e-10, precision="fp64", charges=False, MStep=4, t0=0,
+         device=True):
     Nb, Nc, L = 25, 20, 30.0
     x, y, z = B.random_chains(Nb, Nc, L, 3, bond=2.0, min_sep=2.0)
     x, y = B.lab_frame(flow, x, y)
@@ -40,6 +44,7 @@ def _run(nb, *, flow=1, steps=12, srpy=5, precond="none", noise="philox", hop="p
     c = B.Context(B.make_params(flow, Nb, Nc, L, 0.05, 5e-4, mobility="pme", noise=noise,
                                 precision=precision, shear_kappas_override=1, srpy=srpy,
                                 MStep=MStep, hop=hop, lanczos_tol=tol, noise_block=nb, **kw))
+    c.set_device_krylov(device)
     c.set_positions(x, y, z)
     if track is not None:
         c.set_charges(track)
@@ -80,6 +85,25 @@ def test_block_matches_per_step(flow, precond):
     assert ls1["maxed"] == 0
     if precond != "none":
         assert blk[0].precond_stats()["fallbacks"] == 0
+
+
+@pytest.mark.parametrize("precond,precision,tol", [("none", "fp64", 1e-10),
+                                                    ("segment", "fp64", 1e-6),
+                                                    ("segment", "fp32", 1e-6)])
+def test_device_checked_loop_matches_host_checks(precond, precision, tol):
+    """The whole block solve as one graph with the convergence checks on the
+    device (quadrature square root of the tridiagonal) against the host's
+    checks (implicit QR), one iteration behind: the same Krylov dimensions and
+    displacements to 1e-10 of the total."""
+    dev = _run(8, precond=precond, precision=precision, tol=tol, device=True)
+    host = _run(8, precond=precond, precision=precision, tol=tol, device=False)
+    _compare(host, dev, 1e-10)
+    sd, sh = dev[0].lanczos_stats(), host[0].lanczos_stats()
+    assert sd["iterations"] == sh["iterations"] and sd["calls"] == sh["calls"], (sd, sh)
+    assert dev[0].noise_block_stats() == host[0].noise_block_stats()
+    kd, kh = dev[0].krylov_check_stats(), host[0].krylov_check_stats()
+    assert kd["device_solves"] == dev[0].noise_block_stats()["blocks"] and kd["host_fallbacks"] == 0
+    assert kh["device_solves"] == 0
 
 
 def test_block_capacity_and_start_time():
