@@ -365,14 +365,18 @@ def c2_replicas(seed=20261203, n=64):
 SEGMENT = [10]  # beads per preconditioner segment (--segment)
 
 
-def build_context(w, seed, path="lanczos32", device_noise="philox", **extra):
+def build_context(w, seed, path="lanczos32", device_noise="philox", noise_seed=None, **extra):
+    """A context on w's seeded synthetic configuration (seed), stepping path;
+    the noise stream is keyed by noise_seed (default: seed)."""
     import bd_b200 as B
     edot = edot_of(w)
     x, y, z, q, beta, C = synth_inputs(w, seed)
     pp = PATHS[path]
     north = pp.get("physics") == "north"
     p = B.make_params(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
-                      noise=device_noise, philox_seed=seed, mobility=pp["mobility"],
+                      noise=device_noise,
+                      philox_seed=seed if noise_seed is None else noise_seed,
+                      mobility=pp["mobility"],
                       precision=pp["precision"], lanczos_tol=1e-6,
                       coulomb="ewald" if north else "dh",
                       hop="parallel" if north else "sequential",
@@ -667,18 +671,26 @@ def run_batch(args, world):
 
 def accuracy_vs_fp64(w, path, noise_block, pme_rc, pme_grid, seed=1000):
     """Per-result relative error (2-norm over all beads) of the measured path
-    against the plain FP64 path (pme64: FP64 grids, transforms and pair
-    tensors, no preconditioner) on the same configuration at the bench's
-    discretisation: the forces, the mobility product M F, and the Brownian
-    displacement sqrt(M) z for one seeded z (each solve at tolerance 1e-6).
-    The FP64 path is itself checked against the CPU oracle's dense Ewald sum
-    at sizes the oracle can hold (the particle-mesh tests)."""
+    against FP64 on the same configuration at the bench's discretisation:
+    the forces and the mobility product M F against pme64; the Brownian
+    displacement for one seeded z (each solve at tolerance 1e-6) against
+    pme64 computing the same square-root factor, i.e. with the path's own
+    preconditioner G (a preconditioned solve returns G^-1 sqrt(G M G^T) z,
+    another valid factor than sqrt(M) z), and the plain FP32 sqrt(M) z
+    (pme32) against plain pme64.  The FP64 path is itself checked against the
+    CPU oracle's dense Ewald sum at sizes the oracle can hold (the
+    particle-mesh tests)."""
     N = w["Nb"] * w["Nc"]
     z = np.random.default_rng(seed).normal(size=3 * N)
-    res = {}
-    for name in (path, "pme64"):
+    pre = PATHS[path].get("precond")
+
+    def run(name, precond_from=None):
         c = build_context(w, seed, name, noise_block=noise_block if name == path else 1,
                           pme_rc=pme_rc, pme_grid=pme_grid)
+        if precond_from is not None:
+            if precond_from == "learned":
+                c.mpnn_set_params(np.load(os.path.join(PKG, "mpnn_params.npy")))
+            c.set_preconditioner(precond_from, SEGMENT[0] if w["Nb"] % SEGMENT[0] == 0 else 5)
         ext = w["flow"] == 1
         # the step's order: forces and the mobility build in the flow frame,
         # the products after rotating back
@@ -697,16 +709,26 @@ def accuracy_vs_fp64(w, path, noise_block, pme_rc, pme_grid, seed=1000):
         f = np.ascontiguousarray(F.T).reshape(-1)
         mf = c.mobility_apply(f)
         y, it = c.lanczos_sqrt(z)
-        res[name] = (F, mf, y, it)
         c.close()
-    a, b = res[path], res["pme64"]
+        return F, mf, y, it
+
     rel = lambda u, v: float(np.linalg.norm(u - v) / np.linalg.norm(v))
-    return {"against": "pme64 on the same configuration (FP64 storage, plain Lanczos)",
-            "forces": rel(a[0], b[0]), "mobility_product": rel(a[1], b[1]),
-            "displacement": rel(a[2], b[2]),
-            "krylov_iterations": {path: a[3], "pme64": b[3]}, "gate": 1e-5,
-            "note": "forces are FP64 in every path (springs, excluded volume, Ewald Coulomb); "
-                    "the displacement holds both solves' tolerance and the FP32 storage error"}
+    a = run(path)
+    b = run("pme64", pre)
+    out = {"against": "pme64 on the same configuration (FP64 storage)",
+           "forces": rel(a[0], b[0]), "mobility_product": rel(a[1], b[1]),
+           "displacement": rel(a[2], b[2]),
+           "displacement_against": "pme64 with the same preconditioner (the same factor)",
+           "krylov_iterations": {path: a[3], "pme64+" + str(pre): b[3]}, "gate": 1e-5,
+           "note": "forces are FP64 in every path (springs, excluded volume, Ewald Coulomb); "
+                   "a displacement error holds both solves' tolerance and the FP32 storage "
+                   "error"}
+    if pre is not None:
+        p32 = run("pme32")
+        p64 = run("pme64")
+        out["displacement_plain"] = rel(p32[2], p64[2])
+        out["krylov_iterations"].update({"pme32": p32[3], "pme64": p64[3]})
+    return out
 
 
 def run_ours(args, rank, world, dist):

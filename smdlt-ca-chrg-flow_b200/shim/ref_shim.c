@@ -10,7 +10,9 @@
  * streams (ran1/gasdev: getNoise, chargeHop, initChains), diagnostics and
  * file output stay as they are.  Each routine moves the globals it reads to
  * the device context, runs the device routine, and moves back what the
- * reference routine writes:
+ * reference routine writes (updateHI also loads the lookup table D and the
+ * CA-TEA parameters at an iteration's first step: the reference reads D in
+ * resetAverage at the end of iteration 0, main26.c:1840-1860):
  *
  *   applyPBC     shear/src/main26.c:1409   rx, ry, rz
  *   verletlist   shear/src/main26.c:682    list on the device; dxv reset
@@ -48,7 +50,7 @@ static void bd_fail(int s, const char *where) {
   } while (0)
 
 /* The context, created at the first replaced call (after Initialization()
- * has read the command line, Input.txt and the lookup table). */
+ * has read the command line and Input.txt). */
 static bd_ctx *ctx(void) {
   if (g_bd) return g_bd;
   bd_params q;
@@ -81,7 +83,6 @@ static bd_ctx *ctx(void) {
   q.mobility = BD_MOB_HYBRID;
   q.precision = BD_PREC_FP64;
   BD(bd_create(&q, &g_bd));
-  for (int nt = 0; nt < nt_avg; nt++) BD(bd_load_grid(g_bd, nt, D[nt]));
   g_old = malloc(sizeof(double) * 3 * (size_t)N);
   return g_bd;
 }
@@ -149,8 +150,10 @@ void updateFD(void) {
 
 void updateHI(void) {
   put_state();
-  if (t % srpy == 0 || t == tstart)  /* the CA-TEA parameters of the last iteration */
+  if (t == tstart) {  /* the lookup table and the last iteration's CA-TEA parameters */
+    for (int nt = 0; nt < nt_avg; nt++) BD(bd_load_grid(g_bd, nt, D[nt]));
     for (int b = 0; b <= sbins; b++) BD(bd_set_tea(g_bd, b, bp[b], C[b]));
+  }
   BD(bd_upload_forces(g_bd, fx, fy, fz));
   BD(bd_upload_noise(g_bd, R));
   BD(bd_upload_displacements(g_bd, dxv, dyv, dzv));
