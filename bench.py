@@ -74,6 +74,11 @@ WORKLOADS = {
     "c2": dict(name="64 replicas, 2k-20k beads each (chains 20-200 x 25-100), half shear half "
                     "KRBC, Wi uniform in [0.5, 5], 50% charged, hop/100 steps",
                flow=1, Nb=100, Nc=20, L=37.8, Wi=2.0, dt=5e-4, frac=0.5, ensemble=True),
+    # config 4: semidilute charged solution in shear, 256^3 grid (the cutoff
+    # that the grid rule pairs with it, 12.9 L / 256 = 8.82), hop every 50 steps
+    "c4": dict(name="shear LE 2000x100 beads (200000), box 175, Wi 10, 50% charged, hop/50 steps",
+               flow=0, Nb=100, Nc=2000, L=175.0, Wi=10.0, dt=5e-4, frac=0.5, pme_rc=8.82,
+               force=dict(MStep=50)),
     "c0": dict(name="shear LE 20x25 beads (500), box 30, Wi 1, 50% charged, hop/100 steps",
                flow=0, Nb=25, Nc=20, L=30.0, Wi=1.0, dt=5e-4, frac=0.5,
                force=dict(spring="Hookean", kappas=200.0, qmax=2.0, epsilon=0.1)),
@@ -497,7 +502,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
     c.profile(False)
     t_build = per["HI_BUILD"][0] / max(per["HI_BUILD"][1], 1)
     t_sweep = per["HOP"][0] / max(per["HOP"][1], 1)
-    srpy, mstep = COMMON["srpy"], COMMON["MStep"]
+    srpy, mstep = COMMON["srpy"], force_params(w)["MStep"]
 
     def amortise(ms, t_first, n):
         # remove the rebuilds and sweeps that fell in steps [t_first, t_first + n)
@@ -843,7 +848,7 @@ def main():
     ap.add_argument("--noise-block", type=int, default=8,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
-    ap.add_argument("--pme-rc", type=float, default=12.1,
+    ap.add_argument("--pme-rc", type=float, default=None,
                     help="particle-mesh real-space cutoff; the grid follows it (12.9 L / rc "
                          "points, constant interpolation accuracy)")
     ap.add_argument("--pme-grid", type=int, default=0,
@@ -858,6 +863,8 @@ def main():
     ap.add_argument("--errors", type=int, default=1,
                     help="per-result error of the path against pme64 at the bench config")
     args = ap.parse_args()
+    if args.pme_rc is None:
+        args.pme_rc = WORKLOADS[args.workload].get("pme_rc", 12.1)
     SEGMENT[0] = args.segment
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

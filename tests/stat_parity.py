@@ -37,7 +37,6 @@ from __future__ import annotations
 import argparse
 import json
 import math
-import multiprocessing as mp
 import os
 import sys
 import time
@@ -112,7 +111,8 @@ def run_gpu(workload, path, steps, every, noise_seed, config_seed=1000, noise_bl
     pp = bench.PATHS[path]
     extra = {}
     if pp["mobility"] == "pme":
-        extra = dict(noise_block=noise_block if path != "pme64" else 1, pme_rc=12.1)
+        extra = dict(noise_block=noise_block if path != "pme64" else 1,
+                     pme_rc=w.get("pme_rc", 12.1))
     if reference_step:
         c = bench.build_context(w, config_seed, path, device_noise="ran1", seed=noise_seed,
                                 **extra)
@@ -184,9 +184,12 @@ def _ref_worker(args):
 def run_reference_host(workload, steps, every, seed, config_seed=1000, threads=None):
     """The reference's own routines (oracle/_ref) on the host, in a fresh
     process (its generator and state are process-global)."""
+    import subprocess
     threads = threads or len(os.sched_getaffinity(0))
-    with mp.get_context("spawn").Pool(1) as pool:
-        return pool.apply(_ref_worker, ((workload, steps, every, seed, config_seed, threads),))
+    args = json.dumps([workload, steps, every, seed, config_seed, threads])
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-worker", args],
+                       capture_output=True, text=True, check=True)
+    return json.loads(r.stdout.strip().splitlines()[-1])
 
 
 def run_pair(pair, workload, steps, every):
@@ -206,7 +209,18 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--every", type=int, default=50)
     ap.add_argument("--out", default="")
+    ap.add_argument("--ref-worker", default="")
     args = ap.parse_args()
+    if args.ref_worker:
+        # the host reference run of run_reference_host, in this fresh process;
+        # the reference's own status lines go to stderr
+        saved = os.dup(1)
+        os.dup2(2, 1)
+        r = _ref_worker(tuple(json.loads(args.ref_worker)))
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        print(json.dumps(r))
+        return
     a, b, cmp_ = run_pair(args.pair, args.workload, args.steps, args.every)
     res = {"pair": args.pair, "workload": args.workload, "steps": args.steps,
            "every": args.every, "compare": cmp_,
