@@ -19,8 +19,8 @@ box of 60a at Wi = 2).  Inputs are seeded synthetic chains.  The default path
 smooth particle-mesh Ewald (FP32 grids, cutoff 12.1 with the grid from the
 library's rule) and the Brownian displacement sqrt(M) z by a preconditioned
 Lanczos solve at tolerance 1e-6 (learned bead blocks on 10-bead segment
-blocks), the displacements of 8 consecutive steps solved by one multi-vector
-Krylov run (noise blocks).  --compare 1 also times the plain FP64 method
+blocks), the displacements of 10 consecutive steps solved by one multi-vector
+Krylov run (noise blocks of 10 steps, which tile the rebuild period).  --compare 1 also times the plain FP64 method
 (pme64, no preconditioner) on the same grid, with one solve per step and with
 the same noise blocks; --errors 1 reports the per-result error of the path
 against pme64 on the same configuration.  The rebuild (every 100 steps) and
@@ -845,7 +845,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--path", choices=sorted(PATHS), default="pme32-learned")
-    ap.add_argument("--noise-block", type=int, default=8,
+    # 10 divides the rebuild period of 100 steps (a block never spans a
+    # rebuild), so every block is full; 8 would leave one of 4 per period
+    ap.add_argument("--noise-block", type=int, default=10,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
     ap.add_argument("--pme-rc", type=float, default=None,

@@ -116,7 +116,7 @@ struct bd_ctx {
   int *Bctl;           // device convergence check, k ints each: done, conv, neg, last
                        // checked dimension, consecutive changes known; then the first
                        // dimension to check
-  double *Bdh;         // the last four relative changes per right-hand side
+  double *Bdh;         // the last eight relative changes per right-hand side
   double *Bpsi;        // quadrature pivots of the device check (k L1 nodes)
   void *blk_while[4];  // whole noise-block solves as one graph (conditional while node),
   int blk_while_key[4];

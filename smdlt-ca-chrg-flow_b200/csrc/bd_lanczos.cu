@@ -10,9 +10,9 @@
 // sqrt(M) z ~= |z| V_m T_m^(1/2) e_1.  The relative change d_m of the iterate
 // between successive m (the quantity of Ando, Chow and Skolnick, J. Chem.
 // Phys. 137, 064106 (2012)) decays geometrically; the solve stops when the
-// tail it implies, d_m rho / (1 - rho) with rho the largest of the last three
-// ratios d_j / d_(j-1), is below the tolerance, an estimate of the error of
-// the iterate itself rather than of its last change.  T_m^(1/2) e_1 comes
+// tail it implies, d_m rho / (1 - rho) with rho = (d_m / d_(m-6))^(1/6) the
+// mean decay of the last six changes, is below the tolerance, an estimate of
+// the error of the iterate itself rather than of its last change.  T_m^(1/2) e_1 comes
 // from an eigen-decomposition of T_m on the host by the implicit symmetric QR
 // iteration with Wilkinson shifts (Golub and Van Loan, Matrix Computations,
 // section 8.3).  Vectors live on the device in component-major SoA with the
@@ -332,10 +332,10 @@ struct BlkCheck {
   int* conv;
   int* neg;
   int* last;            // dimension of the coefficients in c (-1: none)
-  int* nd;              // consecutive relative changes known (up to 4)
+  int* nd;              // consecutive relative changes known (up to 7)
   const int* first;     // first dimension to check
   int* mr;              // Krylov dimension used per right-hand side
-  double* dh;           // 4 per right-hand side, ring indexed by dimension % 4
+  double* dh;           // 8 per right-hand side, ring indexed by dimension % 8
   double* c;            // coefficients, L1 per right-hand side
   double* psi;          // k x L1 x kQuadNodes scratch
 };
@@ -378,9 +378,9 @@ __device__ void quad_sqrt_e1(const double* a, const double* b, int mm, double* c
 // After an iteration: for every open right-hand side at or past the first
 // checked dimension, the coefficients c_m = T_m^(1/2) e_1, the relative
 // change against c_(m-1) (the previous check's, or solved here at a first
-// check, with those of m-2 .. m-4), and the host path's stopping test (tail
-// d_m rho/(1-rho) <= tol, rho the largest of the last three ratios, capped at
-// 0.99; or a breakdown beta_(m-1) <= 1e-300; or the Krylov cap).
+// check, with those of m-2 .. m-7), and the host path's stopping test (tail
+// d_m rho/(1-rho) <= tol, rho = (d_m/d_(m-6))^(1/6) capped at 0.99; or a
+// breakdown beta_(m-1) <= 1e-300; or the Krylov cap).
 __global__ void __launch_bounds__(kQuadNodes) k_block_check(BlkCheck q) {
   extern __shared__ double sh[];
   int r = blockIdx.x, t = threadIdx.x, L1 = q.L1;
@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(kQuadNodes) k_block_check(BlkCheck q) {
   __syncthreads();
   double* crow = q.c + (size_t)r * L1;
   double* psi_row = q.psi + (size_t)r * L1 * kQuadNodes;
-  int mm0 = q.last[r] == m - 1 ? m : max(1, m - 4);
+  int mm0 = q.last[r] == m - 1 ? m : max(1, m - 7);
   if (mm0 < m && t == 0) q.nd[r] = 0;
   for (int mm = mm0; mm <= m; mm++) {
     quad_sqrt_e1(a, b, mm, cm, psi_row, &bad);
@@ -427,8 +427,8 @@ __global__ void __launch_bounds__(kQuadNodes) k_block_check(BlkCheck q) {
         Cn += red[2 * w + 1];
       }
       if (have_prev) {
-        q.dh[4 * r + (mm & 3)] = Cn > 0 ? sqrt(D / Cn) : 0.0;
-        q.nd[r] = min(q.nd[r] + 1, 4);
+        q.dh[8 * r + (mm & 7)] = Cn > 0 ? sqrt(D / Cn) : 0.0;
+        q.nd[r] = min(q.nd[r] + 1, 7);
       }
     }
     __syncthreads();  // every thread has read crow and last before they change
@@ -439,14 +439,11 @@ __global__ void __launch_bounds__(kQuadNodes) k_block_check(BlkCheck q) {
   if (t == 0) {
     if (bad) q.neg[r] = 1;
     bool ok = false;
-    if (q.nd[r] >= 4) {
-      double rho = 0.0;
-      for (int j = m - 2; j <= m; j++) {
-        double d1 = q.dh[4 * r + (j & 3)], d0 = q.dh[4 * r + ((j - 1) & 3)];
-        rho = fmax(rho, d0 > 0 ? d1 / d0 : 0.0);
-      }
+    if (q.nd[r] >= 7) {
+      double d1 = q.dh[8 * r + (m & 7)], d0 = q.dh[8 * r + ((m - 6) & 7)];
+      double rho = d0 > 0 ? pow(d1 / d0, 1.0 / 6.0) : 0.0;
       rho = fmin(rho, 0.99);
-      ok = q.dh[4 * r + (m & 3)] * rho / (1.0 - rho) <= q.tol;
+      ok = d1 * rho / (1.0 - rho) <= q.tol;
     }
     ok = ok || b[m - 1] <= 1e-300;
     if (ok || m >= q.lmax || bad) {
@@ -627,18 +624,17 @@ static double rel_change(const std::vector<double>& cm, const std::vector<double
   return cn > 0 ? sqrt(dn / cn) : 0.0;
 }
 
-// Stopping test at dimension m from the changes dh[m-3 .. m] (negative where
+// Stopping test at dimension m from the changes dh[m-6 .. m] (negative where
 // unknown): with the changes decaying at rate rho the error left in the
-// iterate is the geometric tail d_m rho / (1 - rho).  rho is the largest of
-// the last three ratios d_j / d_(j-1), capped at 0.99, so one fast step does
-// not end the solve; the cap makes d_m <= tol / 99 sufficient on its own.
+// iterate is the geometric tail d_m rho / (1 - rho).  rho is the mean decay
+// over the last six changes, (d_m / d_(m-6))^(1/6) (steadier than one ratio,
+// which the rounding of FP32 products makes noisy near convergence), capped
+// at 0.99, so that d_m <= tol / 99 is sufficient on its own.
+constexpr int kTailSpan = 6;
 static bool tail_converged(const std::vector<double>& dh, int m, double tol) {
-  if (m < 4 || (int)dh.size() <= m) return false;
-  double rho = 0;
-  for (int j = m - 2; j <= m; j++) {
-    if (dh[j] < 0 || dh[j - 1] < 0) return false;
-    rho = std::max(rho, dh[j - 1] > 0 ? dh[j] / dh[j - 1] : 0.0);
-  }
+  if (m <= kTailSpan + 1 || (int)dh.size() <= m) return false;
+  if (dh[m] < 0 || dh[m - kTailSpan] < 0) return false;
+  double rho = dh[m - kTailSpan] > 0 ? pow(dh[m] / dh[m - kTailSpan], 1.0 / kTailSpan) : 0.0;
   rho = std::min(rho, 0.99);
   return dh[m] * rho / (1.0 - rho) <= tol;
 }
@@ -780,13 +776,13 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
   // alpha_j, beta_j stay on the device (Lh, Lsc + 8); the host reads them
   // only at checkpoints: from two before the previous call's Krylov
   // dimension on, every second iteration.  Each check needs the changes at
-  // the last four dimensions: the coefficients of the dimensions it lacks
+  // the last seven dimensions: the coefficients of the dimensions it lacks
   // are solved for (cs: the last few, by dimension), the previous check's
   // reused.
   double* d_alpha = c->Lh;
   double* d_beta = c->Lsc + 8;
   int& last = pre ? c->pre_last : c->lan_last;
-  int next_check = std::max(5, last - 2);
+  int next_check = std::max(kTailSpan + 2, last - 2);
   std::vector<double> dh;
   std::vector<std::vector<double>> cs;
   std::vector<int> cs_m;
@@ -816,14 +812,14 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
     CU(cudaStreamSynchronize(st));
     // keep only the coefficients that later checks can reuse
     for (size_t i = 0; i < cs_m.size();)
-      if (cs_m[i] < m - 4) {
+      if (cs_m[i] < m - kTailSpan - 1) {
         cs.erase(cs.begin() + i);
         cs_m.erase(cs_m.begin() + i);
       } else {
         i++;
       }
     dh.resize(m + 1, -1.0);
-    for (int mm = std::max(2, m - 3); mm <= m; mm++)
+    for (int mm = std::max(2, m - kTailSpan); mm <= m; mm++)
       if (dh[mm] < 0) dh[mm] = rel_change(coeffs(mm), coeffs(mm - 1));
     cc = coeffs(m);
     if (tail_converged(dh, m, c->ltol) || beta[m - 1] <= 1e-300) {
@@ -893,9 +889,9 @@ static int alloc_blocks(bd_ctx* c) {
   CU(cudaMalloc(&c->Bm, 4 * (size_t)k));
   CU(cudaMalloc(&c->Bjd, 16));
   CU(cudaMalloc(&c->Bctl, 4 * (size_t)(5 * k + 4)));
-  CU(cudaMalloc(&c->Bdh, 8 * 4 * (size_t)k));
+  CU(cudaMalloc(&c->Bdh, 8 * 8 * (size_t)k));
   CU(cudaMalloc(&c->Bpsi, 8 * (size_t)k * L1 * kQuadNodes));
-  c->bytes += 4 * (size_t)(5 * k + 4) + 32 * (size_t)k + 8 * (size_t)k * L1 * kQuadNodes;
+  c->bytes += 4 * (size_t)(5 * k + 4) + 64 * (size_t)k + 8 * (size_t)k * L1 * kQuadNodes;
   if (!c->Bhost) return BD_ERR_STATE;  // pinned at bd_create (see there)
   CU(cudaMalloc(&c->Brng, sizeof(Ran1) * (size_t)(k + 1)));
   cudaEvent_t ev;
@@ -1174,7 +1170,7 @@ static int lanczos_run_multi_device(bd_ctx* c, int k, bool pre, double* out,
   CU(cudaMemsetAsync(c->Bctl, 0, 4 * 3 * (size_t)k, st));             // done, conv, neg
   CU(cudaMemsetAsync(c->Bctl + 3 * k, 0xff, 4 * (size_t)k, st));      // last = -1
   CU(cudaMemsetAsync(c->Bctl + 4 * k, 0, 4 * (size_t)k, st));         // nd
-  k_set_int<<<1, 32, 0, st>>>(c->Bctl + 5 * k, std::max(5, c->blk_last - 2));
+  k_set_int<<<1, 32, 0, st>>>(c->Bctl + 5 * k, std::max(kTailSpan + 2, c->blk_last - 2));
   if ((s = launch_ok(c)) != BD_OK) return s;
   CU(cudaGraphLaunch(ex, st));
   k_combo_m<<<dim3(blk, k), 256, 0, st>>>(c->BV, n * k, c->Bc, L1, c->Bm, c->Bsc, out, (int)n);
@@ -1256,7 +1252,7 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
   mr.assign(k, 0);
   conv.assign(k, 0);
   int ndone = 0, pending = 0, m = 0;
-  int next_check = std::max(5, c->blk_last - 2);
+  int next_check = std::max(kTailSpan + 2, c->blk_last - 2);
   const double* ha = c->Bhost;
   const double* hb = c->Bhost + (size_t)L1 * k;
   // convergence of every open right-hand side at Krylov dimension mm, from the
@@ -1286,11 +1282,11 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
       if (mlast[r] == mm - 1) {
         cprev.swap(clast[r]);
       } else {
-        // first check: the changes at mm - 1 .. mm - 3 as well
+        // first check: the changes at mm - 1 .. mm - 6 as well
         std::vector<double> ca, cb;
         sqrt_e1(alpha, beta, mm - 1, cprev, 0.5);
         ca = cprev;
-        for (int j = mm - 1; j >= std::max(2, mm - 3); j--) {
+        for (int j = mm - 1; j >= std::max(2, mm - kTailSpan); j--) {
           sqrt_e1(alpha, beta, j - 1, cb, 0.5);
           d[j] = rel_change(ca, cb);
           ca.swap(cb);

@@ -102,7 +102,7 @@ def compare(a, b):
     return out
 
 
-def run_gpu(workload, path, steps, every, noise_seed, config_seed=1000, noise_block=8,
+def run_gpu(workload, path, steps, every, noise_seed, config_seed=1000, noise_block=10,
             reference_step=False):
     """One GPU run of `path` (bench.PATHS) from the seeded configuration."""
     import bench
