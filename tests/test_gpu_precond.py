@@ -180,44 +180,69 @@ def test_learned_on_segment_blocks():
 
 
 def test_training_and_iteration_gain():
-    """Trains on four 500-bead configurations (shear and extension), then
-    compares Krylov iterations with and without the network on held-out
-    configurations; the gain of per-bead blocks is small (the diagonal
-    blocks of M^-1/2 vary little between beads), so the bound is that the
-    learned blocks never cost more than one extra iteration, with no
-    fallback, and that the loss falls."""
+    """Trains the network on top of 5-bead segment blocks (the production
+    arrangement) on four 500-bead extensional configurations, then on two
+    held-out configurations: the loss of the trained network is below 0.9 of
+    the untrained one's (it learned something that generalises), and the
+    learned blocks never cost Krylov iterations against segment blocks alone,
+    with no fallback.  The gain itself is small (measured and printed): the
+    diagonal blocks of (G M G^T)^-1/2 vary little between beads; the
+    leverage is in the coupling between segments (the design notes give the
+    measurement)."""
     Nb, Nc, L = 25, 20, 30.0
     c, o, _ = _system(1, 0, Nb=Nb, Nc=Nc, L=L)
-    c.mpnn_set_params(B.mpnn_init(11))
-    configs = []
-    for s in range(4):
-        x, y, z = B.random_chains(Nb, Nc, L, 100 + s, bond=2.0, min_sep=2.0)
+    w0 = B.mpnn_init(11)
+    c.mpnn_set_params(w0)
+    c.set_preconditioner("segment", 5)
+
+    def placed(seed):
+        x, y, z = B.random_chains(Nb, Nc, L, seed, bond=2.0, min_sep=2.0)
         x, y = B.lab_frame(1, x, y)
         o.lattice(0)
         o.rotate(x, y, 0)
         o.apply_pbc(x, y, z)
-        configs.append((x, y, z, 0))
+        return x, y, z
+
+    configs = [(*placed(100 + s), 0) for s in range(4)]
     losses = B.train_preconditioner(c, configs, steps_per_config=40, lr=3e-3, seed=1)
     assert np.mean(losses[-20:]) < 0.8 * np.mean(losses[:5])
+    w1 = c.mpnn_params()
+
+    def held_out_loss(params, x, y, z, seed):
+        c.mpnn_set_params(params)
+        c.set_positions(x, y, z)
+        c.set_time(0, 0)
+        c.update_lattice(0)
+        c.build_neighbors()
+        c.set_preconditioner("segment", 5)
+        c.calc_hi()
+        c.mpnn_features()
+        r = np.random.default_rng(seed)
+        out = []
+        for _ in range(4):
+            zz = r.normal(size=3 * o.N)
+            tgt, _ = c.lanczos_inv_sqrt(zz)
+            out.append(c.mpnn_loss_grad(zz, tgt))
+        return np.mean(out)
+
     gains = []
     for s in range(2):
-        x, y, z = B.random_chains(Nb, Nc, L, 200 + s, bond=2.0, min_sep=2.0)
-        x, y = B.lab_frame(1, x, y)
-        o.rotate(x, y, 0)
-        o.apply_pbc(x, y, z)
-        c.set_positions(x, y, z)
-        c.build_neighbors()
-        c.set_preconditioner("none")
-        c.calc_hi()
+        x, y, z = placed(200 + s)
+        l_untrained = held_out_loss(w0, x, y, z, 400 + s)
+        l_trained = held_out_loss(w1, x, y, z, 400 + s)
+        assert l_trained < 0.9 * l_untrained, (l_trained, l_untrained)
         zz = np.random.default_rng(300 + s).normal(size=3 * o.N)
-        _, it_plain = c.lanczos_sqrt(zz)
-        c.set_preconditioner("learned")
+        c.set_preconditioner("segment", 5)
+        c.calc_hi()
+        _, it_seg = c.lanczos_sqrt(zz)
+        c.set_preconditioner("learned", 5)
+        c.calc_hi()
         got, it_learned = c.lanczos_sqrt(zz)
-        gains.append((it_plain, it_learned))
-        Gd, Gi = c.precond_blocks(1)
+        gains.append((it_seg, it_learned, l_untrained, l_trained))
+        Gd, Gi = c.precond_blocks(5)
         M = O.full_mobility(o.calc_hi_ewald(x, y, z), o.N)
         ref = _reference_displacement(M, _block_diag(Gd), _block_diag(Gi), zz)
         assert rel_err(got, ref) < 1e-6, rel_err(got, ref)
-    print("plain vs learned Krylov iterations:", gains)
-    assert all(l <= p + 1 for p, l in gains)
+    print("segment vs learned-on-segment Krylov iterations, held-out losses:", gains)
+    assert all(l <= sg for sg, l, _, _ in gains)
     assert c.precond_stats()["fallbacks"] == 0
