@@ -2,7 +2,10 @@
  * GPU through the bd_b200 C ABI.
  *
  * A maintainer compiles this file next to the reference's own sources
- * (shear/src: main26.c, Parameters.h), against the reference's Parameters.h
+ * (shear/src: main26.c, Parameters.h; or extensional/src: main14.c, whose
+ * routines of the same names it replaces alike, the flow chosen by the tree's
+ * THETA0; compile it with -DREF_EXTENSIONAL there), against the tree's
+ * Parameters.h
  * so that every global below is the reference's own, and links it with
  * libbd_b200.so.  The routines defined here replace the reference's bodies of
  * the same names (its object is linked with those symbols weakened, see
@@ -124,7 +127,9 @@ static void force_call(int (*f)(bd_ctx *)) {
   BD(bd_download_stress(g_bd, tau));
   tauxx += tau[0];
   tauyy += tau[1];
-  tauxy += tau[2];
+#ifndef REF_EXTENSIONAL
+  tauxy += tau[2];  /* the extensional tree keeps only tauxx, tauyy */
+#endif
 }
 
 void bondforce(void) { force_call(bd_bond_force); }
@@ -164,15 +169,27 @@ void updateHI(void) {
   BD(bd_download_positions(g_bd, rx, ry, rz));
   BD(bd_download_displacements(g_bd, dxv, dyv, dzv));
   /* the charges' displacement log, as the reference's updateHI writes it:
-   * the hydrodynamic displacement (the step without its flow term
-   * dt flowrate y) plus the flow relative to the chain's centre of mass */
+   * the hydrodynamic displacement (the step without its flow term: shear
+   * dt flowrate (y, 0, 0), main26.c:845; planar extension
+   * dt flowrate (x, -y, 0), extensional/src/main14.c:883-884) plus the flow
+   * relative to the chain's centre of mass */
   tcount++;
   for (int i = 0; i < Ncharges; i++) {
     int j = Charge_track[i];
     int chain = (int)floor(j / Nb);
-    double dxh = (rx[j] - g_old[j]) - dt * flowrate * g_old[N + j];
-    dxt[i * printprops + tcount] = dxh + dt * flowrate * (comy[chain] - py[j]);
-    dyt[i * printprops + tcount] = ry[j] - g_old[N + j];
+    double x0 = g_old[j], y0 = g_old[N + j];
+    double dxh, dyh;
+    if (THETA0 == 0) {
+      dxh = (rx[j] - x0) - dt * flowrate * y0;
+      dyh = ry[j] - y0;
+      dxt[i * printprops + tcount] = dxh + dt * flowrate * (comy[chain] - py[j]);
+      dyt[i * printprops + tcount] = dyh;
+    } else {
+      dxh = (rx[j] - x0) - dt * flowrate * x0;
+      dyh = (ry[j] - y0) + dt * flowrate * y0;
+      dxt[i * printprops + tcount] = dxh + dt * flowrate * (comx[chain] - px[j]);
+      dyt[i * printprops + tcount] = dyh - dt * flowrate * (comy[chain] - py[j]);
+    }
     dzt[i * printprops + tcount] = rz[j] - g_old[2 * N + j];
   }
 }

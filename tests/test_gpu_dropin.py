@@ -1,11 +1,12 @@
 """The drop-in adapter inside the reference's own simulator.
 
-oracle/Makefile's dropin target builds the reference's shear program twice
-from its unmodified sources (shear/src/main26.c, gridHI.c): as it is
-(oracle/_ref/run_shear), and with its hot step-loop routines (applyPBC,
+oracle/Makefile's dropin target builds each of the reference's programs
+(shear: shear/src/main26.c; planar extension: extensional/src/main14.c; each
+with its gridHI.c) twice from the unmodified sources: as it is
+(oracle/_ref/run_<tree>), and with its hot step-loop routines (applyPBC,
 verletlist, checkVerlet, bondforce, LJforce, coulombForce, updateFD,
 updateHI) replaced at link time by smdlt-ca-chrg-flow_b200/shim/ref_shim.c on
-libbd_b200.so (oracle/_ref/dropin_shear).  Both run the reference's own
+libbd_b200.so (oracle/_ref/dropin_<tree>).  Both run the reference's own
 main(): command line, Input.txt, the lookup table written by its gridHI
 program, iteration 0 (free-draining steps with CA-TEA sampling) and iteration
 1 (hydrodynamic steps with charge hopping every 5 steps and a mobility
@@ -50,13 +51,13 @@ RUN = ["-d", "0.0005", "-t", "120", "-n", "1", "-r", "0", "-i", "0", "-m", "2", 
 NUM = re.compile(r"^[-+]?(\d+\.?\d*|\.\d+)([eE][-+]?\d+)?$")
 
 
-def _run(exe, d):
+def _run(exe, d, tree="shear"):
     os.makedirs(d)
     for sub in ("prop", "mm", "txt", "xyz", "res", "decomp", "bin", "build"):
         os.makedirs(os.path.join(d, sub))
     with open(os.path.join(d, "Input.txt"), "w") as f:
         f.write(INPUT)
-    subprocess.run([os.path.join(REF, "grid_shear"), *SYS, "-n", "4"], cwd=d, check=True,
+    subprocess.run([os.path.join(REF, "grid_" + tree), *SYS, "-n", "4"], cwd=d, check=True,
                    capture_output=True, timeout=300)
     r = subprocess.run([os.path.join(REF, exe), *SYS, *RUN], cwd=d, capture_output=True,
                        text=True, timeout=600)
@@ -95,11 +96,12 @@ def _same(a, b):
     return True, worst
 
 
-def test_dropin_simulator_matches_reference(tmp_path):
-    for exe in ("run_shear", "grid_shear", "dropin_shear"):
-        assert os.path.exists(os.path.join(REF, exe)), f"{exe}: build with make -C oracle dropin"
-    ref = _run("run_shear", str(tmp_path / "ref"))
-    gpu = _run("dropin_shear", str(tmp_path / "gpu"))
+@pytest.mark.parametrize("tree", ["shear", "ext"])
+def test_dropin_simulator_matches_reference(tmp_path, tree):
+    for exe in ("run_", "grid_", "dropin_"):
+        assert os.path.exists(os.path.join(REF, exe + tree)), f"{exe}{tree}: make -C oracle dropin"
+    ref = _run("run_" + tree, str(tmp_path / "ref"), tree)
+    gpu = _run("dropin_" + tree, str(tmp_path / "gpu"), tree)
     assert sorted(ref) == sorted(gpu)
     compared = 0
     for name in ref:
