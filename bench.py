@@ -378,6 +378,10 @@ def build_context(w, seed, path="lanczos32", device_noise="philox", noise_seed=N
     x, y, z, q, beta, C = synth_inputs(w, seed)
     pp = PATHS[path]
     north = pp.get("physics") == "north"
+    if device_noise == "ran1" and noise_seed is not None:
+        extra.setdefault("seed", noise_seed)
+    if pp["mobility"] == "pme":
+        extra.setdefault("lanczos_max", 400)  # the plain method needs ~200 at 200 000 beads
     p = B.make_params(w["flow"], w["Nb"], w["Nc"], w["L"], edot, w["dt"], Ncharges=len(q),
                       noise=device_noise,
                       philox_seed=seed if noise_seed is None else noise_seed,

@@ -1191,27 +1191,23 @@ static int lanczos_run_multi_device(bd_ctx* c, int k, bool pre, double* out,
   }
   c->launches += per_iter * j;
   if (!negr.empty()) {
-    // a tridiagonal that is not positive definite: the host's QR square root
-    // (negative Ritz values clamped to zero), as the host-checked path does
+    // a tridiagonal that is not positive definite (an indefinite operator):
+    // the device stopped that right-hand side at its first non-positive
+    // pivot.  Preconditioned, it is reported unconverged (the caller re-solves
+    // it plainly); plain, it is re-solved by the host-checked single-vector
+    // Lanczos, which clamps negative Ritz values, into its output slot
     c->host_fallbacks++;
-    std::vector<double> ab(2 * (size_t)L1 * k);
-    CU(cudaMemcpyAsync(ab.data(), c->Bab, 8 * ab.size(), cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
     for (int r : negr) {
-      int mm = mr[r];
-      std::vector<double> alpha(mm), beta(mm), cm;
-      for (int i = 0; i < mm; i++) {
-        alpha[i] = ab[(size_t)i * k + r];
-        beta[i] = ab[(size_t)L1 * k + (size_t)i * k + r];
-      }
-      c->lan_negative += sqrt_e1(alpha, beta, mm, cm, 0.5);
       conv[r] = 0;
-      CU(cudaMemcpyAsync(c->Bc + (size_t)r * L1, cm.data(), 8 * (size_t)mm,
-                         cudaMemcpyHostToDevice, st));
+      if (pre) continue;
+      int m1 = 0;
+      bool cv = false;
+      if ((s = lanczos_run(c, c->BR + 3 * (size_t)N * r, false, false, 0.5, out + n * r, &m1,
+                           &cv)) != BD_OK)
+        return s;
+      mr[r] = m1;
+      conv[r] = cv;
     }
-    c->launches++;
-    k_combo_m<<<dim3(blk, k), 256, 0, st>>>(c->BV, n * k, c->Bc, L1, c->Bm, c->Bsc, out, (int)n);
-    CU(cudaStreamSynchronize(st));  // the host vectors above are read by the copies
   }
   int mmin = c->lmax;
   for (int r = 0; r < k; r++) mmin = std::min(mmin, mr[r]);

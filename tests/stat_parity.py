@@ -114,8 +114,8 @@ def run_gpu(workload, path, steps, every, noise_seed, config_seed=1000, noise_bl
         extra = dict(noise_block=noise_block if path != "pme64" else 1,
                      pme_rc=w.get("pme_rc", 12.1))
     if reference_step:
-        c = bench.build_context(w, config_seed, path, device_noise="ran1", seed=noise_seed,
-                                **extra)
+        c = bench.build_context(w, config_seed, path, device_noise="ran1",
+                                noise_seed=noise_seed, **extra)
     else:
         c = bench.build_context(w, config_seed, path, noise_seed=noise_seed, **extra)
     step = c.step_reference if pp["step"] == "reference" else c.step_lanczos

@@ -87,20 +87,25 @@ def test_block_matches_per_step(flow, precond):
         assert blk[0].precond_stats()["fallbacks"] == 0
 
 
-@pytest.mark.parametrize("precond,precision,tol", [("none", "fp64", 1e-10),
-                                                    ("segment", "fp64", 1e-6),
-                                                    ("segment", "fp32", 1e-6)])
-def test_device_checked_loop_matches_host_checks(precond, precision, tol):
+@pytest.mark.parametrize("precond,precision,tol,agree", [("none", "fp64", 1e-10, 1e-10),
+                                                          ("segment", "fp64", 1e-6, 1e-10),
+                                                          ("segment", "fp32", 1e-6, 1e-7)])
+def test_device_checked_loop_matches_host_checks(precond, precision, tol, agree):
     """The whole block solve as one graph with the convergence checks on the
     device (quadrature square root of the tridiagonal) against the host's
-    checks (implicit QR), one iteration behind: the same Krylov dimensions and
-    displacements to 1e-10 of the total."""
+    checks (implicit QR), one iteration behind: the same Krylov dimensions
+    and displacements to 1e-10 of the total (1e-7 with FP32 grids, whose
+    atomic spreading differs in rounding between any two runs).  The host
+    loop runs one more block iteration per block (the one it launches ahead
+    while checking), the device loop none."""
     dev = _run(8, precond=precond, precision=precision, tol=tol, device=True)
     host = _run(8, precond=precond, precision=precision, tol=tol, device=False)
-    _compare(host, dev, 1e-10)
+    _compare(host, dev, agree)
     sd, sh = dev[0].lanczos_stats(), host[0].lanczos_stats()
     assert sd["iterations"] == sh["iterations"] and sd["calls"] == sh["calls"], (sd, sh)
-    assert dev[0].noise_block_stats() == host[0].noise_block_stats()
+    bd, bh = dev[0].noise_block_stats(), host[0].noise_block_stats()
+    assert bd["blocks"] == bh["blocks"]
+    assert bh["iterations"] - bh["blocks"] <= bd["iterations"] <= bh["iterations"], (bd, bh)
     kd, kh = dev[0].krylov_check_stats(), host[0].krylov_check_stats()
     assert kd["device_solves"] == dev[0].noise_block_stats()["blocks"] and kd["host_fallbacks"] == 0
     assert kh["device_solves"] == 0
