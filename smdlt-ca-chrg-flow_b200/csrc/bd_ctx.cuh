@@ -197,6 +197,7 @@ struct bd_ctx {
   float *pme_vpk;    // FP32 block products: per packed pair and bead the pair's
                      // 6 input values (+2 padding), written by the spread
   void *rl_tt;       // per pair t1 and t2 / r^2 of the real-space tensor (FP64 or FP32)
+  double *pme_rsum;  // FP32 block products: real-space sums of every packed pair (6 per bead)
   double pme_cellbuf[19];  // its cell: H, H^-1, volume
   double pme_alpha_ref;    // calcHI's split parameter at that step
 

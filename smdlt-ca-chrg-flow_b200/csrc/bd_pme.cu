@@ -410,14 +410,14 @@ __device__ __forceinline__ void pair_terms(double alpha, double alpha_ref, doubl
 // row (pair terms, positions and minimum image once for the chunk), then a
 // butterfly reduction; lane e < 3 kc writes component e % 3 of right-hand
 // side r0 + e / 3.
-template <int P, typename R, int KG, bool PK>
+template <int P, typename R, int KG, bool PK, bool RS = false>
 __global__ void __launch_bounds__(256) k_pme_gather(
     const int* __restrict__ base, const double* __restrict__ w, int N, int K,
     const R* __restrict__ grid, int k, double self, const double* __restrict__ soff, VecIn v,
     size_t vr, const int* __restrict__ rcnt, const int* __restrict__ rrows,
     const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
     double* o0, double* o1, double* o2, int ostride, size_t orr,
-    const float* __restrict__ vpk) {
+    const float* __restrict__ vpk, const double* __restrict__ rsum) {
   constexpr int NA = 3 * KG;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
@@ -476,7 +476,10 @@ __global__ void __launch_bounds__(256) k_pme_gather(
   const double h00 = cell.H[0], h01 = cell.H[1], h10 = cell.H[3], h11 = cell.H[4];
   const double g00 = cell.Hi[0], g01 = cell.Hi[1], g10 = cell.Hi[3], g11 = cell.Hi[4];
   const double Lz = cell.H[8], iLz = cell.Hi[8];
-  if (PK && vpk) {
+  if constexpr (RS) {
+    // the real-space sums of this packed pair, formed for all pairs at once
+    // by k_pme_real_pairs (added below)
+  } else if (PK && vpk) {
     // packed pair: the neighbour's six values as two float4 stored by the
     // spread; two pairs per lane and iteration, so two independent chains
     // of loads (row entry, then position and values) are in flight
@@ -554,6 +557,8 @@ __global__ void __launch_bounds__(256) k_pme_gather(
 #pragma unroll
   for (int e = 0; e < NA; e++)
     if (e == lane) mine = u[e];
+  if constexpr (RS)
+    if (lane < nj) mine += rsum[((size_t)blockIdx.y * N + i) * 6 + lane];
   if (lane < nj) {
     int r = lane / 3, c = lane % 3;
     size_t o = (size_t)(r0 + r) * vr + (size_t)i * v.stride;
@@ -569,6 +574,67 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     double* dst = c == 0 ? o0 : (c == 1 ? o1 : o2);
     dst[(size_t)(r0 + r) * orr + (size_t)i * ostride] = out;
   }
+}
+
+// The real-space part of a block product in one pass over the pair rows,
+// for all NP packed pairs of right-hand sides at once (FP32 block products):
+// one warp per bead; a lane takes row entries, loads each entry (index, t1,
+// t2/r^2) and the neighbour's position once, forms the minimum-image
+// displacement once, and adds T_ij v_j for every packed pair (the six FP32
+// inputs the spread stored in vpk) into 6 NP FP64 accumulators.  The
+// interpolation then adds rsum[(p N + i) 6 + e] instead of walking the rows
+// again for each packed pair p.
+template <int NP>
+__global__ void __launch_bounds__(256) k_pme_real_pairs(
+    const int* __restrict__ rcnt, const int* __restrict__ rrows,
+    const double4* __restrict__ pos, Cell cell, const float* __restrict__ tt, int rcap,
+    const float* __restrict__ vpk, int N, double* __restrict__ rsum) {
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= N) return;
+  double u[6 * NP];
+#pragma unroll
+  for (int e = 0; e < 6 * NP; e++) u[e] = 0.0;
+  int n = rcnt[i];
+  const int* prow = rrows + (size_t)i * rcap;
+  const float* tr = tt + 2 * (size_t)i * rcap;
+  double4 pi = pos[i];
+  const double h00 = cell.H[0], h01 = cell.H[1], h10 = cell.H[3], h11 = cell.H[4];
+  const double g00 = cell.Hi[0], g01 = cell.Hi[1], g10 = cell.Hi[3], g11 = cell.Hi[4];
+  const double Lz = cell.H[8], iLz = cell.Hi[8];
+  for (int kk = lane; kk < n; kk += 32) {
+    int j = prow[kk];
+    double4 pj = pos[j];
+    double t1 = tr[2 * kk], t2r = tr[2 * kk + 1];
+    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
+    s0 -= rint(s0);
+    s1 -= rint(s1);
+    s2 -= rint(s2);
+    dx = h00 * s0 + h01 * s1;
+    dy = h10 * s0 + h11 * s1;
+    dz = Lz * s2;
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      const float4* vj = (const float4*)(vpk + ((size_t)p * N + j) * 8);
+      float4 a = vj[0], b = vj[1];
+      double qa = t2r * (dx * a.x + dy * a.y + dz * a.z);
+      double qb = t2r * (dx * a.w + dy * b.x + dz * b.y);
+      u[6 * p] += t1 * a.x + qa * dx;
+      u[6 * p + 1] += t1 * a.y + qa * dy;
+      u[6 * p + 2] += t1 * a.z + qa * dz;
+      u[6 * p + 3] += t1 * a.w + qb * dx;
+      u[6 * p + 4] += t1 * b.x + qb * dy;
+      u[6 * p + 5] += t1 * b.y + qb * dz;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 6 * NP; e++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) u[e] += __shfl_xor_sync(0xffffffffu, u[e], o);
+  }
+#pragma unroll
+  for (int e = 0; e < 6 * NP; e++)
+    if (e == lane) rsum[((size_t)(e / 6) * N + i) * 6 + e % 6] = u[e];
 }
 
 // Cells of the real-space list (fractional, width >= rc).
@@ -719,7 +785,8 @@ int pme_alloc(bd_ctx* c) {
   CU(cudaMalloc(&c->rl_pos, 32 * (size_t)N));
   if (c->pme_f32 && nr > 1) {
     CU(cudaMalloc(&c->pme_vpk, 32 * (size_t)N * ((nr + 1) / 2)));
-    c->bytes += 32 * (size_t)N * ((nr + 1) / 2);
+    CU(cudaMalloc(&c->pme_rsum, 48 * (size_t)N * ((nr + 1) / 2)));
+    c->bytes += 80 * (size_t)N * ((nr + 1) / 2);
   }
   CU(cudaMalloc(&c->rl_tt, 2 * es * (size_t)N * c->rl_cap));
   c->rl_ncell_cap = 4096;
@@ -790,7 +857,7 @@ void pme_free(bd_ctx* c) {
       cufftDestroy((cufftHandle)c->pme_mplan_f[q]);
       c->pme_mplan_k[q] = 0;
     }
-  void* ptrs[] = {c->pme_vpk, c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
+  void* ptrs[] = {c->pme_vpk, c->pme_rsum, c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
                   c->rl_cnt, c->rl_rows, c->rl_pos, c->rl_tt, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
                   c->rl_cell_start, c->rl_cursor};
   for (void* q : ptrs)
@@ -924,7 +991,7 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   k_pme_gather<P_, R, 1, false><<<nb8, 256, 0, c->stream>>>(                                  \
       c->pme_base, c->pme_w, N, K, grid, 1, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,       \
       c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
-      ostride, orr, nullptr)
+      ostride, orr, nullptr, nullptr)
     switch (p) {
       case 4: PME_GATHER(4); break;
       case 6: PME_GATHER(6); break;
@@ -963,15 +1030,47 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
     CF(cufftExecC2C(plan, (cufftComplex*)cg, (cufftComplex*)cg, CUFFT_INVERSE));
   else
     CF(cufftExecZ2Z(plan, (cufftDoubleComplex*)cg, (cufftDoubleComplex*)cg, CUFFT_INVERSE));
-#define PME_GATHER(P_)                                                                        \
-  k_pme_gather<P_, R, 2, true><<<gp, 256, 0, c->stream>>>(                                    \
+  // FP32: the real-space sums of all packed pairs in one pass over the rows
+  double* rsum = nullptr;
+  if constexpr (sizeof(R) == 4) {
+    if (vpk && c->pme_rsum && np <= 8) {
+      rsum = c->pme_rsum;
+      c->launches++;
+#define PME_REAL(NP_)                                                                          \
+  k_pme_real_pairs<NP_><<<nb8, 256, 0, c->stream>>>(c->rl_cnt, c->rl_rows,                     \
+                                                    (const double4*)c->rl_pos, cell,           \
+                                                    (const float*)c->rl_tt, c->rl_cap, vpk, N, \
+                                                    rsum)
+      switch (np) {
+        case 1: PME_REAL(1); break;
+        case 2: PME_REAL(2); break;
+        case 3: PME_REAL(3); break;
+        case 4: PME_REAL(4); break;
+        case 5: PME_REAL(5); break;
+        case 6: PME_REAL(6); break;
+        case 7: PME_REAL(7); break;
+        default: PME_REAL(8);
+      }
+#undef PME_REAL
+    }
+  }
+#define PME_GATHER(P_, RS_)                                                                   \
+  k_pme_gather<P_, R, 2, true, RS_><<<gp, 256, 0, c->stream>>>(                               \
       c->pme_base, c->pme_w, N, K, (const R*)cg, k, c->pme_self, c->pme_soff, v, vr,          \
       c->rl_cnt, c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap,  \
-      o0, o1, o2, ostride, orr, vpk)
-  switch (p) {
-    case 4: PME_GATHER(4); break;
-    case 6: PME_GATHER(6); break;
-    default: PME_GATHER(8);
+      o0, o1, o2, ostride, orr, vpk, rsum)
+  if (rsum) {
+    switch (p) {
+      case 4: PME_GATHER(4, true); break;
+      case 6: PME_GATHER(6, true); break;
+      default: PME_GATHER(8, true);
+    }
+  } else {
+    switch (p) {
+      case 4: PME_GATHER(4, false); break;
+      case 6: PME_GATHER(6, false); break;
+      default: PME_GATHER(8, false);
+    }
   }
 #undef PME_GATHER
   return BD_OK;
