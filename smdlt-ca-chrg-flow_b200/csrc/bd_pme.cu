@@ -79,13 +79,14 @@ __global__ void k_pme_weights(Cell cell, const double* __restrict__ rx,
 }
 
 // FP32 grids: the spread skips stencil points whose weight W_i(g) is below
-// 1e-10 (for order 8, 28 % of the 512 points, carrying at most 2.2e-9 of the
-// stencil's unit weight: below FP32 rounding, 6e-8, and three orders below
-// the particle-mesh error), saving their atomics; the interpolation keeps
-// every point (skipping there only added divergence), so the product is
-// symmetric to ~1e-9, inside the rounding of its FP32 grids.  The FP64 path
-// keeps every point.
-constexpr double kSkipWeight = 1e-10;
+// 1e-9 (for order 8, 35 % of the 512 points, carrying at most 2.7e-8 of the
+// stencil's unit weight, mean 1.4e-8: below FP32 rounding, 6e-8, and two
+// orders below the particle-mesh error), saving their atomics; the
+// interpolation keeps every point (skipping there only added divergence), so
+// the product is symmetric to ~3e-8, inside the rounding of its FP32 grids.
+// (1e-8 would skip 42 % but drop up to 3e-7 of the weight, the size of the
+// FP32 storage error itself.)  The FP64 path keeps every point.
+constexpr double kSkipWeight = 1e-9;
 
 // Q_r[c][g] += v_r,c(i) W_i(g) for the right-hand sides r0 .. r0 + kc - 1
 // of chunk blockIdx.y (r0 = KS blockIdx.y; KS = 1 for single products): one
