@@ -631,6 +631,13 @@ static double rel_change(const std::vector<double>& cm, const std::vector<double
 // which the rounding of FP32 products makes noisy near convergence), capped
 // at 0.99, so that d_m <= tol / 99 is sufficient on its own.
 constexpr int kTailSpan = 6;
+
+// The stopping tolerance of a solve: the context's for sqrt(M) z; half of it
+// for the preconditioned sqrt(G M G^T) z, whose error G^-1 carries into the
+// displacement amplified (by up to 1.6 measured with segment blocks), so that
+// the displacement itself stays within the tolerance.
+static double stop_tol(const bd_ctx* c, bool pre) { return pre ? 0.5 * c->ltol : c->ltol; }
+
 static bool tail_converged(const std::vector<double>& dh, int m, double tol) {
   if (m <= kTailSpan + 1 || (int)dh.size() <= m) return false;
   if (dh[m] < 0 || dh[m - kTailSpan] < 0) return false;
@@ -822,7 +829,7 @@ static int lanczos_run(bd_ctx* c, const double* z, bool with_force, bool pre, do
     for (int mm = std::max(2, m - kTailSpan); mm <= m; mm++)
       if (dh[mm] < 0) dh[mm] = rel_change(coeffs(mm), coeffs(mm - 1));
     cc = coeffs(m);
-    if (tail_converged(dh, m, c->ltol) || beta[m - 1] <= 1e-300) {
+    if (tail_converged(dh, m, stop_tol(c, pre)) || beta[m - 1] <= 1e-300) {
       conv = true;
       break;
     }
@@ -1049,7 +1056,7 @@ static void parallel_for(int n, F f) {
   HostPool::get().run(n, f);
 }
 
-static BlkCheck block_check_args(bd_ctx* c, int k) {
+static BlkCheck block_check_args(bd_ctx* c, int k, bool pre) {
   int L1 = c->lmax + 1;
   BlkCheck q;
   q.alpha = c->Bab;
@@ -1057,7 +1064,7 @@ static BlkCheck block_check_args(bd_ctx* c, int k) {
   q.k = k;
   q.L1 = L1;
   q.lmax = c->lmax;
-  q.tol = c->ltol;
+  q.tol = stop_tol(c, pre);
   q.jd = c->Bjd;
   q.done = c->Bctl;
   q.conv = c->Bctl + k;
@@ -1114,7 +1121,7 @@ static int block_while_graph(bd_ctx* c, int k, bool pre, cudaGraphExec_t* out) {
       s = block_part(c, k, pre, 0);
       if (s == BD_OK) s = block_part(c, k, pre, 1);
       if (s == BD_OK) {
-        BlkCheck q = block_check_args(c, k);
+        BlkCheck q = block_check_args(c, k, pre);
         size_t smem = 8 * (3 * (size_t)q.L1 + 16);
         if (smem > 48 * 1024)
           cudaFuncSetAttribute(k_block_check, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1289,7 +1296,7 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
         }
       }
       d[mm] = rel_change(cm, cprev);
-      bool ok = tail_converged(d, mm, c->ltol) || beta[mm - 1] <= 1e-300;
+      bool ok = tail_converged(d, mm, stop_tol(c, pre)) || beta[mm - 1] <= 1e-300;
       if (ok || mm >= c->lmax) {
         done[r] = 1;
         conv[r] = ok;

@@ -90,10 +90,35 @@ static bd_ctx *ctx(void) {
   return g_bd;
 }
 
+/* The device lattice is the one the reference computed last: its main calls
+ * updateLattice(t) in the step loop but updateLattice(tstart) before an
+ * iteration's first applyPBC, while the global t still holds the end of the
+ * previous iteration (applyPBC then takes delx from that t and the cell from
+ * tstart, main26.c:44-47, 1409-1428).  The device lattice of the candidate
+ * steps is compared with the reference's lattice globals (the same formula,
+ * so equal to the bit); the step the kernels see is t itself. */
+static unsigned long g_lat_t = 0;
+
 static void put_state(void) {
-  BD(bd_set_time(ctx(), t, tstart));
-  BD(bd_update_lattice(g_bd, t));
-  BD(bd_upload_positions(g_bd, rx, ry, rz));
+  bd_ctx *c = ctx();
+  unsigned long cand[4] = {g_lat_t, t, tstart, t > 0 ? t - 1 : 0};
+  int found = 0;
+  for (int k = 0; k < 4 && !found; k++) {
+    double lat[10];
+    BD(bd_update_lattice(c, cand[k]));
+    BD(bd_get_lattice(c, lat));
+    if (lat[4] == L1xp && lat[5] == L1yp && lat[6] == L2xp && lat[7] == L2yp) {
+      g_lat_t = cand[k];
+      found = 1;
+    }
+  }
+  if (!found) {
+    printf("bd_b200 adapter: the reference's lattice at step %lu is none of steps %lu, %lu\n", t,
+           t, tstart);
+    exit(1);
+  }
+  BD(bd_set_time(c, t, tstart));
+  BD(bd_upload_positions(c, rx, ry, rz));
 }
 
 void applyPBC(void) {
