@@ -22,7 +22,7 @@
  *   checkVerlet  shear/src/main26.c:858    dxv (reset when the list is rebuilt)
  *   bondforce    shear/src/main26.c:541    fx, fy, fz; tauxx, tauyy, tauxy
  *   LJforce      shear/src/main26.c:619    fx, fy, fz; tauxx, tauyy, tauxy
- *   coulombForce shear/src/main26.c:1891   fx, fy, fz (charges from Charge_track)
+ *   coulombForce shear/src/main26.c:1891   fx, fy, fz (charges from Charge_track); kappa_d
  *   updateFD     shear/src/main26.c:731    rx, ry, rz, dxv
  *   updateHI     shear/src/main26.c:745    rx, ry, rz, dxv; dxt/dyt/dzt and tcount
  *                                          (the charges' displacement log)
@@ -161,6 +161,9 @@ void bondforce(void) { force_call(bd_bond_force); }
 void LJforce(void) { force_call(bd_ev_force); }
 
 void coulombForce(void) {
+  /* the reference's coulombForce also sets the screening global that its
+   * chargeHop reads for the Metropolis energies (main26.c:1899, 1966, 2194) */
+  kappa_d = 1 / lambda_d;
   put_state();
   BD(bd_set_charges(g_bd, Charge_track, Ncharges));
   BD(bd_upload_forces(g_bd, fx, fy, fz));
