@@ -767,12 +767,37 @@ def accuracy_vs_fp64(w, path, noise_block, pme_rc, pme_grid, seed=1000):
     return out
 
 
+def tune_cutoff(w, path, noise_block, rank, dist):
+    """The particle-mesh cutoff (grid by the library's rule) whose product of
+    the noise block's right-hand sides is fastest on this GPU for the
+    workload's seeded configuration (bd_b200.autotune_pme_cutoff); rank 0
+    decides and the other ranks take its choice."""
+    import bd_b200 as B
+    choice = [None, None]
+    if rank == 0:
+        def make(rc):
+            c = build_context(w, 1000, path, noise_block=max(noise_block, 2), pme_rc=rc)
+            c.calc_hi()
+            return c
+        best, times = B.autotune_pme_cutoff(make, w["L"], max(noise_block, 2))
+        choice = [best, {str(k): round(v, 4) for k, v in times.items()}]
+    if dist is not None:
+        dist.broadcast_object_list(choice, src=0)
+    return choice[0], choice[1]
+
+
 def run_ours(args, rank, world, dist):
     w = WORKLOADS[args.workload]
     N = w["Nb"] * w["Nc"]
     K, W = args.steps, args.warmup
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    tuned = None
+    if args.pme_rc == "auto":
+        if PATHS[args.path]["mobility"] == "pme":
+            args.pme_rc, tuned = tune_cutoff(w, args.path, args.noise_block, rank, dist)
+        else:
+            args.pme_rc = 12.1
     main = measure(w, args.path, K, W, rank, dist, args.e2e_steps, args.noise_block, args.pme_rc,
                    args.pme_grid)
     value = world * N * K / (main["t_max_ms"] / 1e3)
@@ -810,6 +835,7 @@ def run_ours(args, rank, world, dist):
                                        __import__("bd_b200").pme_default_grid(w["L"], args.pme_rc),
                                        args.pme_rc) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
+                       "pme_cutoff_autotune_ms": tuned,
                        "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation" +
                                 (", noise blocks of %d steps" % main["block"]["noise_block"]
                                  if main["block"] else ""),
@@ -881,9 +907,11 @@ def main():
     ap.add_argument("--noise-block", type=int, default=10,
                     help="steps whose Brownian displacements one multi-vector Lanczos run "
                          "solves (particle-mesh paths; 1 = one solve per step)")
-    ap.add_argument("--pme-rc", type=float, default=None,
-                    help="particle-mesh real-space cutoff; the grid follows it (12.9 L / rc "
-                         "points, constant interpolation accuracy)")
+    ap.add_argument("--pme-rc", default=None,
+                    help="particle-mesh real-space cutoff, or 'auto' (the default where the "
+                         "workload fixes none): the fastest of bd_b200.PME_CUTOFFS for the "
+                         "product on this GPU; the grid follows it (12.9 L / rc points, "
+                         "constant interpolation accuracy)")
     ap.add_argument("--pme-grid", type=int, default=0,
                     help="particle-mesh grid points per cell edge (0: the library's rule "
                          "for the cutoff)")
@@ -897,7 +925,9 @@ def main():
                     help="per-result error of the path against pme64 at the bench config")
     args = ap.parse_args()
     if args.pme_rc is None:
-        args.pme_rc = WORKLOADS[args.workload].get("pme_rc", 12.1)
+        args.pme_rc = WORKLOADS[args.workload].get("pme_rc", "auto")
+    if args.pme_rc != "auto":
+        args.pme_rc = float(args.pme_rc)
     SEGMENT[0] = args.segment
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

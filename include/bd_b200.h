@@ -262,7 +262,8 @@ enum {
   BD_PROF_HOP = 2,      /* charge-hop sweep kernel */
   BD_PROF_FORCES = 3,   /* bond + excluded-volume + electrostatic kernels */
   BD_PROF_STEP = 4,     /* one whole bd_step_reference call */
-  BD_PROF_BLOCK = 5,    /* particle-mesh product of a noise block (all its right-hand sides) */
+  BD_PROF_BLOCK = 5,    /* particle-mesh product of a noise block or of
+                           bd_mobility_apply_block (all its right-hand sides) */
   BD_PROF_SLOTS = 8
 };
 /* Replay each Lanczos iteration (product and orthogonalisation) as a CUDA
@@ -304,8 +305,11 @@ int bd_mobility_apply(bd_ctx *ctx, const double *v, double *out);
  * in complex pairs; otherwise one product each. */
 int bd_mobility_apply_block(bd_ctx *ctx, int k, const double *v, double *out);
 /* out = sqrt(M) z by Lanczos with full FP64 reorthogonalisation, stopped when
- * the relative change between successive iterates is below lanczos_tol;
- * *iters receives the Krylov dimension used. */
+ * the geometric tail of the successive relative changes d_m, d_m rho / (1 -
+ * rho) with rho = (d_m / d_(m-6))^(1/6) capped at 0.99 (an estimate of the
+ * iterate's own error), is below lanczos_tol (half of it with a
+ * preconditioner, whose inverse factor amplifies the error); *iters receives
+ * the Krylov dimension used. */
 int bd_lanczos_sqrt(bd_ctx *ctx, const double *z, double *out, int *iters);
 /* calls, total Krylov iterations, calls that hit lanczos_max, negative Ritz
  * values clamped (a hybrid mobility need not be positive definite) */

@@ -328,6 +328,40 @@ def pme_default_grid(L, rc=None):
         K += 1
 
 
+PME_CUTOFFS = (10.0, 12.1, 13.6, 15.5, 17.5)
+
+
+def autotune_pme_cutoff(make_context, L, nrhs, candidates=PME_CUTOFFS, reps=4, seed=0):
+    """Picks the particle-mesh cutoff, and with it the real-space cells and
+    the grid (pme_default_grid: the accuracy rule fixes the grid spacing per
+    cutoff), whose product of nrhs right-hand sides is fastest on this GPU
+    for one configuration.  make_context(rc) returns a context with that
+    cutoff and its mobility prepared (bd_calc_hi); each candidate's product
+    is timed on the device (the BD_PROF_BLOCK events of
+    bd_mobility_apply_block) after one untimed call, and the context is
+    closed.  Candidates above 0.43 L (the minimum-image bound) are skipped.
+    Returns (best cutoff, {cutoff: ms per product})."""
+    times = {}
+    for rc in candidates:
+        if rc > 0.43 * L:
+            continue
+        c = make_context(rc)
+        try:
+            V = np.random.default_rng(seed).normal(size=(nrhs, 3 * c.N))
+            c.mobility_apply_block(V)  # plans and first-touch allocations
+            c.profile(True)
+            for _ in range(reps):
+                c.mobility_apply_block(V)
+            ms, n = c.profile_read(Context.PROF_BLOCK)
+            c.profile(False)
+            times[rc] = ms / max(n, 1)
+        finally:
+            c.close()
+    if not times:
+        raise ValueError("autotune_pme_cutoff: no candidate cutoff fits the box")
+    return min(times, key=times.get), times
+
+
 def make_params(flow, Nb, Nc, L, edot, dt, *, spring="FENE", kappas=30.0, qmax=3.0, kappab=0.0,
                 epsilon=1.0, lambda_b=2.0, lambda_d=5.0, Ncharges=0, barrier=3.0, barrier2=3.0,
                 MStep=100, nt_avg=8, bin_size=2.0, srpy=100, sbins=20, strain_ss=10.0,

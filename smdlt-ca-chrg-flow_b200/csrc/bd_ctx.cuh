@@ -193,11 +193,14 @@ struct bd_ctx {
   int pme_mplan_k[4], pme_mplan_f[4];  // packed-pair transforms for k right-hand sides
   int rl_cap, rl_ncell_cap;  // real-space pair rows
   int *rl_cnt, *rl_rows, *rl_cell_of, *rl_beads, *rl_cell_count, *rl_cell_start, *rl_cursor;
+  int *rl_need;      // longest pair row of the last build that overflowed the cap (0: none)
   void *rl_pos;      // lab-frame positions of the last preparation (double4)
   float *pme_vpk;    // FP32 block products: per packed pair and bead the pair's
                      // 6 input values (+2 padding), written by the spread
   void *rl_tt;       // per pair t1 and t2 / r^2 of the real-space tensor (FP64 or FP32)
   double *pme_rsum;  // FP32 block products: real-space sums of every packed pair (6 per bead)
+  float4 *rl_w;      // FP32 block products: per pair (t1, w), w = sqrt(|t2| / r^2) d, the sign
+                     // of t2 in the lowest mantissa bit of t1
   double pme_cellbuf[19];  // its cell: H, H^-1, volume
   double pme_alpha_ref;    // calcHI's split parameter at that step
 

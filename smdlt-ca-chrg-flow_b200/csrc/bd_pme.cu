@@ -169,8 +169,8 @@ struct Pair<double> {
 };
 
 // With vpk (FP32), lanes 0..7 of a bead's warp also store the pair's six
-// input values (plus two zeros) at vpk[(p N + i) 8], for the interpolation's
-// real-space part to read as two float4.
+// input values (plus two zeros) at vpk[(p N + i) 8], for the real-space sums
+// to read as a float4 and a float2.
 template <int P, typename R>
 __global__ void __launch_bounds__(256) k_pme_spread_pairs(const int* __restrict__ base,
                                                           const double* __restrict__ w, int N,
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(256) k_pme_gather(
     size_t vr, const int* __restrict__ rcnt, const int* __restrict__ rrows,
     const double4* __restrict__ pos, Cell cell, const R* __restrict__ tt, int rcap,
     double* o0, double* o1, double* o2, int ostride, size_t orr,
-    const float* __restrict__ vpk, const double* __restrict__ rsum) {
+    const double* __restrict__ rsum) {
   constexpr int NA = 3 * KG;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
@@ -480,47 +480,6 @@ __global__ void __launch_bounds__(256) k_pme_gather(
   if constexpr (RS) {
     // the real-space sums of this packed pair, formed for all pairs at once
     // by k_pme_real_pairs (added below)
-  } else if (PK && vpk) {
-    // packed pair: the neighbour's six values as two float4 stored by the
-    // spread; two pairs per lane and iteration, so two independent chains
-    // of loads (row entry, then position and values) are in flight
-    const float* vp = vpk + (size_t)blockIdx.y * N * 8;
-    const R* tr = tt + 2 * (size_t)i * rcap;
-    auto add = [&](double4 pj, double t1, double t2r, float4 a, float4 b) {
-      double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
-      s0 -= rint(s0);
-      s1 -= rint(s1);
-      s2 -= rint(s2);
-      dx = h00 * s0 + h01 * s1;
-      dy = h10 * s0 + h11 * s1;
-      dz = Lz * s2;
-      double qa = t2r * (dx * a.x + dy * a.y + dz * a.z);
-      u[0] += t1 * a.x + qa * dx;
-      u[1] += t1 * a.y + qa * dy;
-      u[2] += t1 * a.z + qa * dz;
-      double qb = t2r * (dx * a.w + dy * b.x + dz * b.y);
-      u[3] += t1 * a.w + qb * dx;
-      u[4] += t1 * b.x + qb * dy;
-      u[5] += t1 * b.y + qb * dz;
-    };
-    int kk = lane;
-    for (; kk + 32 < n; kk += 64) {
-      int ja = prow[kk], jb = prow[kk + 32];
-      double4 pa = pos[ja], pb = pos[jb];
-      const float4* va = (const float4*)(vp + (size_t)ja * 8);
-      const float4* vb = (const float4*)(vp + (size_t)jb * 8);
-      float4 a0 = va[0], a1 = va[1], b0 = vb[0], b1 = vb[1];
-      double t1a = tr[2 * kk], t2a = tr[2 * kk + 1];
-      double t1b = tr[2 * (kk + 32)], t2b = tr[2 * (kk + 32) + 1];
-      add(pa, t1a, t2a, a0, a1);
-      add(pb, t1b, t2b, b0, b1);
-    }
-    if (kk < n) {
-      int ja = prow[kk];
-      const float4* va = (const float4*)(vp + (size_t)ja * 8);
-      add(pos[ja], tr[2 * kk], tr[2 * kk + 1], va[0], va[1]);
-    }
   } else {
     for (int kk = lane; kk < n; kk += 32) {
       int j = prow[kk];
@@ -577,65 +536,79 @@ __global__ void __launch_bounds__(256) k_pme_gather(
   }
 }
 
-// The real-space part of a block product in one pass over the pair rows,
-// for all NP packed pairs of right-hand sides at once (FP32 block products):
-// one warp per bead; a lane takes row entries, loads each entry (index, t1,
-// t2/r^2) and the neighbour's position once, forms the minimum-image
-// displacement once, and adds T_ij v_j for every packed pair (the six FP32
-// inputs the spread stored in vpk) into 6 NP FP64 accumulators.  The
-// interpolation then adds rsum[(p N + i) 6 + e] instead of walking the rows
-// again for each packed pair p.
+// The real-space part of a block product (FP32 block products): for every
+// packed pair p and bead i, rsum[(p N + i) 6 + 3h + c] = sum_j (T_ij v_j)_c of
+// the pair's vector h (0: real part, 1: imaginary part), for NP pairs (at
+// most five) in one pass over the pair rows.  One warp per bead; a lane takes
+// row entries, each an index and the preparation's float4 (t1, w): T_ij =
+// t1 I + s w w^T, the sign s of t2 kept in the lowest mantissa bit of t1;
+// then it reads the neighbour's six inputs of every pair (the spread's
+// vpk[(p N + j) 8], a float4 and a float2) and adds T_ij v into 6 NP FP32
+// partial sums (a lane sums about a 32nd of the row).  The
+// partials are summed over the warp by a transposing butterfly (31 exchanges
+// per 32 values, lane l ends with the sum of value l), its first two stages
+// in FP32 and the last three in FP64.
 template <int NP>
-__global__ void __launch_bounds__(256) k_pme_real_pairs(
-    const int* __restrict__ rcnt, const int* __restrict__ rrows,
-    const double4* __restrict__ pos, Cell cell, const float* __restrict__ tt, int rcap,
-    const float* __restrict__ vpk, int N, double* __restrict__ rsum) {
+__global__ void __launch_bounds__(256, 3) k_pme_real_pairs(
+    const int* __restrict__ rcnt, const int* __restrict__ rrows, const float4* __restrict__ rw,
+    int rcap, const float* __restrict__ vpk, int N, double* __restrict__ rsum) {
+  constexpr int NV = 6 * NP;
   int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
-  double u[6 * NP];
+  float u[NV];
 #pragma unroll
-  for (int e = 0; e < 6 * NP; e++) u[e] = 0.0;
+  for (int e = 0; e < NV; e++) u[e] = 0.f;
   int n = rcnt[i];
   const int* prow = rrows + (size_t)i * rcap;
-  const float* tr = tt + 2 * (size_t)i * rcap;
-  double4 pi = pos[i];
-  const double h00 = cell.H[0], h01 = cell.H[1], h10 = cell.H[3], h11 = cell.H[4];
-  const double g00 = cell.Hi[0], g01 = cell.Hi[1], g10 = cell.Hi[3], g11 = cell.Hi[4];
-  const double Lz = cell.H[8], iLz = cell.Hi[8];
+  const float4* prw = rw + (size_t)i * rcap;
   for (int kk = lane; kk < n; kk += 32) {
-    int j = prow[kk];
-    double4 pj = pos[j];
-    double t1 = tr[2 * kk], t2r = tr[2 * kk + 1];
-    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    double s0 = g00 * dx + g01 * dy, s1 = g10 * dx + g11 * dy, s2 = iLz * dz;
-    s0 -= rint(s0);
-    s1 -= rint(s1);
-    s2 -= rint(s2);
-    dx = h00 * s0 + h01 * s1;
-    dy = h10 * s0 + h11 * s1;
-    dz = Lz * s2;
+    int j = __ldg(prow + kk);
+    float4 q = __ldg(prw + kk);
+    float s = (__float_as_uint(q.x) & 1u) ? -1.f : 1.f;
 #pragma unroll
     for (int p = 0; p < NP; p++) {
       const float4* vj = (const float4*)(vpk + ((size_t)p * N + j) * 8);
-      float4 a = vj[0], b = vj[1];
-      double qa = t2r * (dx * a.x + dy * a.y + dz * a.z);
-      double qb = t2r * (dx * a.w + dy * b.x + dz * b.y);
-      u[6 * p] += t1 * a.x + qa * dx;
-      u[6 * p + 1] += t1 * a.y + qa * dy;
-      u[6 * p + 2] += t1 * a.z + qa * dz;
-      u[6 * p + 3] += t1 * a.w + qb * dx;
-      u[6 * p + 4] += t1 * b.x + qb * dy;
-      u[6 * p + 5] += t1 * b.y + qb * dz;
+      float4 a = __ldg(vj);
+      float2 b = __ldg((const float2*)(vj + 1));
+      float qa = s * (q.y * a.x + q.z * a.y + q.w * a.z);
+      float qb = s * (q.y * a.w + q.z * b.x + q.w * b.y);
+      u[6 * p] += q.x * a.x + qa * q.y;
+      u[6 * p + 1] += q.x * a.y + qa * q.z;
+      u[6 * p + 2] += q.x * a.z + qa * q.w;
+      u[6 * p + 3] += q.x * a.w + qb * q.y;
+      u[6 * p + 4] += q.x * b.x + qb * q.z;
+      u[6 * p + 5] += q.x * b.y + qb * q.w;
     }
   }
+  // the first two exchanges in FP32 (sums of 2 and 4 lanes), the rest in FP64
+  float f[32];
 #pragma unroll
-  for (int e = 0; e < 6 * NP; e++) {
+  for (int e = 0; e < 32; e++) f[e] = e < NV ? u[e] : 0.f;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) u[e] += __shfl_xor_sync(0xffffffffu, u[e], o);
+  for (int off = 16; off >= 8; off >>= 1) {
+    bool up = lane & off;
+#pragma unroll
+    for (int e = 0; e < off; e++) {
+      float send = up ? f[e] : f[e + off];
+      float keep = up ? f[e + off] : f[e];
+      f[e] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
   }
+  double d[8];
 #pragma unroll
-  for (int e = 0; e < 6 * NP; e++)
-    if (e == lane) rsum[((size_t)(e / 6) * N + i) * 6 + e % 6] = u[e];
+  for (int e = 0; e < 8; e++) d[e] = (double)f[e];
+#pragma unroll
+  for (int off = 4; off >= 1; off >>= 1) {
+    bool up = lane & off;
+#pragma unroll
+    for (int e = 0; e < off; e++) {
+      double send = up ? d[e] : d[e + off];
+      double keep = up ? d[e + off] : d[e];
+      d[e] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  // value e = 6 p + 3 h + c
+  if (lane < NV) rsum[((size_t)(lane / 6) * N + i) * 6 + lane % 6] = d[0];
 }
 
 // Cells of the real-space list (fractional, width >= rc).
@@ -704,7 +677,7 @@ template <typename R>
 __global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, int N,
                           const int* __restrict__ cell_start, const int* __restrict__ beads,
                           double rc2, double alpha, double alpha_ref, int rcap, int* cnt,
-                          int* rows, R* tt, int* err) {
+                          int* rows, R* tt, float4* rw, int* need, int* err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double4 p = pos[i];
@@ -715,7 +688,7 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, i
     lo[d] = g.n[d] >= 3 ? -1 : 0;
     hi[d] = g.n[d] >= 3 ? 1 : g.n[d] - 1;
   }
-  int n = 0;
+  int n = 0, nall = 0;
   bool over = false;
   for (int a = lo[0]; a <= hi[0]; a++)
     for (int b = lo[1]; b <= hi[1]; b++)
@@ -738,6 +711,7 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, i
           if (rr >= rc2) continue;
           if (n >= rcap) {
             over = true;
+            nall++;
             continue;
           }
           double t1, t2;
@@ -745,11 +719,23 @@ __global__ void k_rl_rows(Cell cell, RGeom g, const double4* __restrict__ pos, i
           rows[(size_t)i * rcap + n] = j;
           tt[2 * ((size_t)i * rcap + n)] = (R)t1;
           tt[2 * ((size_t)i * rcap + n) + 1] = (R)(t2 / rr);
+          if (rw) {
+            double sw = sqrt(fabs(t2 / rr));
+            unsigned b = (__float_as_uint((float)t1) & ~1u) | (t2 < 0.0 ? 1u : 0u);
+            rw[(size_t)i * rcap + n] =
+                make_float4(__uint_as_float(b), (float)(sw * dx), (float)(sw * dy), (float)(sw * dz));
+          }
           n++;
+          nall++;
         }
       }
   cnt[i] = n;
-  if (over) atomicOr(err, ERRB_NBR_OVERFLOW);
+  if (over) {
+    if (need)
+      atomicMax(need, nall);  // the host grows the rows and builds them again
+    else
+      atomicOr(err, ERRB_NBR_OVERFLOW);
+  }
 }
 
 namespace bd {
@@ -782,12 +768,15 @@ int pme_alloc(bd_ctx* c) {
     c->rl_cap = std::max(512, ((int)ceil(2.5 * mean) + 31) / 32 * 32);
   }
   CU(cudaMalloc(&c->rl_cnt, 4 * (size_t)N));
+  CU(cudaMalloc(&c->rl_need, 4));
+  CU(cudaMemsetAsync(c->rl_need, 0, 4, c->stream));
   CU(cudaMalloc(&c->rl_rows, 4 * (size_t)N * c->rl_cap));
   CU(cudaMalloc(&c->rl_pos, 32 * (size_t)N));
   if (c->pme_f32 && nr > 1) {
     CU(cudaMalloc(&c->pme_vpk, 32 * (size_t)N * ((nr + 1) / 2)));
     CU(cudaMalloc(&c->pme_rsum, 48 * (size_t)N * ((nr + 1) / 2)));
-    c->bytes += 80 * (size_t)N * ((nr + 1) / 2);
+    CU(cudaMalloc(&c->rl_w, 16 * (size_t)N * c->rl_cap));
+    c->bytes += 80 * (size_t)N * ((nr + 1) / 2) + 16 * (size_t)N * c->rl_cap;
   }
   CU(cudaMalloc(&c->rl_tt, 2 * es * (size_t)N * c->rl_cap));
   c->rl_ncell_cap = 4096;
@@ -858,7 +847,7 @@ void pme_free(bd_ctx* c) {
       cufftDestroy((cufftHandle)c->pme_mplan_f[q]);
       c->pme_mplan_k[q] = 0;
     }
-  void* ptrs[] = {c->pme_vpk, c->pme_rsum, c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
+  void* ptrs[] = {c->pme_vpk, c->pme_rsum, c->rl_w, c->rl_need, c->pme_grid, c->pme_spec, c->pme_infl, c->pme_bsq, c->pme_soff, c->pme_base, c->pme_w,
                   c->rl_cnt, c->rl_rows, c->rl_pos, c->rl_tt, c->rl_cell_of, c->rl_beads, c->rl_cell_count,
                   c->rl_cell_start, c->rl_cursor};
   for (void* q : ptrs)
@@ -870,6 +859,28 @@ void pme_free(bd_ctx* c) {
 // spline weights, influence tensor of the current cell, self off-diagonal
 // sums, real-space pair list and tensors.  The products that follow use this
 // configuration until the next preparation, as the dense matrix does.
+// Pair rows of a larger cap (the rows are rebuilt by the caller).
+static int rl_grow(bd_ctx* c, int cap) {
+  size_t N = c->N, es = c->pme_f32 ? 4 : 8, old = (size_t)c->rl_cap;
+  CU(cudaStreamSynchronize(c->stream));
+  cudaFree(c->rl_rows);
+  cudaFree(c->rl_tt);
+  c->rl_rows = nullptr;
+  c->rl_tt = nullptr;
+  CU(cudaMalloc(&c->rl_rows, 4 * N * cap));
+  CU(cudaMalloc(&c->rl_tt, 2 * es * N * cap));
+  c->bytes += (4 + 2 * es) * N * (cap - old);
+  if (c->rl_w) {
+    cudaFree(c->rl_w);
+    c->rl_w = nullptr;
+    CU(cudaMalloc(&c->rl_w, 16 * N * cap));
+    c->bytes += 16 * N * (cap - old);
+  }
+  c->rl_cap = cap;
+  CU(cudaMemsetAsync(c->rl_need, 0, 4, c->stream));
+  return BD_OK;
+}
+
 int pme_prepare(bd_ctx* c, const Lat& l) {
   int s;
   if ((s = pme_alloc(c)) != BD_OK) return s;
@@ -926,14 +937,25 @@ int pme_prepare(bd_ctx* c, const Lat& l) {
   k_rl_fill<<<nblk(N, 256), 256, 0, c->stream>>>(c->rl_cell_of, c->rl_cell_start, c->rl_cursor,
                                                  c->rl_beads, N);
   if ((s = launch_ok(c)) != BD_OK) return s;
-if (c->pme_f32)
-    k_rl_rows<float><<<nblk(N, 128), 128, 0, c->stream>>>(
-        cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
-        alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (float*)c->rl_tt, c->err);
-  else
-    k_rl_rows<double><<<nblk(N, 128), 128, 0, c->stream>>>(
-        cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
-        alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (double*)c->rl_tt, c->err);
+  // the pair rows; with the default cap (no pme_max_pairs), rows that
+  // overflow it are grown to 1.25 times the longest row and built again
+  int* need = c->p.pme_max_pairs > 0 ? nullptr : c->rl_need;
+  for (int pass = 0; pass < 2; pass++) {
+    if (c->pme_f32)
+      k_rl_rows<float><<<nblk(N, 128), 128, 0, c->stream>>>(
+          cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
+          alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (float*)c->rl_tt, c->rl_w, need, c->err);
+    else
+      k_rl_rows<double><<<nblk(N, 128), 128, 0, c->stream>>>(
+          cell, g, (const double4*)c->rl_pos, N, c->rl_cell_start, c->rl_beads, rc * rc, alpha,
+          alpha_ref, c->rl_cap, c->rl_cnt, c->rl_rows, (double*)c->rl_tt, nullptr, need, c->err);
+    if (!need) break;
+    int longest = 0;
+    CU(cudaMemcpyAsync(&longest, need, 4, cudaMemcpyDeviceToHost, c->stream));
+    if ((s = check(c)) != BD_OK) return s;
+    if (longest <= c->rl_cap) break;
+    if ((s = rl_grow(c, ((int)ceil(1.25 * longest) + 31) / 32 * 32)) != BD_OK) return s;
+  }
   // the cell and calcHI's split parameter of this configuration, for the
   // products until the next preparation
   memcpy(c->pme_cellbuf, cell.H, sizeof(cell.H));
@@ -992,7 +1014,7 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
   k_pme_gather<P_, R, 1, false><<<nb8, 256, 0, c->stream>>>(                                  \
       c->pme_base, c->pme_w, N, K, grid, 1, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,       \
       c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
-      ostride, orr, nullptr, nullptr)
+      ostride, orr, nullptr)
     switch (p) {
       case 4: PME_GATHER(4); break;
       case 6: PME_GATHER(6); break;
@@ -1031,35 +1053,35 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
     CF(cufftExecC2C(plan, (cufftComplex*)cg, (cufftComplex*)cg, CUFFT_INVERSE));
   else
     CF(cufftExecZ2Z(plan, (cufftDoubleComplex*)cg, (cufftDoubleComplex*)cg, CUFFT_INVERSE));
-  // FP32: the real-space sums of all packed pairs in one pass over the rows
+  // FP32: the real-space sums of the packed pairs, in passes over the rows of
+  // up to five pairs (30 FP32 partial sums per lane at 80 registers)
   double* rsum = nullptr;
   if constexpr (sizeof(R) == 4) {
-    if (vpk && c->pme_rsum && np <= 8) {
+    if (vpk && c->pme_rsum && c->rl_w) {
       rsum = c->pme_rsum;
-      c->launches++;
-#define PME_REAL(NP_)                                                                          \
-  k_pme_real_pairs<NP_><<<nb8, 256, 0, c->stream>>>(c->rl_cnt, c->rl_rows,                     \
-                                                    (const double4*)c->rl_pos, cell,           \
-                                                    (const float*)c->rl_tt, c->rl_cap, vpk, N, \
-                                                    rsum)
-      switch (np) {
-        case 1: PME_REAL(1); break;
-        case 2: PME_REAL(2); break;
-        case 3: PME_REAL(3); break;
-        case 4: PME_REAL(4); break;
-        case 5: PME_REAL(5); break;
-        case 6: PME_REAL(6); break;
-        case 7: PME_REAL(7); break;
-        default: PME_REAL(8);
-      }
+      for (int p0 = 0; p0 < np; p0 += 5) {
+        const float* vp = vpk + (size_t)p0 * N * 8;
+        double* rs = rsum + (size_t)p0 * N * 6;
+        c->launches++;
+#define PME_REAL(NP_)                                                                        \
+  k_pme_real_pairs<NP_><<<nb8, 256, 0, c->stream>>>(c->rl_cnt, c->rl_rows, c->rl_w, c->rl_cap, \
+                                                    vp, N, rs)
+        switch (std::min(5, np - p0)) {
+          case 1: PME_REAL(1); break;
+          case 2: PME_REAL(2); break;
+          case 3: PME_REAL(3); break;
+          case 4: PME_REAL(4); break;
+          default: PME_REAL(5);
+        }
 #undef PME_REAL
+      }
     }
   }
 #define PME_GATHER(P_, RS_)                                                                   \
   k_pme_gather<P_, R, 2, true, RS_><<<gp, 256, 0, c->stream>>>(                               \
       c->pme_base, c->pme_w, N, K, (const R*)cg, k, c->pme_self, c->pme_soff, v, vr,          \
       c->rl_cnt, c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap,  \
-      o0, o1, o2, ostride, orr, vpk, rsum)
+      o0, o1, o2, ostride, orr, rsum)
   if (rsum) {
     switch (p) {
       case 4: PME_GATHER(4, true); break;

@@ -25,7 +25,9 @@ No reference counterpart; checked against
   transforms), FP64 1e-12, FP32 2e-6, and FP32 blocks against FP64 single
   products 1e-5, with an odd number of vectors (a lone right-hand side in the
   last pair);
-* a few hundred Krylov Brownian steps with the PME mobility run without error.
+* a few hundred Krylov Brownian steps with the PME mobility run without error;
+* pair rows past the default cap (600 beads within 5 of each other) grown
+  and built again, an explicit cap overflowing reported as an error.
 """
 import numpy as np
 import pytest
@@ -140,6 +142,48 @@ def test_block_product_matches_single(precision, K, tol, flow, t):
         c64, _, _ = _prepared(flow, t, pme_grid=K)
         errs = [rel_err(got[r], c64.mobility_apply(V[r])) for r in range(7)]
         assert max(errs) < 1e-5, errs
+
+
+def _clustered(precision="fp64", **pme):
+    """600 beads uniform within 5 of the centre of a box of 30: with cutoff
+    12.9 each has 599 others within the cutoff, past the default cap of 512
+    pairs per row."""
+    Nb, Nc, L = 25, 24, 30.0
+    r = np.random.default_rng(17).uniform(-5.0, 5.0, size=(3, Nb * Nc))
+    c = B.Context(B.make_params(0, Nb, Nc, L, 0.2, 5e-4, mobility="pme", noise="philox",
+                                precision=precision, pme_grid=32, pme_order=6, pme_rc=12.9,
+                                pme_alpha=0.3, **pme))
+    c.set_positions(*r)
+    c.set_time(0, 0)
+    c.update_lattice(0)
+    return c, r
+
+
+def test_pair_rows_grow_past_the_default_cap():
+    """With the default cap the rows that overflow it are grown and built
+    again: the product matches the CPU model of the same discretisation, and
+    the FP32 block product (its own pair data) matches the FP64 product."""
+    c, r = _clustered()
+    c.calc_hi()
+    o = O.Oracle(0, 25, 24, 30.0, 0.2, 5e-4)
+    o.lattice(0)
+    pos, H = _lab_cell(o, r[0], r[1], r[2], 30.0)
+    v = np.random.default_rng(5).normal(size=(600, 3))
+    ref = P.pme_apply(H, pos, v, 32, 6, 0.3, 12.9, alpha_ref=P.ref_alpha(0, o.s.tp, o.s.L2yp))
+    got = c.mobility_apply(v.reshape(-1)).reshape(600, 3)
+    assert rel_err(got, ref) < 1e-11
+    c32, _ = _clustered("fp32", noise_block=4)
+    c32.calc_hi()
+    V = np.random.default_rng(6).normal(size=(4, 1800))
+    out = c32.mobility_apply_block(V)
+    assert max(rel_err(out[k], c.mobility_apply(V[k])) for k in range(4)) < 1e-5
+
+
+def test_explicit_pair_cap_overflow_is_an_error():
+    c, _ = _clustered(pme_max_pairs=64)
+    with pytest.raises(B.BDError, match="overflow"):
+        c.calc_hi()
+        c.mobility_apply(np.ones(1800))
 
 
 def test_pme_rejects_dense_download():
