@@ -16,8 +16,10 @@ Default workload (c3): planar extension with Kraynik-Reinelt boundaries,
 Q0=3, WCA, 50% charged, charge hop every 100 steps (c1: 80 x 100 beads in a
 box of 60a at Wi = 2).  Inputs are seeded synthetic chains.  The default path
 (pme32-learned) computes the Ewald-summed Rotne-Prager-Yamakawa mobility by
-smooth particle-mesh Ewald (FP32 grids, cutoff 12.1 with the grid from the
-library's rule) and the Brownian displacement sqrt(M) z by a preconditioned
+smooth particle-mesh Ewald (FP32 grids; the cutoff, and with it the grid by
+the library's accuracy rule, picked by bd_b200.autotune_pme_cutoff as the
+fastest product on this GPU, reported in config) and the Brownian
+displacement sqrt(M) z by a preconditioned
 Lanczos solve at tolerance 1e-6 (learned bead blocks on 10-bead segment
 blocks), the displacements of 10 consecutive steps solved by one multi-vector
 Krylov run (noise blocks of 10 steps, which tile the rebuild period).  --compare 1 also times the plain FP64 method

@@ -104,6 +104,7 @@ struct bd_ctx {
   // noise_block > 1); vector (j, r) of the basis at BV + (j * nbk + r) * 3 NTp
   int nbk;             // block capacity (1: per-step solves)
   double *BV;          // (lmax+1) x nbk basis vectors
+  float *BVs;          // FP32 contexts: their FP32 copy, read by the reorthogonalisation pass
   double *Bw, *Bvcur, *Bt1, *Bt2, *BY;  // nbk x 3 NTp each
   double *BR;          // nbk x 3N noise draws (bead-interleaved)
   double *Bpart;       // 3 x nbk x (lmax+1) x kDotBlocks partial dots

@@ -116,22 +116,23 @@ __device__ __forceinline__ void chunk_range(int n, int& lo, int& hi) {
 // Dots of four vectors at a time per warp (vectors k0..k0+3, warps strided
 // by groups): lanes over the chunk, so each lane keeps several independent
 // loads in flight; butterfly reductions.
-__device__ __forceinline__ void chunk_dots(const double* __restrict__ V, size_t vs, int nv,
+template <typename T>
+__device__ __forceinline__ void chunk_dots(const T* __restrict__ V, size_t vs, int nv,
                                            const double* __restrict__ w, int lo, int hi,
                                            double* part) {
   int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k0 = 4 * wp; k0 < nv; k0 += 4 * nw) {
-    const double* v0 = V + (size_t)k0 * vs;
-    const double* v1 = V + (size_t)min(k0 + 1, nv - 1) * vs;
-    const double* v2 = V + (size_t)min(k0 + 2, nv - 1) * vs;
-    const double* v3 = V + (size_t)min(k0 + 3, nv - 1) * vs;
+    const T* v0 = V + (size_t)k0 * vs;
+    const T* v1 = V + (size_t)min(k0 + 1, nv - 1) * vs;
+    const T* v2 = V + (size_t)min(k0 + 2, nv - 1) * vs;
+    const T* v3 = V + (size_t)min(k0 + 3, nv - 1) * vs;
     double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
     for (int i = lo + lane; i < hi; i += 32) {
       double x = w[i];
-      s0 += v0[i] * x;
-      s1 += v1[i] * x;
-      s2 += v2[i] * x;
-      s3 += v3[i] * x;
+      s0 += (double)v0[i] * x;
+      s1 += (double)v1[i] * x;
+      s2 += (double)v2[i] * x;
+      s3 += (double)v3[i] * x;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -151,16 +152,17 @@ __device__ __forceinline__ void chunk_dots(const double* __restrict__ V, size_t 
 
 // sum_k h[k] V_k[i] with eight independent partial sums (loads in flight),
 // combined in a fixed order.
-__device__ __forceinline__ double combo_row(const double* __restrict__ V, size_t vs,
+template <typename T>
+__device__ __forceinline__ double combo_row(const T* __restrict__ V, size_t vs,
                                             const double* h, int nv, int i) {
   double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int k = 0;
   for (; k + 8 <= nv; k += 8) {
 #pragma unroll
-    for (int q = 0; q < 8; q++) a[q] += h[k + q] * V[(size_t)(k + q) * vs + i];
+    for (int q = 0; q < 8; q++) a[q] += h[k + q] * (double)V[(size_t)(k + q) * vs + i];
   }
   double t = 0;
-  for (; k < nv; k++) t += h[k] * V[(size_t)k * vs + i];
+  for (; k < nv; k++) t += h[k] * (double)V[(size_t)k * vs + i];
   a[0] += t;
   return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
 }
@@ -184,6 +186,7 @@ __device__ __forceinline__ void sum_parts(const double* __restrict__ part, int n
 // r * hst, alpha_j and beta_j at [j * kst + r].
 struct Kry {
   double* V;
+  float* Vs;  // FP32 copy of the basis for the reorthogonalisation pass, or null
   size_t bs;
   double *w, *vcur;
   double *part1, *part2, *part3;
@@ -207,6 +210,11 @@ struct Kry {
 //   k_orth1: alpha; three-term update; partial V^T w per chunk
 //   k_orth2: d = V^T w; w -= V d; |w|^2 partials; alpha_j = alpha + d_j
 //   k_orth3: beta_j = |w|; v_{j+1} = w / beta_j
+// With Vs (FP32 block products) the Gram-Schmidt pass reads an FP32 copy of
+// the basis: its coefficients are at the level of the lost orthogonality,
+// so their FP32 error (about 1e-10 of |w|) keeps the basis orthogonal well
+// within sqrt(eps_64); the recurrence, alpha, beta and the final
+// combination stay on the FP64 basis.
 __global__ void __launch_bounds__(256) k_orth0(Kry q) {
   __shared__ double red[8];
   int r = blockIdx.y, j = *q.jd, lo, hi;
@@ -245,7 +253,10 @@ __global__ void __launch_bounds__(256) k_orth1(Kry q) {
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x)
     w[i] = w[i] - alpha * vj[i] - bprev * vp[i];
   __syncthreads();
-  chunk_dots(V, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
+  if (q.Vs)
+    chunk_dots(q.Vs + (size_t)r * q.n, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
+  else
+    chunk_dots(V, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
 }
 
 __global__ void __launch_bounds__(256) k_orth2(Kry q) {
@@ -257,8 +268,9 @@ __global__ void __launch_bounds__(256) k_orth2(Kry q) {
   chunk_range(q.n, lo, hi);
   sum_parts(q.part2 + r * q.pst, nv, h);
   double s2 = 0;
+  const float* Vs = q.Vs ? q.Vs + (size_t)r * q.n : nullptr;
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double x = w[i] - combo_row(V, q.bs, h, nv, i);
+    double x = w[i] - (Vs ? combo_row(Vs, q.bs, h, nv, i) : combo_row(V, q.bs, h, nv, i));
     w[i] = x;
     s2 += x * x;
   }
@@ -290,13 +302,21 @@ __global__ void __launch_bounds__(256) k_orth3(Kry q) {
   const double* w = q.w + (size_t)r * q.n;
   double* vnext = q.V + (size_t)(j + 1) * q.bs + (size_t)r * q.n;
   double* vcur = q.vcur + (size_t)r * q.n;
+  float* vsnext = q.Vs ? q.Vs + (size_t)(j + 1) * q.bs + (size_t)r * q.n : nullptr;
   int lo, hi;
   chunk_range(q.n, lo, hi);
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     double x = w[i] * f;
     vnext[i] = x;
     vcur[i] = x;
+    if (vsnext) vsnext[i] = (float)x;
   }
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
 }
 
 __global__ void k_next_j(int* jd) {
@@ -705,6 +725,7 @@ static int lanczos_iteration(bd_ctx* c, bool pre, bool force) {
   }
   Kry q;
   q.V = c->LV;
+  q.Vs = nullptr;
   q.bs = vs;
   q.w = c->Lw;
   q.vcur = vc;
@@ -883,6 +904,10 @@ static int alloc_blocks(bd_ctx* c) {
   int k = c->nbk, L1 = c->lmax + 1, blk = kDotBlocks;
   size_t n = 3 * (size_t)c->NT * 32;
   CU(cudaMalloc(&c->BV, 8 * n * k * L1));
+  if (c->p.precision == BD_PREC_FP32) {  // FP32 copy for the reorthogonalisation pass
+    CU(cudaMalloc(&c->BVs, 4 * n * k * L1));
+    c->bytes += 4 * n * k * L1;
+  }
   for (double** q : {&c->Bw, &c->Bvcur, &c->Bt1, &c->Bt2, &c->BY}) {
     CU(cudaMalloc(q, 8 * n * k));
     CU(cudaMemsetAsync(*q, 0, 8 * n * k, c->stream));  // padding entries stay zero
@@ -918,6 +943,8 @@ void lanczos_blocks_free(bd_ctx* c) {
   if (c->Bctl) cudaFree(c->Bctl);
   if (c->Bdh) cudaFree(c->Bdh);
   if (c->Bpsi) cudaFree(c->Bpsi);
+  if (c->BVs) cudaFree(c->BVs);
+  c->BVs = nullptr;
   c->Bctl = nullptr;
   c->Bdh = c->Bpsi = nullptr;
   if (c->Bhost) cudaFreeHost(c->Bhost);
@@ -951,6 +978,7 @@ static Kry block_kry(bd_ctx* c, int k) {
   size_t n = 3 * (size_t)c->NT * 32;
   Kry q;
   q.V = c->BV;
+  q.Vs = c->BVs;
   q.bs = n * k;
   q.w = c->Bw;
   q.vcur = c->Bvcur;
@@ -1173,6 +1201,10 @@ static int lanczos_run_multi_device(bd_ctx* c, int k, bool pre, double* out,
   k_interleaved_to_soa<<<dim3((NTp + 255) / 256, k), 256, 0, st>>>(c->BR, 3 * (size_t)N, c->Bsc,
                                                                    c->BV, n, N, NTp);
   CU(cudaMemcpyAsync(c->Bvcur, c->BV, 8 * n * k, cudaMemcpyDeviceToDevice, st));
+  if (c->BVs) {
+    c->launches++;
+    k_to_f32<<<592, 256, 0, st>>>(c->BV, c->BVs, n * k);
+  }
   CU(cudaMemsetAsync(c->Bjd, 0, sizeof(int), st));
   CU(cudaMemsetAsync(c->Bctl, 0, 4 * 3 * (size_t)k, st));             // done, conv, neg
   CU(cudaMemsetAsync(c->Bctl + 3 * k, 0xff, 4 * (size_t)k, st));      // last = -1
@@ -1248,6 +1280,10 @@ static int lanczos_run_multi(bd_ctx* c, int k, bool pre, double* out, std::vecto
   k_interleaved_to_soa<<<dim3((NTp + 255) / 256, k), 256, 0, st>>>(c->BR, 3 * (size_t)N, c->Bsc,
                                                                    c->BV, n, N, NTp);
   CU(cudaMemcpyAsync(c->Bvcur, c->BV, 8 * n * k, cudaMemcpyDeviceToDevice, st));
+  if (c->BVs) {
+    c->launches++;
+    k_to_f32<<<592, 256, 0, st>>>(c->BV, c->BVs, n * k);
+  }
   CU(cudaMemsetAsync(c->Bjd, 0, sizeof(int), st));
   std::vector<std::vector<double>> cc(k);
   std::vector<char> done(k, 0);
