@@ -838,9 +838,12 @@ def run_ours(args, rank, world, dist):
                                        args.pme_rc) if pme else
                                     "Ewald-summed RPY, every pair (dense packed tiles)"),
                        "pme_cutoff_autotune_ms": tuned,
-                       "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 orthogonalisation" +
+                       "noise": "Lanczos sqrt(M) z, tol 1e-6, FP64 recurrence and basis" +
                                 (", noise blocks of %d steps" % main["block"]["noise_block"]
-                                 if main["block"] else ""),
+                                 if main["block"] else "") +
+                                (" (Gram-Schmidt pass on an FP32 copy of the basis)"
+                                 if main["block"] and PATHS[args.path]["precision"] == "fp32"
+                                 else ""),
                        "noise_block": main["block"],
                        "electrostatics": ("Ewald Coulomb, chains alternately -1 / +1 on half "
                                           "their beads" if PATHS[args.path].get("physics") ==
