@@ -24,7 +24,8 @@ Lanczos solve at tolerance 1e-6 (learned bead blocks on 10-bead segment
 blocks), the displacements of 10 consecutive steps solved by one multi-vector
 Krylov run (noise blocks of 10 steps, which tile the rebuild period).  --compare 1 also times the plain FP64 method
 (pme64, no preconditioner) on the same grid, with one solve per step and with
-the same noise blocks; --errors 1 reports the per-result error of the path
+the same noise blocks, and the unpreconditioned FP32 path (pme32, same noise
+blocks); --errors 1 reports the per-result error of the path
 against pme64 on the same configuration.  The rebuild (every 100 steps) and
 the sweep (every 100 steps) are timed on the device once each and carried at
 their frequency in every figure (breakdown.amortised).
@@ -415,6 +416,13 @@ def build_context(w, seed, path="lanczos32", device_noise="philox", noise_seed=N
     return c
 
 
+# DRAM bytes (read + write, cold cache) of one block product, summed over its
+# kernels from an ncu capture of the bench's own command
+# (profiles/traffic_product_c3.md); keyed by (beads, grid, cutoff,
+# right-hand sides per product)
+PRODUCT_TRAFFIC = {(50000, 108, 13.6, 10): 2.6445e9}
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -766,6 +774,9 @@ def accuracy_vs_fp64(w, path, noise_block, pme_rc, pme_grid, seed=1000):
         p64 = run("pme64")
         out["displacement_plain"] = rel(p32[2], p64[2])
         out["krylov_iterations"].update({"pme32": p32[3], "pme64": p64[3]})
+    if pre == "learned" and "pme32-seg" in PATHS:
+        # the learned blocks' own share: the same solve on segment blocks alone
+        out["krylov_iterations"]["pme32-seg"] = run("pme32-seg")[3]
     return out
 
 
@@ -818,6 +829,10 @@ def run_ours(args, rank, world, dist):
                                "per launch: spread, R2C, influence, C2R, gather)"
                                % b["rhs_per_iteration"],
                      "achieved": b["achieved_gbs"], "frac": b["achieved_gbs"] / peak,
+                     "traffic": PRODUCT_TRAFFIC.get(
+                         (N, args.pme_grid or __import__("bd_b200").pme_default_grid(
+                             w["L"], args.pme_rc), round(float(args.pme_rc), 2),
+                          int(round(b["rhs_per_iteration"])))),
                      "alg_bytes_per_launch": b["alg_bytes"], "avg_launch_ms": b["avg_product_ms"],
                      "launches": b["products"],
                      "single_product": {"achieved": main["achieved_gbs"],
@@ -891,6 +906,18 @@ def run_ours(args, rank, world, dist):
                 "lanczos_iters_per_step": refb["lanczos_iters_per_step"]}
             line["speedup_vs_plain_fp64_noise_blocks"] = (
                 line["value"] / line["plain_fp64_noise_blocks"]["value"])
+            if PATHS[args.path].get("precond") and "pme32" in PATHS:
+                # unpreconditioned Lanczos with everything else the same (FP32
+                # storage, noise blocks): what the preconditioner gains
+                refu = measure(w, "pme32", K, W, rank, dist, 1, args.noise_block, args.pme_rc,
+                               args.pme_grid)
+                line["unpreconditioned_fp32"] = {
+                    "path": "pme32", "noise_block": args.noise_block,
+                    "value": world * N * K / (refu["t_max_ms"] / 1e3),
+                    "ms_per_step": refu["t_max_ms"] / K,
+                    "lanczos_iters_per_step": refu["lanczos_iters_per_step"]}
+                line["speedup_vs_unpreconditioned_fp32"] = (
+                    line["value"] / line["unpreconditioned_fp32"]["value"])
     if pme and args.errors and args.path != "pme64":
         line["errors"] = accuracy_vs_fp64(w, args.path, args.noise_block, args.pme_rc,
                                           args.pme_grid)

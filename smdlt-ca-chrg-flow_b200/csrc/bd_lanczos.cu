@@ -107,10 +107,87 @@ __global__ void k_combo(const double* __restrict__ V, size_t vstride,
 //   stage 2: h2 = sum_b part2; w_b -= V_b h2; part3[b] = |w_b|^2;
 //            CTA 0 stores alpha_j = h_j + h2_j
 //   stage 3: beta_j = sqrt(sum_b part3); v_{j+1,b} = w_b / beta_j
+// Chunks are multiples of 4 entries (the vectors' lengths are multiples of
+// 96), so the passes over an FP32 basis can read four rows per load.
 __device__ __forceinline__ void chunk_range(int n, int& lo, int& hi) {
-  int per = (n + gridDim.x - 1) / gridDim.x;
-  lo = blockIdx.x * per;
+  int per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~3;
+  lo = min(n, (int)blockIdx.x * per);
   hi = min(n, lo + per);
+}
+
+// chunk_dots over an FP32 basis, four rows per load (lo, hi multiples of 4)
+__device__ __forceinline__ void chunk_dots4(const float* __restrict__ V, size_t vs, int nv,
+                                            const double* __restrict__ w, int lo, int hi,
+                                            double* part) {
+  int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double2* w2 = (const double2*)w;
+  for (int k0 = 4 * wp; k0 < nv; k0 += 4 * nw) {
+    const float4* v0 = (const float4*)(V + (size_t)k0 * vs);
+    const float4* v1 = (const float4*)(V + (size_t)min(k0 + 1, nv - 1) * vs);
+    const float4* v2 = (const float4*)(V + (size_t)min(k0 + 2, nv - 1) * vs);
+    const float4* v3 = (const float4*)(V + (size_t)min(k0 + 3, nv - 1) * vs);
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i4 = (lo >> 2) + lane; i4 < (hi >> 2); i4 += 32) {
+      double2 wa = w2[2 * i4], wb = w2[2 * i4 + 1];
+      float4 a = v0[i4], b = v1[i4], c = v2[i4], d = v3[i4];
+      s0 += ((double)a.x * wa.x + (double)a.y * wa.y) + ((double)a.z * wb.x + (double)a.w * wb.y);
+      s1 += ((double)b.x * wa.x + (double)b.y * wa.y) + ((double)b.z * wb.x + (double)b.w * wb.y);
+      s2 += ((double)c.x * wa.x + (double)c.y * wa.y) + ((double)c.z * wb.x + (double)c.w * wb.y);
+      s3 += ((double)d.x * wa.x + (double)d.y * wa.y) + ((double)d.z * wb.x + (double)d.w * wb.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+    }
+    if (lane == 0) {
+      part[(size_t)k0 * gridDim.x + blockIdx.x] = s0;
+      if (k0 + 1 < nv) part[(size_t)(k0 + 1) * gridDim.x + blockIdx.x] = s1;
+      if (k0 + 2 < nv) part[(size_t)(k0 + 2) * gridDim.x + blockIdx.x] = s2;
+      if (k0 + 3 < nv) part[(size_t)(k0 + 3) * gridDim.x + blockIdx.x] = s3;
+    }
+  }
+}
+
+// w[i..i+3] -= sum_k h[k] V_k[i..i+3] over an FP32 basis (i = 4 i4), four
+// vectors per step with their own partial sums, combined in a fixed order;
+// returns the four new entries' squares summed
+__device__ __forceinline__ double combo_rows4(const float* __restrict__ V, size_t vs,
+                                              const double* h, int nv, int i4, double* w) {
+  double a[4][4] = {};
+  int k = 0;
+  for (; k + 4 <= nv; k += 4) {
+    float4 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = ((const float4*)(V + (size_t)(k + q) * vs))[i4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      a[q][0] += h[k + q] * (double)v[q].x;
+      a[q][1] += h[k + q] * (double)v[q].y;
+      a[q][2] += h[k + q] * (double)v[q].z;
+      a[q][3] += h[k + q] * (double)v[q].w;
+    }
+  }
+  for (; k < nv; k++) {
+    float4 v = ((const float4*)(V + (size_t)k * vs))[i4];
+    a[0][0] += h[k] * (double)v.x;
+    a[0][1] += h[k] * (double)v.y;
+    a[0][2] += h[k] * (double)v.z;
+    a[0][3] += h[k] * (double)v.w;
+  }
+  double2* w2 = (double2*)w;
+  double2 wa = w2[2 * i4], wb = w2[2 * i4 + 1];
+  double x[4] = {wa.x, wa.y, wb.x, wb.y}, sq = 0;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    x[e] -= (a[0][e] + a[1][e]) + (a[2][e] + a[3][e]);
+    sq += x[e] * x[e];
+  }
+  w2[2 * i4] = make_double2(x[0], x[1]);
+  w2[2 * i4 + 1] = make_double2(x[2], x[3]);
+  return sq;
 }
 
 // Dots of four vectors at a time per warp (vectors k0..k0+3, warps strided
@@ -233,7 +310,7 @@ __global__ void __launch_bounds__(256) k_orth0(Kry q) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_orth1(Kry q) {
+__global__ void __launch_bounds__(256, 4) k_orth1(Kry q) {
   __shared__ double sa;
   int r = blockIdx.y, j = *q.jd, nv = j + 1, lo, hi;
   const double* V = q.V + (size_t)r * q.n;
@@ -254,12 +331,12 @@ __global__ void __launch_bounds__(256) k_orth1(Kry q) {
     w[i] = w[i] - alpha * vj[i] - bprev * vp[i];
   __syncthreads();
   if (q.Vs)
-    chunk_dots(q.Vs + (size_t)r * q.n, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
+    chunk_dots4(q.Vs + (size_t)r * q.n, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
   else
     chunk_dots(V, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
 }
 
-__global__ void __launch_bounds__(256) k_orth2(Kry q) {
+__global__ void __launch_bounds__(256, 4) k_orth2(Kry q) {
   __shared__ double h[kMaxKrylov + 1];
   __shared__ double red[8];
   int r = blockIdx.y, j = *q.jd, nv = j + 1, lo, hi;
@@ -268,11 +345,16 @@ __global__ void __launch_bounds__(256) k_orth2(Kry q) {
   chunk_range(q.n, lo, hi);
   sum_parts(q.part2 + r * q.pst, nv, h);
   double s2 = 0;
-  const float* Vs = q.Vs ? q.Vs + (size_t)r * q.n : nullptr;
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double x = w[i] - (Vs ? combo_row(Vs, q.bs, h, nv, i) : combo_row(V, q.bs, h, nv, i));
-    w[i] = x;
-    s2 += x * x;
+  if (q.Vs) {
+    const float* Vs = q.Vs + (size_t)r * q.n;
+    for (int i4 = (lo >> 2) + threadIdx.x; i4 < (hi >> 2); i4 += blockDim.x)
+      s2 += combo_rows4(Vs, q.bs, h, nv, i4, w);
+  } else {
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      double x = w[i] - combo_row(V, q.bs, h, nv, i);
+      w[i] = x;
+      s2 += x * x;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
