@@ -30,7 +30,7 @@ Pairs compared:
 tests/test_gpu_stat_parity.py runs short versions; the long runs:
 
     python tests/stat_parity.py --pair north --workload c4 --steps 2000
-    python tests/stat_parity.py --pair reference --workload c0 --steps 5000
+    python tests/stat_parity.py --pair reference --workload c0 --steps 5000 --replicas 8
 """
 from __future__ import annotations
 
@@ -192,13 +192,30 @@ def run_reference_host(workload, steps, every, seed, config_seed=1000, threads=N
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-def run_pair(pair, workload, steps, every):
-    if pair == "north":
-        a = run_gpu(workload, "pme32-learned", steps, every, noise_seed=11)
-        b = run_gpu(workload, "pme64", steps, every, noise_seed=22)
-    else:
-        a = run_gpu(workload, "tea", steps, every, noise_seed=830062920, reference_step=True)
-        b = run_reference_host(workload, steps, every, seed=123456789)
+def merge(runs):
+    """Independent runs (different noise streams) as one sample: their
+    chains and stress blocks side by side."""
+    out = dict(runs[0])
+    for key in ("ree_per_chain", "tau_blocks", "msd_z_per_chain"):
+        out[key] = [x for r in runs for x in r[key]]
+    out["wall_s"] = sum(r["wall_s"] for r in runs)
+    out["runs"] = len(runs)
+    return out
+
+
+def run_pair(pair, workload, steps, every, replicas=1):
+    """Both sides of a pair, each as `replicas` independent runs from the same
+    configuration with different noise streams."""
+    A, B = [], []
+    for k in range(replicas):
+        if pair == "north":
+            A.append(run_gpu(workload, "pme32-learned", steps, every, noise_seed=11 + 100 * k))
+            B.append(run_gpu(workload, "pme64", steps, every, noise_seed=22 + 100 * k))
+        else:
+            A.append(run_gpu(workload, "tea", steps, every, noise_seed=830062920 + 7919 * k,
+                             reference_step=True))
+            B.append(run_reference_host(workload, steps, every, seed=123456789 + 104729 * k))
+    a, b = (A[0], B[0]) if replicas == 1 else (merge(A), merge(B))
     return a, b, compare(a, b)
 
 
@@ -208,6 +225,8 @@ def main():
     ap.add_argument("--workload", default="c4")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--every", type=int, default=50)
+    ap.add_argument("--replicas", type=int, default=1,
+                    help="independent noise streams per side, pooled")
     ap.add_argument("--out", default="")
     ap.add_argument("--ref-worker", default="")
     args = ap.parse_args()
@@ -221,9 +240,9 @@ def main():
         os.dup2(saved, 1)
         print(json.dumps(r))
         return
-    a, b, cmp_ = run_pair(args.pair, args.workload, args.steps, args.every)
+    a, b, cmp_ = run_pair(args.pair, args.workload, args.steps, args.every, args.replicas)
     res = {"pair": args.pair, "workload": args.workload, "steps": args.steps,
-           "every": args.every, "compare": cmp_,
+           "every": args.every, "replicas": args.replicas, "compare": cmp_,
            "wall_s": [a["wall_s"], b["wall_s"]],
            "lanczos": [a.get("lanczos"), b.get("lanczos")]}
     print(json.dumps(res))
