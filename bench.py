@@ -423,6 +423,25 @@ def build_context(w, seed, path="lanczos32", device_noise="philox", noise_seed=N
 PRODUCT_TRAFFIC = {(50000, 108, 13.6, 10): 2.6445e9}
 
 
+def ranks_max(values, dist):
+    """Element-wise maximum over the ranks (the slowest rank's device
+    times); the values themselves without a process group."""
+    if not dist:
+        return [float(v) for v in values]
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def rank0_choice(choice, dist):
+    """Rank 0's list of picks (the autotuned cutoff) on every rank."""
+    if dist:
+        dist.broadcast_object_list(choice, src=0)
+    return choice
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -528,11 +547,7 @@ def measure(w, path, K, W, rank, dist, e2e_steps, noise_block=1, pme_rc=10.0, pm
     step_ms_raw = step_ms
     step_ms = amortise(step_ms, W, K)
     e2e_s = amortise(e2e_s * 1e3, W + K, Ke) / 1e3
-    t_max = step_ms
-    if dist:
-        tt = torch.tensor([step_ms, e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max, e2e_s = float(tt[0].item()), float(tt[1].item())
+    t_max, e2e_s = ranks_max([step_ms, e2e_s], dist)
     mv_ms, mv_n = prof["MATVEC"]
     if pp["mobility"] == "pme":
         # compulsory bytes of one particle-mesh product, s bytes per value:
@@ -794,8 +809,7 @@ def tune_cutoff(w, path, noise_block, rank, dist):
             return c
         best, times = B.autotune_pme_cutoff(make, w["L"], max(noise_block, 2))
         choice = [best, {str(k): round(v, 4) for k, v in times.items()}]
-    if dist is not None:
-        dist.broadcast_object_list(choice, src=0)
+    choice = rank0_choice(choice, dist)
     return choice[0], choice[1]
 
 
