@@ -417,10 +417,10 @@ def build_context(w, seed, path="lanczos32", device_noise="philox", noise_seed=N
 
 
 # DRAM bytes (read + write, cold cache) of one block product, summed over its
-# kernels from an ncu capture of the bench's own command
-# (profiles/traffic_product_c3.md); keyed by (beads, grid, cutoff,
+# kernels from ncu captures of the bench's own command
+# (profiles/launches_pme32-learned_c3.md); keyed by (beads, grid, cutoff,
 # right-hand sides per product)
-PRODUCT_TRAFFIC = {(50000, 108, 13.6, 10): 2.6445e9}
+PRODUCT_TRAFFIC = {(50000, 100, 14.5, 10): 2.1933e9, (50000, 108, 13.6, 10): 2.6445e9}
 
 
 def ranks_max(values, dist):

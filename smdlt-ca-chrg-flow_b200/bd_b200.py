@@ -328,7 +328,7 @@ def pme_default_grid(L, rc=None):
         K += 1
 
 
-PME_CUTOFFS = (10.0, 12.1, 13.6, 15.5, 17.5)
+PME_CUTOFFS = (10.0, 11.1, 12.1, 13.6, 14.5, 15.5, 17.5)
 
 
 def autotune_pme_cutoff(make_context, L, nrhs, candidates=PME_CUTOFFS, reps=4, seed=0):
