@@ -2,7 +2,7 @@
 holds the statistics and the long runs' command lines).
 
 * north: the headline path (FP32 particle-mesh products, learned
-  preconditioner, noise blocks of 8) against the plain FP64 method (pme64) on
+  preconditioner, noise blocks of 10) against the plain FP64 method (pme64) on
   the 4000-bead extensional workload, 600 steps each from the same
   configuration with independent Philox noise;
 * reference: the GPU's reference-mode step (dense hybrid mobility, CA-TEA
