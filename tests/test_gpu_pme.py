@@ -27,7 +27,9 @@ No reference counterpart; checked against
   last pair);
 * a few hundred Krylov Brownian steps with the PME mobility run without error;
 * pair rows past the default cap (600 beads within 5 of each other) grown
-  and built again, an explicit cap overflowing reported as an error.
+  and built again, an explicit cap overflowing reported as an error;
+* the cutoff autotuner of the Python binding times every candidate that
+  fits the box and returns the fastest.
 """
 import numpy as np
 import pytest
@@ -184,6 +186,24 @@ def test_explicit_pair_cap_overflow_is_an_error():
     with pytest.raises(B.BDError, match="overflow"):
         c.calc_hi()
         c.mobility_apply(np.ones(1800))
+
+
+def test_cutoff_autotuner_times_every_candidate_that_fits():
+    """bd_b200.autotune_pme_cutoff times the block product of each candidate
+    cutoff up to 0.43 L (20 is skipped in a box of 30) on the device and
+    returns the fastest; the contexts it was given are closed."""
+    made = []
+
+    def make(rc):
+        c, _, _ = _prepared(0, 0, precision="fp32", pme_rc=rc, noise_block=4)
+        made.append(c)
+        return c
+
+    best, times = B.autotune_pme_cutoff(make, 30.0, 4, candidates=(10.0, 12.5, 20.0))
+    assert sorted(times) == [10.0, 12.5]
+    assert best == min(times, key=times.get)
+    assert all(v > 0 for v in times.values())
+    assert len(made) == 2 and all(c.h is None for c in made)
 
 
 def test_pme_rejects_dense_download():
