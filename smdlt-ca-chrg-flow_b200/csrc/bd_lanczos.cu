@@ -151,38 +151,45 @@ __device__ __forceinline__ void chunk_dots4(const float* __restrict__ V, size_t 
   }
 }
 
-// w[i..i+3] -= sum_k h[k] V_k[i..i+3] over an FP32 basis (i = 4 i4), four
-// vectors per step with their own partial sums, combined in a fixed order;
-// returns the four new entries' squares summed
+// w[i..i+3] -= sum_k h[k] V_k[i..i+3] over an FP32 basis (i = 4 i4), eight
+// vectors' loads in flight per step.  The sum is formed in FP32: the
+// coefficients h are the Gram-Schmidt pass's corrections, at the level of
+// the lost orthogonality (far below |w|), so its FP32 rounding is many
+// orders below w's own; w and its update stay FP64.  Returns the four new
+// entries' squares summed.
 __device__ __forceinline__ double combo_rows4(const float* __restrict__ V, size_t vs,
                                               const double* h, int nv, int i4, double* w) {
-  double a[4][4] = {};
+  float a[2][4] = {};
   int k = 0;
-  for (; k + 4 <= nv; k += 4) {
-    float4 v[4];
+  const float4* V4 = (const float4*)V + i4;
+  const size_t vs4 = vs >> 2;  // vs is a multiple of 4
+  for (; k + 8 <= nv; k += 8) {
+    float4 v[8];
 #pragma unroll
-    for (int q = 0; q < 4; q++) v[q] = ((const float4*)(V + (size_t)(k + q) * vs))[i4];
+    for (int q = 0; q < 8; q++) v[q] = V4[(size_t)(k + q) * vs4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      a[q][0] += h[k + q] * (double)v[q].x;
-      a[q][1] += h[k + q] * (double)v[q].y;
-      a[q][2] += h[k + q] * (double)v[q].z;
-      a[q][3] += h[k + q] * (double)v[q].w;
+    for (int q = 0; q < 8; q++) {
+      float hq = (float)h[k + q];
+      a[q & 1][0] += hq * v[q].x;
+      a[q & 1][1] += hq * v[q].y;
+      a[q & 1][2] += hq * v[q].z;
+      a[q & 1][3] += hq * v[q].w;
     }
   }
   for (; k < nv; k++) {
-    float4 v = ((const float4*)(V + (size_t)k * vs))[i4];
-    a[0][0] += h[k] * (double)v.x;
-    a[0][1] += h[k] * (double)v.y;
-    a[0][2] += h[k] * (double)v.z;
-    a[0][3] += h[k] * (double)v.w;
+    float4 v = V4[(size_t)k * vs4];
+    float hk = (float)h[k];
+    a[0][0] += hk * v.x;
+    a[0][1] += hk * v.y;
+    a[0][2] += hk * v.z;
+    a[0][3] += hk * v.w;
   }
   double2* w2 = (double2*)w;
   double2 wa = w2[2 * i4], wb = w2[2 * i4 + 1];
   double x[4] = {wa.x, wa.y, wb.x, wb.y}, sq = 0;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
-    x[e] -= (a[0][e] + a[1][e]) + (a[2][e] + a[3][e]);
+    x[e] -= (double)a[0][e] + (double)a[1][e];
     sq += x[e] * x[e];
   }
   w2[2 * i4] = make_double2(x[0], x[1]);
@@ -336,6 +343,7 @@ __global__ void __launch_bounds__(256, 4) k_orth1(Kry q) {
     chunk_dots(V, q.bs, nv, w, lo, hi, q.part2 + r * q.pst);
 }
 
+template <bool SHADOW>  // the pass reads the FP32 copy of the basis (q.Vs)
 __global__ void __launch_bounds__(256, 4) k_orth2(Kry q) {
   __shared__ double h[kMaxKrylov + 1];
   __shared__ double red[8];
@@ -345,7 +353,7 @@ __global__ void __launch_bounds__(256, 4) k_orth2(Kry q) {
   chunk_range(q.n, lo, hi);
   sum_parts(q.part2 + r * q.pst, nv, h);
   double s2 = 0;
-  if (q.Vs) {
+  if constexpr (SHADOW) {
     const float* Vs = q.Vs + (size_t)r * q.n;
     for (int i4 = (lo >> 2) + threadIdx.x; i4 < (hi >> 2); i4 += blockDim.x)
       s2 += combo_rows4(Vs, q.bs, h, nv, i4, w);
@@ -825,7 +833,7 @@ static int lanczos_iteration(bd_ctx* c, bool pre, bool force) {
   c->launches += 5;
   k_orth0<<<blk, 256, 0, st>>>(q);
   k_orth1<<<blk, 256, 0, st>>>(q);
-  k_orth2<<<blk, 256, 0, st>>>(q);
+  k_orth2<false><<<blk, 256, 0, st>>>(q);  // single solves keep no FP32 copy
   k_orth3<<<blk, 256, 0, st>>>(q);
   k_next_j<<<1, 32, 0, st>>>(c->Ljd);
   return launch_ok(c);
@@ -1105,7 +1113,10 @@ static int block_part(bd_ctx* c, int k, bool pre, int part) {
   c->launches += 5;
   k_orth0<<<g, 256, 0, st>>>(q);
   k_orth1<<<g, 256, 0, st>>>(q);
-  k_orth2<<<g, 256, 0, st>>>(q);
+  if (q.Vs)
+    k_orth2<true><<<g, 256, 0, st>>>(q);
+  else
+    k_orth2<false><<<g, 256, 0, st>>>(q);
   k_orth3<<<g, 256, 0, st>>>(q);
   k_next_j<<<1, 32, 0, st>>>(c->Bjd);
   return launch_ok(c);
