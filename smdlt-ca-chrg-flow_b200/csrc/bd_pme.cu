@@ -611,6 +611,45 @@ __global__ void __launch_bounds__(256, 3) k_pme_real_pairs(
   if (lane < NV) rsum[((size_t)(lane / 6) * N + i) * 6 + lane % 6] = d[0];
 }
 
+// The real-space part of a single product (FP32 contexts that hold the
+// mobility build's pair data): one warp per bead; per row entry the index
+// and (t1, w) as for the block products, the neighbour's three input values
+// taken to FP32, FP32 partial sums per lane, summed over the warp in FP64;
+// rsum[6 i + c] for c < 3, which the interpolation adds.
+__global__ void __launch_bounds__(256) k_pme_real_single(
+    const int* __restrict__ rcnt, const int* __restrict__ rrows, const float4* __restrict__ rw,
+    int rcap, VecIn v, int N, double* __restrict__ rsum) {
+  int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= N) return;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  int n = rcnt[i];
+  const int* prow = rrows + (size_t)i * rcap;
+  const float4* prw = rw + (size_t)i * rcap;
+  for (int kk = lane; kk < n; kk += 32) {
+    int j = __ldg(prow + kk);
+    float4 q = __ldg(prw + kk);
+    size_t o = (size_t)j * v.stride;
+    float x0 = (float)v.p[0][o], x1 = (float)v.p[1][o], x2 = (float)v.p[2][o];
+    float d = q.y * x0 + q.z * x1 + q.w * x2;
+    d = (__float_as_uint(q.x) & 1u) ? -d : d;
+    a0 += q.x * x0 + d * q.y;
+    a1 += q.x * x1 + d * q.z;
+    a2 += q.x * x2 + d * q.w;
+  }
+  double d0 = a0, d1 = a1, d2 = a2;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d0 += __shfl_xor_sync(0xffffffffu, d0, o);
+    d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+    d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+  }
+  if (lane == 0) {
+    rsum[6 * (size_t)i] = d0;
+    rsum[6 * (size_t)i + 1] = d1;
+    rsum[6 * (size_t)i + 2] = d2;
+  }
+}
+
 // Cells of the real-space list (fractional, width >= rc).
 struct RGeom {
   int n[3];
@@ -1010,15 +1049,31 @@ static int pme_apply_t(bd_ctx* c, int k, const VecIn& v, size_t vr, double* o0, 
     else
       CF(cufftExecZ2D((cufftHandle)c->pme_plan_b, (cufftDoubleComplex*)spec,
                       (cufftDoubleReal*)grid));
-#define PME_GATHER(P_)                                                                        \
-  k_pme_gather<P_, R, 1, false><<<nb8, 256, 0, c->stream>>>(                                  \
+    // FP32 with the stored pair data: the real-space sums in their own pass
+    // (as for the block products), the interpolation then only reads the grid
+    bool rs = sizeof(R) == 4 && c->rl_w && c->pme_rsum;
+    if (rs) {
+      c->launches++;
+      k_pme_real_single<<<nb8, 256, 0, c->stream>>>(c->rl_cnt, c->rl_rows, c->rl_w, c->rl_cap, v,
+                                                     N, c->pme_rsum);
+    }
+#define PME_GATHER(P_, RS_)                                                                   \
+  k_pme_gather<P_, R, 1, false, RS_><<<nb8, 256, 0, c->stream>>>(                             \
       c->pme_base, c->pme_w, N, K, grid, 1, c->pme_self, c->pme_soff, v, vr, c->rl_cnt,       \
       c->rl_rows, (const double4*)c->rl_pos, cell, (const R*)c->rl_tt, c->rl_cap, o0, o1, o2, \
-      ostride, orr, nullptr)
-    switch (p) {
-      case 4: PME_GATHER(4); break;
-      case 6: PME_GATHER(6); break;
-      default: PME_GATHER(8);
+      ostride, orr, RS_ ? c->pme_rsum : nullptr)
+    if (rs) {
+      switch (p) {
+        case 4: PME_GATHER(4, true); break;
+        case 6: PME_GATHER(6, true); break;
+        default: PME_GATHER(8, true);
+      }
+    } else {
+      switch (p) {
+        case 4: PME_GATHER(4, false); break;
+        case 6: PME_GATHER(6, false); break;
+        default: PME_GATHER(8, false);
+      }
     }
 #undef PME_GATHER
     return BD_OK;
