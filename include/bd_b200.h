@@ -120,7 +120,8 @@ typedef struct {
   unsigned long long philox_seed;
   int mobility;              /* bd_mobility_kind */
   int precision;             /* bd_precision */
-  double lanczos_tol;        /* relative change of sqrt(M) z between iterations; 0 -> 1e-6 */
+  double lanczos_tol;        /* bound on the estimated relative error of sqrt(M) z (the
+                                geometric tail of the successive changes); 0 -> 1e-6 */
   int lanczos_max;           /* Krylov dimension cap, at most 400; 0 -> 200 */
   /* BD_MOB_PME discretisation (no reference counterpart): grid points per
    * reduced lattice direction (0 -> smallest 2^a 3^b 5^c >= 12.9 L / rc,
@@ -129,7 +130,9 @@ typedef struct {
    * B-spline order (even, 4..8; 0 -> 8), real-space cutoff (0 -> the smaller
    * of 10 and 0.43 L; at most 0.43 L), split parameter (0 -> 4 / cutoff) and the cap on
    * real-space pairs per bead (0 -> 2.5 times the mean number of beads within
-   * the cutoff, at least 512). */
+   * the cutoff, at least 512, and rows that overflow it are grown to 1.25
+   * times the longest row at the mobility build; an explicit cap that
+   * overflows is BD_ERR_NBR_OVERFLOW). */
   int pme_grid;
   int pme_order;
   double pme_rc;
